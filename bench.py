@@ -1,0 +1,316 @@
+"""Benchmark: matrix-element points/s of p p -> 3 jets (leading colour, f64) on B200.
+
+Workload (one step): 2^20 seeded RAMBO points at sqrt(s) = 13 TeV with jet cuts (pT > 20 GeV,
+|eta| < 5, Delta R > 0.4), split over the subprocess families gg>ggg, qg>qgg, qq~>ggg and
+gg>qq~g in proportion to seeded random weights; every point's |M|^2 resolved per helicity, all
+colour orderings summed, in f64 (bit for bit the reference runner's f64 arithmetic).
+
+* value: the batched device API, every family in one persistent launch (captured in a CUDA
+  graph), momenta resident in HBM (168 MB of inputs: larger than L2, so no flush is needed);
+* e2e: the reference-facing C ABI (pacman_recurrence_v1_run + _reduce_resolved per tile of 2^16
+  points) from pinned host buffers, the copies in the timed region;
+* roofline: the dominant kernel's algorithmic flops (fixed per-op counts) per launch over its
+  CUDA-event time, against this GPU's f64 FMA throughput measured in the same run;
+* cpu_baseline: the CPU oracle (the runner's arithmetic restated in C++, OpenMP over all cores)
+  on a bounded sample of the same families.
+
+usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+FAMILIES = ["gg>ggg", "qg>qgg", "qq~>ggg", "gg>qq~g"]
+POINTS = 1 << 20
+ECM = 13000.0
+SEED = 20261203
+TILE = 1 << 16
+
+
+def split_points(total, seed):
+    """The points per family: seeded random weights (Dirichlet), at least 1024 each."""
+    rng = np.random.default_rng(seed)
+    w = rng.dirichlet(np.ones(len(FAMILIES)))
+    n = np.maximum(1024, np.floor(w * total).astype(int))
+    n[0] += total - n.sum()
+    return [int(x) for x in n]
+
+
+def workload(rank=0):
+    from pacuda_b200 import phase_space, processes
+
+    counts = split_points(POINTS, SEED)
+    fams = []
+    for k, (name, n) in enumerate(zip(FAMILIES, counts)):
+        t = processes.template(name)
+        p = phase_space.sample(len(processes.PROCESSES[name]), n, SEED + 1000 * rank + k, ecm=ECM)
+        fams.append((name, t, p))
+    return fams
+
+
+class Clocks:
+    """nvidia-smi samples (every 200 ms) during the timed region."""
+
+    def __init__(self, index=0):
+        self.path = f"/tmp/bench_clocks_{os.getpid()}.csv"
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "200",
+                                          "-i", str(index)], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        self.proc.wait()
+        sm, mx, reasons = [], 0.0, set()
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for name, v in zip(["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"], f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def fp64_peak(torch, lib):
+    import ctypes as C
+
+    sink = torch.zeros(1 << 16, dtype=torch.float64, device="cuda")
+    s = torch.cuda.current_stream()
+    blocks, threads = C.c_uint32(), C.c_uint32()
+    iters = 20000
+    fn = lib.pacuda_b200_measure_fp64
+    fn.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]
+    for _ in range(2):
+        fn(C.c_void_p(sink.data_ptr()), iters, C.byref(blocks), C.byref(threads), C.c_void_p(s.cuda_stream))
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn(C.c_void_p(sink.data_ptr()), iters, C.byref(blocks), C.byref(threads), C.c_void_p(s.cuda_stream))
+        e1.record()
+        e1.synchronize()
+        flops = 2.0 * 8 * iters * blocks.value * threads.value
+        best = max(best, flops / (e0.elapsed_time(e1) * 1e-3))
+    return best / 1e12
+
+
+def cpu_baseline(fams, sample=2048):
+    """The oracle on the first `sample` points of each family, all host cores; points/s of the
+    family mix (each family's rate weighted by its share of the workload)."""
+    from oracle import oracle as O
+
+    counts = [p.shape[0] for _, _, p in fams]
+    total = sum(counts)
+    secs = 0.0
+    done = 0
+    for (name, t, p), n in zip(fams, counts):
+        m = min(sample, n)
+        t0 = time.perf_counter()
+        O.evaluate(t, p[:m], kernel=1)
+        dt = time.perf_counter() - t0
+        secs += dt * (n / m)  # the time of the family's full share at this rate
+        done += n
+    return {"value": total / secs, "unit": "points/s", "cores": os.cpu_count(), "kind": "port",
+            "sample": f"first {sample} points of each family (of {total}), OpenMP over all host cores, "
+                      f"rates weighted by the families' shares"}
+
+
+def e2e_abi(fams, steps, warmup, lib=None, kernel="f64"):
+    """points/s through the C ABI: per tile one run (forms on the device, amplitudes kept) and one
+    resolved reduction, from pinned host buffers."""
+    import ctypes as C
+
+    from pacuda_b200 import abi, phase_space
+    from pacuda_b200.runner import Runner
+
+    r = Runner(lib)
+    assert r.configure(kernel) == 0
+    jobs, h2d, d2h = [], 0, 0
+    for name, t, p in fams:
+        n = p.shape[0]
+        for s in range(0, n, TILE):
+            m = min(TILE, n - s)
+            ext = phase_space.source_major(p[s:s + m])
+            pin = r.lib.pacman_recurrence_v1_host_alloc(ext.nbytes)
+            hext = np.ctypeslib.as_array((C.c_double * ext.size).from_address(pin))
+            hext[:] = ext
+            args = t.call(hext, m, stride=TILE)
+            outp = r.lib.pacman_recurrence_v1_host_alloc(8 * m * t.outputs)
+            out = np.ctypeslib.as_array((C.c_double * (m * t.outputs)).from_address(outp))
+            red, keep = abi.reduce_resolved_args(t.planes, t.weights, t.offsets, out, m, 1, t.outputs, abi.OUTPUT_ZERO)
+            jobs.append((args, red, keep, out))
+            h2d += ext.nbytes
+            d2h += out.nbytes
+
+    def step():
+        for args, red, keep, out in jobs:
+            if r.run(args) != 0 or r.reduce_resolved(red) != 0:
+                raise RuntimeError("runner call failed")
+
+    for _ in range(warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        step()
+    dt = (time.perf_counter() - t0) / steps
+    total = sum(p.shape[0] for _, _, p in fams)
+    return {"value": total / dt, "unit": "points/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+            "tile": TILE, "calls_per_step": 2 * len(jobs)}, [j[3] for j in jobs]
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    metric = "matrix-element points/s (p p -> 3 jets, LC, f64)"
+    config = {"workload": "pp>3j LC f64: gg>ggg, qg>qgg, qq~>ggg, gg>qq~g", "points_per_gpu": POINTS,
+              "sqrt_s_gev": ECM, "cuts": "pT>20 GeV, |eta|<5, dR>0.4", "seed": SEED,
+              "l2": "inputs 168 MB per GPU > 126 MB L2 (no flush)", "parallelism": f"points sharded, {world} GPU(s)"}
+
+    if args.impl == "reference":
+        # the reference's path on the host: its arithmetic restated (the oracle, f64), all cores
+        if rank != 0:
+            return
+        fams = workload(0)
+        for _ in range(max(0, args.warmup)):
+            pass
+        vals = []
+        for _ in range(args.steps):
+            vals.append(cpu_baseline(fams, sample=512)["value"])
+        v = statistics.median(vals)
+        cb = {"value": v, "unit": "points/s", "cores": os.cpu_count(), "kind": "port",
+              "sample": "first 512 points of each family per step, rates weighted by the families' shares"}
+        print(json.dumps({"impl": "reference", "metric": metric, "value": v, "unit": "points/s", "n_gpus": 1,
+                          "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+                          "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config,
+                          "cpu_baseline": cb,
+                          "e2e": {"value": v, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        return
+
+    import torch
+
+    from pacuda_b200 import batch as B
+    from pacuda_b200 import build
+
+    build.build()
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    fams = workload(rank)
+    plans, ext, out = [], [], []
+    flops = 0.0
+    for name, t, p in fams:
+        pl = B.Plan(t, "f64")
+        plans.append(pl)
+        ext.append(torch.tensor(phase_space_major(p), dtype=torch.float64, device="cuda"))
+        out.append(torch.empty(p.shape[0] * t.outputs, dtype=torch.float64, device="cuda"))
+        flops += pl.flops * p.shape[0]
+    batch = B.Batch(plans, ext, out)
+    batch.tune()
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):
+        batch.capture(stream)
+    for _ in range(args.warmup):
+        batch.run(stream)
+    stream.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(int(os.environ.get("LOCAL_RANK", 0))) if rank == 0 else None
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        batch.run(stream)
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    clk = clocks.stop() if clocks else None
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    points = sum(p.shape[0] for _, _, p in fams) * world
+    value = points / (ms * 1e-3)
+    # the total |M|^2 of each family (the path's one exchange: summed over the ranks)
+    sums = torch.stack([o.sum() for o in out])
+    if world > 1:
+        dist.all_reduce(sums)
+    peak = fp64_peak(torch, B.lib())
+    achieved = flops / (ms * 1e-3) / 1e12 if world == 1 else flops / (ms * 1e-3) / 1e12
+    res = {"metric": metric, "value": value, "unit": "points/s", "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config,
+           "gpu_launches": args.steps * batch.launches,
+           "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                        "frac": achieved / peak, "traffic": None,
+                        "peak_source": "f64 FMA throughput measured in this run (2 flops per DFMA); the "
+                                       "reference's arithmetic has no FMA, so half of it is the ceiling",
+                        "flops_per_point": {n: pl.flops for (n, _, _), pl in zip(fams, plans)}},
+           "points_per_family": {n: p.shape[0] for n, _, p in fams},
+           "points_per_warp": {n: pl.points_per_warp for (n, _, _), pl in zip(fams, plans)},
+           "sum_m2_per_family": [float(x) for x in sums.cpu()]}
+    if clk:
+        res["clocks"] = clk
+    if rank == 0 and world == 1:
+        if not args.no_e2e:
+            e2e, _ = e2e_abi(fams, max(1, args.steps // 5), 1)
+            res["e2e"] = e2e
+        if not args.no_cpu:
+            res["cpu_baseline"] = cpu_baseline(fams)
+    if world > 1:
+        import torch.distributed as dist
+
+        del batch
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(res))
+
+
+def phase_space_major(p):
+    from pacuda_b200 import phase_space
+
+    return phase_space.source_major(p)
+
+
+if __name__ == "__main__":
+    main()

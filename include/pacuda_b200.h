@@ -1,0 +1,73 @@
+/* pacuda-b200: the batched, device-resident entry points of the recurrence runner.
+ *
+ * These have no counterpart in the reference (runner/pacman_recurrence.h): they are this
+ * library's B200 interface for callers that keep their phase-space points on the GPU. A plan is
+ * compiled once (its words and tables as a pacman_recurrence_call describes them, and its
+ * resolved reduction); a batch evaluates several plans, each on its own points, in one
+ * persistent kernel launch, and can be captured in a CUDA graph. Inputs and outputs are device
+ * arrays: per plan the external momenta as source-major planes [(leg * 4 + k) * count + i], the
+ * outputs as [point][output] (the resolved reduction from zero, OUTPUT_ZERO semantics).
+ * Statuses are the PACMAN_RECURRENCE_* codes. */
+#ifndef PACUDA_B200_H
+#define PACUDA_B200_H
+#include <stddef.h>
+#include <stdint.h>
+
+#include "pacman_recurrence.h"
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* pacman_recurrence_v1_configure accepts this larger options struct (struct_size = its size): the
+ * reference's fields, then the executor of runs (0: the on-chip executor when the plan's points
+ * fit a warp's shared memory, else the global-arena one; 1: always the global-arena executor;
+ * 2: the on-chip executor, or INVALID at run time when it does not fit) and the on-chip
+ * executor's points per warp (0: automatic). A runner given the reference's struct keeps the
+ * defaults. */
+typedef struct {
+    pacman_recurrence_options base;
+    uint32_t executor;
+    uint32_t points_per_warp;
+} pacuda_b200_options;
+enum { PACUDA_B200_EXECUTOR_AUTO = 0, PACUDA_B200_EXECUTOR_ARENA = 1, PACUDA_B200_EXECUTOR_ONCHIP = 2 };
+
+typedef struct pacuda_b200_plan pacuda_b200_plan;
+typedef struct pacuda_b200_batch pacuda_b200_batch;
+
+/* Compiles the plan of `call` (its words, widths, plane counts, scales, factors and form terms;
+ * its arrays and runs are not used) with the reduction (offsets[outputs + 1], planes, weights)
+ * for the kernel kind `kernel` (PACMAN_RECURRENCE_KERNEL_*). NULL on error, with a message on
+ * stderr. The plan may read no current plane before writing it (its inputs are its sources). */
+pacuda_b200_plan *pacuda_b200_plan_create(const pacman_recurrence_call *call, const uint32_t *offsets,
+                                          const uint32_t *planes, const double *weights, uint32_t outputs,
+                                          uint32_t kernel);
+void pacuda_b200_plan_destroy(pacuda_b200_plan *plan);
+/* the plan's algorithmic flops per point (fixed per-op counts) */
+uint64_t pacuda_b200_plan_flops(const pacuda_b200_plan *plan);
+/* points per warp (1, 2, 4, ..., 32), or 0 for the tuned or default choice */
+int pacuda_b200_plan_set_points_per_warp(pacuda_b200_plan *plan, uint32_t points_per_warp);
+uint32_t pacuda_b200_plan_points_per_warp(const pacuda_b200_plan *plan);
+
+/* A batch of `nplans` plans (all of one kernel kind); plan k on count[k] points. */
+pacuda_b200_batch *pacuda_b200_batch_create(pacuda_b200_plan *const *plans, uint32_t nplans,
+                                            const double *const *external, const uint32_t *count,
+                                            double *const *output);
+/* Times each plan's points-per-warp choices on its own points and keeps the fastest. */
+int pacuda_b200_batch_tune(pacuda_b200_batch *batch, void *stream);
+/* One persistent launch over every plan's points, on `stream` (a cudaStream_t; NULL: default). */
+int pacuda_b200_batch_run(pacuda_b200_batch *batch, void *stream);
+/* Captures the launch into a CUDA graph on `stream`; later runs replay it. */
+int pacuda_b200_batch_capture(pacuda_b200_batch *batch, void *stream);
+/* kernel launches of one run (1) */
+uint32_t pacuda_b200_batch_launches(const pacuda_b200_batch *batch);
+void pacuda_b200_batch_destroy(pacuda_b200_batch *batch);
+
+/* Measurement: launches blocks x threads threads that each run 8 independent chains of
+ * `iterations` f64 fused multiply-adds (2 flops each) on `stream`; the caller times it. `sink`
+ * is a device array of at least *blocks doubles (never written in practice). */
+int pacuda_b200_measure_fp64(double *sink, uint32_t iterations, uint32_t *blocks, uint32_t *threads, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

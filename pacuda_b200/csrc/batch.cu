@@ -1,0 +1,396 @@
+// The batched, device-resident entry points (include/pacuda_b200.h): plans compiled once,
+// batches of plans evaluated in one persistent launch of the on-chip executor.
+#include <cuda_runtime.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "../../include/pacuda_b200.h"
+#include "tiled.cuh"
+#include "tiled_host.h"
+
+using namespace pacuda;
+
+namespace {
+
+const char *const kTag = "pacuda-b200";
+
+bool failed(cudaError_t e, const char *what) {
+    if (e == cudaSuccess) return false;
+    fprintf(stderr, "%s: %s: %s\n", kTag, what, cudaGetErrorString(e));
+    return true;
+}
+
+template <class T> bool to_device(T **dst, const T *src, size_t n) {
+    if (failed(cudaMalloc((void **)dst, std::max<size_t>(1, n) * sizeof(T)), "allocation")) return false;
+    return n == 0 || !failed(cudaMemcpy(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice), "copy");
+}
+
+int device_sms() {
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return sms;
+}
+
+}  // namespace
+
+struct pacuda_b200_plan {
+    int kernel = PACMAN_RECURRENCE_KERNEL_F64;
+    Program prog;
+    TiledDevice tiled;
+    uint32_t forms = 0, scales = 0, factors = 0, outputs = 0;
+    double *consts = nullptr;  // f64 scales re, im, factors re, im; then the kind's layout
+    uint32_t *terms = nullptr;  // form_terms (2 per form), then term_slots
+    double *coefficients = nullptr;
+    uint32_t *red_offsets = nullptr, *red_slots = nullptr;
+    double *red_weights = nullptr;
+    uint32_t log_p = 0;
+    bool fixed = false;
+};
+
+struct LaunchBlock;  // device and pinned host copies of a launch's descriptors
+
+struct pacuda_b200_batch {
+    std::vector<pacuda_b200_plan *> plans;
+    std::vector<const double *> external;
+    std::vector<uint32_t> count;
+    std::vector<double *> output;
+    // descriptor block: TiledPlan[n] | item_first[n + 1] | external[n] | output[n] | count[n] | counter
+    unsigned char *host = nullptr, *device = nullptr;
+    size_t bytes = 0;
+    int warps = 0, sms = 0;
+    size_t warp_bytes = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+namespace {
+
+void fill_plan(const pacuda_b200_plan *p, TiledPlan &d) {
+    memset(&d, 0, sizeof d);
+    describe(p->tiled, p->forms, p->log_p, tiled_warp_bytes(p->tiled.host, p->forms, p->kernel, p->log_p), d);
+    d.s64 = p->consts;
+    d.f64 = p->consts + 2 * p->scales;
+    d.kconst = p->consts + 2 * (p->scales + p->factors);
+    d.scales = p->scales;
+    d.factors = p->factors;
+    d.form_terms = p->terms;
+    d.term_slots = p->terms + 2 * p->forms;
+    d.coefficients = p->coefficients;
+    d.red_offsets = p->red_offsets;
+    d.red_slots = p->red_slots;
+    d.red_weights = p->red_weights;
+    d.outputs = p->outputs;
+}
+
+struct Offsets {
+    size_t plans, items, external, output, count, counter, total;
+};
+Offsets layout(size_t n) {
+    Offsets o;
+    o.plans = 0;
+    o.items = (o.plans + n * sizeof(TiledPlan) + 15) / 16 * 16;
+    o.external = (o.items + (n + 1) * 8 + 15) / 16 * 16;
+    o.output = o.external + n * 8;
+    o.count = o.output + n * 8;
+    o.counter = (o.count + n * 4 + 15) / 16 * 16;
+    o.total = o.counter + 16;
+    return o;
+}
+
+// the host block from the batch's current choices; the launch's shared memory and warps
+bool prepare(pacuda_b200_batch *b) {
+    size_t n = b->plans.size();
+    Offsets o = layout(n);
+    if (!b->host) {
+        b->bytes = o.total;
+        if (failed(cudaMallocHost((void **)&b->host, b->bytes), "pinned descriptors") ||
+            failed(cudaMalloc((void **)&b->device, b->bytes), "descriptors"))
+            return false;
+    }
+    memset(b->host, 0, b->bytes);
+    TiledPlan *plans = (TiledPlan *)(b->host + o.plans);
+    unsigned long long *items = (unsigned long long *)(b->host + o.items);
+    b->warp_bytes = 0;
+    items[0] = 0;
+    for (size_t k = 0; k < n; k++) {
+        fill_plan(b->plans[k], plans[k]);
+        b->warp_bytes = std::max<size_t>(b->warp_bytes, plans[k].warp_bytes);
+        uint32_t per = 1u << b->plans[k]->log_p;
+        items[k + 1] = items[k] + (b->count[k] + per - 1) / per;
+    }
+    memcpy(b->host + o.external, b->external.data(), n * 8);
+    memcpy(b->host + o.output, b->output.data(), n * 8);
+    memcpy(b->host + o.count, b->count.data(), n * 4);
+    b->warps = std::min(16, tiled_warps(b->plans[0]->kernel, b->warp_bytes));
+    if (b->warps <= 0) {
+        fprintf(stderr, "%s: a plan's points do not fit one warp's shared memory\n", kTag);
+        return false;
+    }
+    return true;
+}
+
+TiledLaunch launch_args(const pacuda_b200_batch *b) {
+    size_t n = b->plans.size();
+    Offsets o = layout(n);
+    TiledLaunch L;
+    memset(&L, 0, sizeof L);
+    L.plans = (const TiledPlan *)(b->device + o.plans);
+    L.nplans = (uint32_t)n;
+    L.item_first = (const unsigned long long *)(b->device + o.items);
+    L.external = (const double *const *)(b->device + o.external);
+    L.output = (double *const *)(b->device + o.output);
+    L.count = (const uint32_t *)(b->device + o.count);
+    L.counter = (unsigned long long *)(b->device + o.counter);
+    L.abi = false;
+    return L;
+}
+
+int launch(pacuda_b200_batch *b, cudaStream_t s) {
+    if (failed(cudaMemcpyAsync(b->device, b->host, b->bytes, cudaMemcpyHostToDevice, s), "descriptors"))
+        return PACMAN_RECURRENCE_DEVICE_ERROR;
+    if (!launch_tiled(b->plans[0]->kernel, launch_args(b), b->warps, b->warp_bytes, b->sms, s) ||
+        failed(cudaGetLastError(), "launch"))
+        return PACMAN_RECURRENCE_DEVICE_ERROR;
+    return PACMAN_RECURRENCE_OK;
+}
+
+// the largest points-per-warp whose warps still fill a block of 8, else 1
+uint32_t default_log_p(const pacuda_b200_plan *p) {
+    uint32_t best = 0;
+    for (uint32_t lp = 0; lp <= 5; lp++) {
+        int w = tiled_warps(p->kernel, tiled_warp_bytes(p->tiled.host, p->forms, p->kernel, lp));
+        if (w >= 8) best = lp;
+    }
+    return best;
+}
+
+}  // namespace
+
+extern "C" pacuda_b200_plan *pacuda_b200_plan_create(const pacman_recurrence_call *c, const uint32_t *offsets,
+                                                     const uint32_t *planes, const double *weights, uint32_t outputs,
+                                                     uint32_t kernel) {
+    if (!c || c->abi_version != PACMAN_RECURRENCE_ABI || c->struct_size != sizeof(pacman_recurrence_call) ||
+        !c->words || kernel > PACMAN_RECURRENCE_KERNEL_MIXED64 || !offsets || (offsets[outputs] && (!planes || !weights)) ||
+        (c->scale_count && (!c->scale_re || !c->scale_im)) || (c->factor_count && (!c->factor_re || !c->factor_im)) ||
+        !c->form_terms || (c->term_count && (!c->term_slots || !c->term_coefficients))) {
+        fprintf(stderr, "%s: plan_create: an invalid call description\n", kTag);
+        return nullptr;
+    }
+    uint32_t forms = c->momentum_planes / 4;
+    for (uint32_t f = 0; f < forms; f++)
+        if (c->form_terms[2 * f] > c->term_count || c->form_terms[2 * f + 1] > c->term_count - c->form_terms[2 * f]) {
+            fprintf(stderr, "%s: plan_create: a form's terms outside the term table\n", kTag);
+            return nullptr;
+        }
+    for (uint32_t t = 0; t < c->term_count; t++)
+        if (c->term_slots[t] >= c->external_count) {
+            fprintf(stderr, "%s: plan_create: a term names a leg outside the external momenta\n", kTag);
+            return nullptr;
+        }
+    for (uint32_t o = 0; o < outputs; o++)
+        if (offsets[o] > offsets[o + 1]) return nullptr;
+    for (uint32_t k = 0; k < offsets[outputs]; k++)
+        if (planes[k] >= c->amplitude_planes) {
+            fprintf(stderr, "%s: plan_create: a reduction plane outside the amplitudes\n", kTag);
+            return nullptr;
+        }
+    auto *p = new pacuda_b200_plan();
+    p->kernel = (int)kernel;
+    Limits lim{c->current_planes, c->amplitude_planes, forms, c->scale_count, c->factor_count};
+    BuildError e = build_program(c->words, c->word_count, c->width, true, lim, p->prog);
+    if (e.status) {
+        fprintf(stderr, "%s: plan_create: %s\n", kTag, e.message.c_str());
+        delete p;
+        return nullptr;
+    }
+    if (!p->prog.reads_before_write.empty()) {
+        fprintf(stderr, "%s: plan_create: the plan reads %zu current planes before writing them\n", kTag,
+                p->prog.reads_before_write.size());
+        delete p;
+        return nullptr;
+    }
+    if (!build_schedule(p->prog, c->current_planes, c->amplitude_planes, p->tiled.host)) {
+        fprintf(stderr, "%s: plan_create: %s\n", kTag, p->tiled.host.why.c_str());
+        delete p;
+        return nullptr;
+    }
+    p->forms = forms;
+    p->scales = c->scale_count;
+    p->factors = c->factor_count;
+    p->outputs = outputs;
+    // constants: f64, then the kind's layout (df64 pairs unless f64)
+    size_t nc = 2 * ((size_t)c->scale_count + c->factor_count);
+    std::vector<double> k(2 * nc + 1, 0.0);
+    for (uint32_t i = 0; i < c->scale_count; i++) { k[i] = c->scale_re[i]; k[c->scale_count + i] = c->scale_im[i]; }
+    double *f = k.data() + 2 * c->scale_count;
+    for (uint32_t i = 0; i < c->factor_count; i++) { f[i] = c->factor_re[i]; f[c->factor_count + i] = c->factor_im[i]; }
+    for (size_t i = 0; i < nc; i++) {
+        if (kernel == PACMAN_RECURRENCE_KERNEL_F64) {
+            k[nc + i] = k[i];
+        } else {
+            float hi = (float)k[i], lo = (float)(k[i] - (double)hi);
+            memcpy(&k[nc + i], &hi, 4);
+            memcpy((char *)&k[nc + i] + 4, &lo, 4);
+        }
+    }
+    std::vector<uint32_t> terms(c->form_terms, c->form_terms + 2 * forms);
+    terms.insert(terms.end(), c->term_slots, c->term_slots + c->term_count);
+    std::vector<uint32_t> slots(offsets[outputs]);
+    for (uint32_t j = 0; j < offsets[outputs]; j++) slots[j] = p->tiled.host.amp_slot_of[planes[j]];
+    bool ok = to_device(&p->consts, k.data(), k.size()) && to_device(&p->terms, terms.data(), terms.size()) &&
+              to_device(&p->coefficients, c->term_coefficients, c->term_count) &&
+              to_device(&p->red_offsets, offsets, (size_t)outputs + 1) &&
+              to_device(&p->red_slots, slots.data(), slots.size()) &&
+              to_device(&p->red_weights, weights, offsets[outputs]) && upload_schedule(p->tiled, 0) &&
+              !failed(cudaDeviceSynchronize(), "plan upload");
+    if (!ok) {
+        pacuda_b200_plan_destroy(p);
+        return nullptr;
+    }
+    p->log_p = default_log_p(p);
+    return p;
+}
+
+extern "C" void pacuda_b200_plan_destroy(pacuda_b200_plan *p) {
+    if (!p) return;
+    p->tiled.release();
+    cudaFree(p->consts);
+    cudaFree(p->terms);
+    cudaFree(p->coefficients);
+    cudaFree(p->red_offsets);
+    cudaFree(p->red_slots);
+    cudaFree(p->red_weights);
+    delete p;
+}
+
+extern "C" uint64_t pacuda_b200_plan_flops(const pacuda_b200_plan *p) { return p ? p->prog.flops : 0; }
+
+extern "C" int pacuda_b200_plan_set_points_per_warp(pacuda_b200_plan *p, uint32_t per) {
+    if (!p || per > 32 || (per & (per - 1))) return PACMAN_RECURRENCE_INVALID;
+    if (per == 0) {
+        p->fixed = false;
+        p->log_p = default_log_p(p);
+        return PACMAN_RECURRENCE_OK;
+    }
+    uint32_t lp = 0;
+    while ((1u << lp) < per) lp++;
+    if (tiled_warps(p->kernel, tiled_warp_bytes(p->tiled.host, p->forms, p->kernel, lp)) <= 0)
+        return PACMAN_RECURRENCE_INVALID;
+    p->log_p = lp;
+    p->fixed = true;
+    return PACMAN_RECURRENCE_OK;
+}
+
+extern "C" uint32_t pacuda_b200_plan_points_per_warp(const pacuda_b200_plan *p) { return p ? 1u << p->log_p : 0; }
+
+extern "C" pacuda_b200_batch *pacuda_b200_batch_create(pacuda_b200_plan *const *plans, uint32_t nplans,
+                                                       const double *const *external, const uint32_t *count,
+                                                       double *const *output) {
+    if (!plans || !nplans || !external || !count || !output) return nullptr;
+    for (uint32_t k = 0; k < nplans; k++)
+        if (!plans[k] || plans[k]->kernel != plans[0]->kernel || !count[k] || !external[k] || !output[k]) {
+            fprintf(stderr, "%s: batch_create: plan %u: a missing plan, array or point count, or another kernel kind\n",
+                    kTag, k);
+            return nullptr;
+        }
+    auto *b = new pacuda_b200_batch();
+    b->plans.assign(plans, plans + nplans);
+    b->external.assign(external, external + nplans);
+    b->count.assign(count, count + nplans);
+    b->output.assign(output, output + nplans);
+    b->sms = device_sms();
+    if (!prepare(b)) {
+        pacuda_b200_batch_destroy(b);
+        return nullptr;
+    }
+    return b;
+}
+
+extern "C" int pacuda_b200_batch_run(pacuda_b200_batch *b, void *stream) {
+    if (!b) return PACMAN_RECURRENCE_INVALID;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (b->exec) return failed(cudaGraphLaunch(b->exec, s), "graph") ? PACMAN_RECURRENCE_DEVICE_ERROR : PACMAN_RECURRENCE_OK;
+    return launch(b, s);
+}
+
+extern "C" int pacuda_b200_batch_capture(pacuda_b200_batch *b, void *stream) {
+    if (!b) return PACMAN_RECURRENCE_INVALID;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (b->exec) {
+        cudaGraphExecDestroy(b->exec);
+        cudaGraphDestroy(b->graph);
+        b->exec = nullptr;
+        b->graph = nullptr;
+    }
+    if (failed(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "capture")) return PACMAN_RECURRENCE_DEVICE_ERROR;
+    int st = launch(b, s);
+    cudaError_t e = cudaStreamEndCapture(s, &b->graph);
+    if (st != PACMAN_RECURRENCE_OK || failed(e, "capture") ||
+        failed(cudaGraphInstantiate(&b->exec, b->graph, 0), "graph instantiation"))
+        return PACMAN_RECURRENCE_DEVICE_ERROR;
+    return PACMAN_RECURRENCE_OK;
+}
+
+extern "C" int pacuda_b200_batch_tune(pacuda_b200_batch *b, void *stream) {
+    if (!b) return PACMAN_RECURRENCE_INVALID;
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaEvent_t t0, t1;
+    cudaEventCreate(&t0);
+    cudaEventCreate(&t1);
+    for (size_t k = 0; k < b->plans.size(); k++) {
+        pacuda_b200_plan *p = b->plans[k];
+        if (p->fixed) continue;
+        uint32_t sample = std::min<uint32_t>(b->count[k], 1u << 16);
+        pacuda_b200_plan *one[1] = {p};
+        const double *ext[1] = {b->external[k]};
+        double *out[1] = {b->output[k]};
+        float best = 1e30f;
+        uint32_t best_lp = p->log_p;
+        for (uint32_t lp = 0; lp <= 5; lp++) {
+            if (tiled_warps(p->kernel, tiled_warp_bytes(p->tiled.host, p->forms, p->kernel, lp)) < 2) continue;
+            p->log_p = lp;
+            // the external momenta of the first `sample` points: a plane stride of count[k]
+            // would differ, so the sample is all points when they are few, else the timing
+            // runs on the whole plan
+            uint32_t n = b->count[k];
+            (void)sample;
+            pacuda_b200_batch *tb = pacuda_b200_batch_create(one, 1, ext, &n, out);
+            if (!tb) continue;
+            float ms = 0;
+            bool ok = launch(tb, s) == PACMAN_RECURRENCE_OK;
+            for (int rep = 0; ok && rep < 3; rep++) {
+                cudaEventRecord(t0, s);
+                ok = launch(tb, s) == PACMAN_RECURRENCE_OK;
+                cudaEventRecord(t1, s);
+                cudaEventSynchronize(t1);
+                float m = 0;
+                cudaEventElapsedTime(&m, t0, t1);
+                ms = rep == 0 ? m : std::min(ms, m);
+            }
+            pacuda_b200_batch_destroy(tb);
+            if (ok && ms < best) {
+                best = ms;
+                best_lp = lp;
+            }
+        }
+        p->log_p = best_lp;
+    }
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    return prepare(b) ? PACMAN_RECURRENCE_OK : PACMAN_RECURRENCE_DEVICE_ERROR;
+}
+
+extern "C" uint32_t pacuda_b200_batch_launches(const pacuda_b200_batch *b) { return b ? 1 : 0; }
+
+extern "C" void pacuda_b200_batch_destroy(pacuda_b200_batch *b) {
+    if (!b) return;
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    cudaFreeHost(b->host);
+    cudaFree(b->device);
+    delete b;
+}

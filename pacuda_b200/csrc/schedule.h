@@ -1,0 +1,38 @@
+// The on-chip schedule of a plan: its rows grouped into tasks, the tasks into dataflow levels,
+// and its current planes packed into shared-memory slots by liveness.
+//
+// A task is what one lane runs for one point with its sums in registers: a source row, a
+// destination's run of contribution rows (F_FIRST .. F_LAST) with the propagator that
+// follows it on the same current, a propagator, an identity or clear over one current, or a
+// destination amplitude's consecutive closures. Tasks of one level read nothing another task of
+// that level writes, so the lanes of a point run them in any order; each current's and each
+// amplitude's rows keep their order, so every value is the one the row order gives, bit for bit.
+#pragma once
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "program.h"
+
+namespace pacuda {
+
+enum : uint32_t { F_WB = 8 };  // the instruction's written values also go to the global arena
+
+struct Schedule {
+    std::vector<Ins> ins;               // task instructions; operands are slots
+    std::vector<uint32_t> task_first;   // tasks + 1 entries into ins
+    std::vector<uint32_t> level_first;  // levels + 1 entries into tasks
+    uint32_t cur_slots = 0;             // complex current slots per point
+    uint32_t amp_slots = 0;             // complex amplitude slots per point
+    std::vector<uint32_t> loads;        // live-in currents: (global plane, slot, count) triples
+    std::vector<uint32_t> amp_planes;   // per amplitude slot, its global amplitude plane
+    std::vector<uint32_t> amp_slot_of;  // per global amplitude plane, its slot or ~0u
+    uint32_t max_task_len = 0;
+    std::string why;                    // empty when the schedule exists
+};
+
+// builds the schedule of a program; `forms` is the plan's momentum form count
+bool build_schedule(const Program &p, uint32_t current_planes, uint32_t amplitude_planes, Schedule &out);
+
+}  // namespace pacuda

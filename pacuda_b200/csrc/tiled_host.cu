@@ -1,0 +1,93 @@
+// Host helpers of the on-chip executor (tiled_host.h).
+#include <stdio.h>
+
+#include <algorithm>
+
+#include "../../include/pacman_recurrence.h"
+#include "tiled.cuh"
+#include "tiled_host.h"
+
+namespace pacuda {
+
+namespace {
+template <class T> bool put(T **dst, const std::vector<T> &v, cudaStream_t s) {
+    size_t bytes = std::max<size_t>(1, v.size()) * sizeof(T);
+    if (cudaMalloc((void **)dst, bytes) != cudaSuccess) return false;
+    return v.empty() || cudaMemcpyAsync(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s) == cudaSuccess;
+}
+
+template <class K> const void *kernel_of() { return (const void *)run_tiled<K>; }
+
+const void *kernel_for(int kernel) {
+    switch (kernel) {
+    case PACMAN_RECURRENCE_KERNEL_F64: return kernel_of<KindF64>();
+    case PACMAN_RECURRENCE_KERNEL_MIXED: return kernel_of<KindMixed>();
+    case PACMAN_RECURRENCE_KERNEL_MIXED64: return kernel_of<KindMixed64>();
+    default: return kernel_of<KindDF64>();
+    }
+}
+}  // namespace
+
+void TiledDevice::release() {
+    cudaFree(ins);
+    cudaFree(task_first);
+    cudaFree(level_first);
+    cudaFree(loads);
+    cudaFree(amp_planes);
+    ins = nullptr;
+    task_first = level_first = loads = amp_planes = nullptr;
+    ok = false;
+}
+
+bool upload_schedule(TiledDevice &t, cudaStream_t s) {
+    t.ok = put(&t.ins, t.host.ins, s) && put(&t.task_first, t.host.task_first, s) &&
+           put(&t.level_first, t.host.level_first, s) && put(&t.loads, t.host.loads, s) &&
+           put(&t.amp_planes, t.host.amp_planes, s);
+    return t.ok;
+}
+
+size_t tiled_warp_bytes(const Schedule &s, uint32_t forms, int kernel, uint32_t log_p) {
+    size_t value = kernel == PACMAN_RECURRENCE_KERNEL_MIXED || kernel == PACMAN_RECURRENCE_KERNEL_MIXED64 ? 4 : 8;
+    size_t per_point = 2 * value * s.cur_slots + 2 * 8 * s.amp_slots + 8 * 4 * (size_t)forms;
+    per_point = (per_point + 15) / 16 * 16;
+    return per_point << log_p;
+}
+
+int tiled_warps(int kernel, size_t warp_bytes) {
+    cudaFuncAttributes attr;
+    if (cudaFuncGetAttributes(&attr, kernel_for(kernel)) != cudaSuccess) return 0;
+    int dev = 0, smem = 0, regs = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaDeviceGetAttribute(&regs, cudaDevAttrMaxRegistersPerBlock, dev);
+    int by_smem = warp_bytes ? (int)((size_t)(smem - attr.sharedSizeBytes) / warp_bytes) : 32;
+    int per_warp_regs = ((attr.numRegs * 32 + 255) / 256) * 256;
+    int by_regs = per_warp_regs ? regs / per_warp_regs : 32;
+    int by_threads = attr.maxThreadsPerBlock / 32;
+    return std::max(0, std::min({32, by_smem, by_regs, by_threads}));
+}
+
+void describe(const TiledDevice &t, uint32_t forms, uint32_t log_p, size_t warp_bytes, TiledPlan &p) {
+    p.ins = t.ins;
+    p.task_first = t.task_first;
+    p.level_first = t.level_first;
+    p.levels = (uint32_t)t.host.level_first.size() - 1;
+    p.cur_slots = t.host.cur_slots;
+    p.amp_slots = t.host.amp_slots;
+    p.forms = forms;
+    p.log_p = log_p;
+    p.warp_bytes = (uint32_t)warp_bytes;
+    p.loads = t.loads;
+    p.nloads = (uint32_t)t.host.loads.size() / 3;
+    p.amp_planes = t.amp_planes;
+}
+
+bool launch_tiled(int kernel, const TiledLaunch &args, int warps, size_t warp_bytes, int sms, cudaStream_t stream) {
+    const void *fn = kernel_for(kernel);
+    size_t smem = warp_bytes * (size_t)warps;
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return false;
+    void *params[] = {(void *)&args};
+    return cudaLaunchKernel(fn, dim3(sms), dim3(32 * warps), params, smem, stream) == cudaSuccess;
+}
+
+}  // namespace pacuda

@@ -1,0 +1,81 @@
+"""The batched device API: several plans in one persistent launch, each plan's resolved outputs
+equal to the oracle's bit for bit, for every points-per-warp choice and kernel kind; the tuned and
+graph-captured runs give the same bits."""
+import numpy as np
+import pytest
+
+from tests import scenarios as S
+from oracle import oracle as O
+from pacuda_b200 import abi, phase_space, processes
+
+NAMES = ["gg>ggg", "qg>qgg", "qq~>ggg", "gg>qq~g"]
+
+
+def setup(kind, counts):
+    import torch
+    from pacuda_b200 import batch as B
+
+    plans, ext, out, want = [], [], [], []
+    for name, n in zip(NAMES, counts):
+        t = processes.template(name)
+        p = phase_space.sample(len(processes.PROCESSES[name]), n, 17 + n)
+        _, w = O.evaluate(t, p, kernel=abi.KERNELS[kind])
+        plans.append(B.Plan(t, kind))
+        ext.append(torch.tensor(phase_space.source_major(p), dtype=torch.float64, device="cuda"))
+        out.append(torch.full((n * t.outputs,), float("nan"), dtype=torch.float64, device="cuda"))
+        want.append(w)
+    return plans, ext, out, want
+
+
+def check(out, want):
+    for o, w in zip(out, want):
+        got = o.cpu().numpy().reshape(w.shape)
+        assert np.array_equal(got.view(np.uint64), w.view(np.uint64)), np.abs(got - w).max()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", ["f64", "df64", "mixed", "mixed64"])
+def test_batch_matches_oracle_bitwise(kind):
+    from pacuda_b200 import batch as B
+    import torch
+
+    plans, ext, out, want = setup(kind, [70, 33, 129, 5])
+    b = B.Batch(plans, ext, out)
+    b.run()
+    torch.cuda.synchronize()
+    check(out, want)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("per", [1, 2, 4, 8, 16, 32])
+def test_every_points_per_warp_gives_the_same_bits(per):
+    from pacuda_b200 import batch as B
+    import torch
+
+    plans, ext, out, want = setup("f64", [70, 33, 129, 5])
+    for p in plans:
+        try:
+            p.points_per_warp = per
+        except Exception:
+            pytest.skip(f"{per} points per warp do not fit")
+    b = B.Batch(plans, ext, out)
+    b.run()
+    torch.cuda.synchronize()
+    check(out, want)
+
+
+@pytest.mark.gpu
+def test_tuned_and_captured_runs_give_the_same_bits():
+    from pacuda_b200 import batch as B
+    import torch
+
+    plans, ext, out, want = setup("f64", [300, 200, 100, 50])
+    b = B.Batch(plans, ext, out)
+    b.tune()
+    for o in out:
+        o.fill_(float("nan"))
+    b.capture()
+    b.run()
+    torch.cuda.synchronize()
+    check(out, want)
+    assert b.launches == 1
