@@ -186,6 +186,7 @@ def e2e_abi(fams, steps, warmup, lib=None, kernel="f64"):
 
 
 def main():
+    global POINTS, FAMILIES
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
@@ -193,13 +194,21 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--family", default=None, help="one subprocess family alone (profiling cases)")
+    ap.add_argument("--points", type=int, default=POINTS, help="points per GPU")
+    ap.add_argument("--no-tune", action="store_true", help="keep the default points per warp")
+    ap.add_argument("--lanes-per-point", type=int, default=0)
     args = ap.parse_args()
+    POINTS = args.points
+    if args.family:
+        FAMILIES = [args.family]
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     metric = "matrix-element points/s (p p -> 3 jets, LC, f64)"
-    config = {"workload": "pp>3j LC f64: gg>ggg, qg>qgg, qq~>ggg, gg>qq~g", "points_per_gpu": POINTS,
+    config = {"workload": "pp>3j LC f64: " + ", ".join(FAMILIES), "points_per_gpu": POINTS,
               "sqrt_s_gev": ECM, "cuts": "pT>20 GeV, |eta|<5, dR>0.4", "seed": SEED,
-              "l2": "inputs 168 MB per GPU > 126 MB L2 (no flush)", "parallelism": f"points sharded, {world} GPU(s)"}
+              "l2": f"inputs {POINTS * 160 / 1e6:.0f} MB per GPU" + (" > 126 MB L2 (no flush)" if POINTS * 160 > 126e6 else ""),
+              "parallelism": f"points sharded, {world} GPU(s)"}
 
     if args.impl == "reference":
         # the reference's path on the host: its arithmetic restated (the oracle, f64), all cores
@@ -243,8 +252,12 @@ def main():
         ext.append(torch.tensor(phase_space_major(p), dtype=torch.float64, device="cuda"))
         out.append(torch.empty(p.shape[0] * t.outputs, dtype=torch.float64, device="cuda"))
         flops += pl.flops * p.shape[0]
+    if args.lanes_per_point:
+        for pl in plans:
+            pl.lanes_per_point = args.lanes_per_point
     batch = B.Batch(plans, ext, out)
-    batch.tune()
+    if not args.no_tune and not args.lanes_per_point:
+        batch.tune()
     stream = torch.cuda.Stream()
     with torch.cuda.stream(stream):
         batch.capture(stream)
@@ -287,7 +300,7 @@ def main():
                                        "reference's arithmetic has no FMA, so half of it is the ceiling",
                         "flops_per_point": {n: pl.flops for (n, _, _), pl in zip(fams, plans)}},
            "points_per_family": {n: p.shape[0] for n, _, p in fams},
-           "points_per_warp": {n: pl.points_per_warp for (n, _, _), pl in zip(fams, plans)},
+           "lanes_per_point": {n: pl.lanes_per_point for (n, _, _), pl in zip(fams, plans)},
            "sum_m2_per_family": [float(x) for x in sums.cpu()]}
     if clk:
         res["clocks"] = clk

@@ -22,12 +22,12 @@ extern "C" {
  * reference's fields, then the executor of runs (0: the on-chip executor when the plan's points
  * fit a warp's shared memory, else the global-arena one; 1: always the global-arena executor;
  * 2: the on-chip executor, or INVALID at run time when it does not fit) and the on-chip
- * executor's points per warp (0: automatic). A runner given the reference's struct keeps the
+ * executor's lanes per point (0: automatic). A runner given the reference's struct keeps the
  * defaults. */
 typedef struct {
     pacman_recurrence_options base;
     uint32_t executor;
-    uint32_t points_per_warp;
+    uint32_t lanes_per_point;
 } pacuda_b200_options;
 enum { PACUDA_B200_EXECUTOR_AUTO = 0, PACUDA_B200_EXECUTOR_ARENA = 1, PACUDA_B200_EXECUTOR_ONCHIP = 2 };
 
@@ -44,15 +44,17 @@ pacuda_b200_plan *pacuda_b200_plan_create(const pacman_recurrence_call *call, co
 void pacuda_b200_plan_destroy(pacuda_b200_plan *plan);
 /* the plan's algorithmic flops per point (fixed per-op counts) */
 uint64_t pacuda_b200_plan_flops(const pacuda_b200_plan *plan);
-/* points per warp (1, 2, 4, ..., 32), or 0 for the tuned or default choice */
-int pacuda_b200_plan_set_points_per_warp(pacuda_b200_plan *plan, uint32_t points_per_warp);
-uint32_t pacuda_b200_plan_points_per_warp(const pacuda_b200_plan *plan);
+/* the lanes that run one point's tasks (1, 2, 4, ..., 512: above 32 a point spans several warps),
+ * or 0 for the tuned or default choice (the fewest whose block of points fits shared memory);
+ * INVALID when the block's points do not fit */
+int pacuda_b200_plan_set_lanes_per_point(pacuda_b200_plan *plan, uint32_t lanes);
+uint32_t pacuda_b200_plan_lanes_per_point(const pacuda_b200_plan *plan);
 
 /* A batch of `nplans` plans (all of one kernel kind); plan k on count[k] points. */
 pacuda_b200_batch *pacuda_b200_batch_create(pacuda_b200_plan *const *plans, uint32_t nplans,
                                             const double *const *external, const uint32_t *count,
                                             double *const *output);
-/* Times each plan's points-per-warp choices on its own points and keeps the fastest. */
+/* Times each plan's lanes-per-point choices on its own points and keeps the fastest. */
 int pacuda_b200_batch_tune(pacuda_b200_batch *batch, void *stream);
 /* One persistent launch over every plan's points, on `stream` (a cudaStream_t; NULL: default). */
 int pacuda_b200_batch_run(pacuda_b200_batch *batch, void *stream);

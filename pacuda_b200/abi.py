@@ -190,20 +190,20 @@ def reduce_sample_args(planes, weights, offsets, helicity, points, random, scale
 
 class B200Options(C.Structure):
     """pacuda_b200_options (include/pacuda_b200.h): the reference's options, then the executor and
-    the on-chip executor's points per warp."""
+    the on-chip executor's lanes per point."""
 
-    _fields_ = [("base", Options), ("executor", C.c_uint32), ("points_per_warp", C.c_uint32)]
+    _fields_ = [("base", Options), ("executor", C.c_uint32), ("lanes_per_point", C.c_uint32)]
 
 
 EXECUTORS = {"auto": 0, "arena": 1, "onchip": 2}
 
 
-def options(kernel="f64", block=0, no_sort=False, stats=False, executor=None, points_per_warp=0):
+def options(kernel="f64", block=0, no_sort=False, stats=False, executor=None, lanes_per_point=0):
     """The configuration struct: the reference's, or this library's larger one when an executor
-    or points per warp is given."""
+    or lanes per point is given."""
     k = KERNELS[kernel] if isinstance(kernel, str) else int(kernel)
     base = Options(ABI, C.sizeof(Options), k, block, 1 if no_sort else 0, 1 if stats else 0)
-    if executor is None and not points_per_warp:
+    if executor is None and not lanes_per_point:
         return base
     base.struct_size = C.sizeof(B200Options)
-    return B200Options(base, EXECUTORS[executor or "auto"], points_per_warp)
+    return B200Options(base, EXECUTORS[executor or "auto"], lanes_per_point)

@@ -22,9 +22,9 @@ def lib(path=None):
         L.pacuda_b200_plan_destroy.argtypes = [C.c_void_p]
         L.pacuda_b200_plan_flops.argtypes = [C.c_void_p]
         L.pacuda_b200_plan_flops.restype = C.c_uint64
-        L.pacuda_b200_plan_set_points_per_warp.argtypes = [C.c_void_p, C.c_uint32]
-        L.pacuda_b200_plan_points_per_warp.argtypes = [C.c_void_p]
-        L.pacuda_b200_plan_points_per_warp.restype = C.c_uint32
+        L.pacuda_b200_plan_set_lanes_per_point.argtypes = [C.c_void_p, C.c_uint32]
+        L.pacuda_b200_plan_lanes_per_point.argtypes = [C.c_void_p]
+        L.pacuda_b200_plan_lanes_per_point.restype = C.c_uint32
         L.pacuda_b200_batch_create.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]
         L.pacuda_b200_batch_create.restype = C.c_void_p
         for name in ("pacuda_b200_batch_tune", "pacuda_b200_batch_run", "pacuda_b200_batch_capture"):
@@ -56,13 +56,13 @@ class Plan:
         return lib().pacuda_b200_plan_flops(self.handle)
 
     @property
-    def points_per_warp(self):
-        return lib().pacuda_b200_plan_points_per_warp(self.handle)
+    def lanes_per_point(self):
+        return lib().pacuda_b200_plan_lanes_per_point(self.handle)
 
-    @points_per_warp.setter
-    def points_per_warp(self, p):
-        if lib().pacuda_b200_plan_set_points_per_warp(self.handle, p) != 0:
-            raise RunnerError(f"{p} points per warp do not fit")
+    @lanes_per_point.setter
+    def lanes_per_point(self, n):
+        if lib().pacuda_b200_plan_set_lanes_per_point(self.handle, n) != 0:
+            raise RunnerError(f"{n} lanes per point do not fit")
 
     def __del__(self):
         if getattr(self, "handle", None) and _lib is not None:

@@ -47,7 +47,8 @@ struct pacuda_b200_plan {
     double *coefficients = nullptr;
     uint32_t *red_offsets = nullptr, *red_slots = nullptr;
     double *red_weights = nullptr;
-    uint32_t log_p = 0;
+    uint32_t log_lanes = 5;   // lanes per point, as an exponent
+    size_t point_bytes = 0;
     bool fixed = false;
 };
 
@@ -61,8 +62,8 @@ struct pacuda_b200_batch {
     // descriptor block: TiledPlan[n] | item_first[n + 1] | external[n] | output[n] | count[n] | counter
     unsigned char *host = nullptr, *device = nullptr;
     size_t bytes = 0;
-    int warps = 0, sms = 0;
-    size_t warp_bytes = 0;
+    int threads = 0, sms = 0;
+    size_t smem = 0;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
 };
@@ -71,7 +72,7 @@ namespace {
 
 void fill_plan(const pacuda_b200_plan *p, TiledPlan &d) {
     memset(&d, 0, sizeof d);
-    describe(p->tiled, p->forms, p->log_p, tiled_warp_bytes(p->tiled.host, p->forms, p->kernel, p->log_p), d);
+    describe(p->tiled, p->forms, p->log_lanes, p->point_bytes, d);
     d.s64 = p->consts;
     d.f64 = p->consts + 2 * p->scales;
     d.kconst = p->consts + 2 * (p->scales + p->factors);
@@ -114,22 +115,26 @@ bool prepare(pacuda_b200_batch *b) {
     memset(b->host, 0, b->bytes);
     TiledPlan *plans = (TiledPlan *)(b->host + o.plans);
     unsigned long long *items = (unsigned long long *)(b->host + o.items);
-    b->warp_bytes = 0;
+    b->threads = tiled_threads(b->plans[0]->kernel);
+    size_t max_smem = tiled_max_smem(b->plans[0]->kernel);
+    b->smem = 0;
     items[0] = 0;
     for (size_t k = 0; k < n; k++) {
-        fill_plan(b->plans[k], plans[k]);
-        b->warp_bytes = std::max<size_t>(b->warp_bytes, plans[k].warp_bytes);
-        uint32_t per = 1u << b->plans[k]->log_p;
+        pacuda_b200_plan *p = b->plans[k];
+        int lo = tiled_min_log_lanes(p->point_bytes, b->threads, max_smem);
+        if (lo < 0) {
+            fprintf(stderr, "%s: a plan's point does not fit a block's shared memory\n", kTag);
+            return false;
+        }
+        if ((int)p->log_lanes < lo || (1 << p->log_lanes) > b->threads) p->log_lanes = (uint32_t)lo;
+        fill_plan(p, plans[k]);
+        uint32_t per = (uint32_t)b->threads >> p->log_lanes;
+        b->smem = std::max<size_t>(b->smem, (size_t)per * p->point_bytes);
         items[k + 1] = items[k] + (b->count[k] + per - 1) / per;
     }
     memcpy(b->host + o.external, b->external.data(), n * 8);
     memcpy(b->host + o.output, b->output.data(), n * 8);
     memcpy(b->host + o.count, b->count.data(), n * 4);
-    b->warps = std::min(16, tiled_warps(b->plans[0]->kernel, b->warp_bytes));
-    if (b->warps <= 0) {
-        fprintf(stderr, "%s: a plan's points do not fit one warp's shared memory\n", kTag);
-        return false;
-    }
     return true;
 }
 
@@ -152,20 +157,16 @@ TiledLaunch launch_args(const pacuda_b200_batch *b) {
 int launch(pacuda_b200_batch *b, cudaStream_t s) {
     if (failed(cudaMemcpyAsync(b->device, b->host, b->bytes, cudaMemcpyHostToDevice, s), "descriptors"))
         return PACMAN_RECURRENCE_DEVICE_ERROR;
-    if (!launch_tiled(b->plans[0]->kernel, launch_args(b), b->warps, b->warp_bytes, b->sms, s) ||
+    if (!launch_tiled(b->plans[0]->kernel, launch_args(b), b->threads, b->smem, b->sms, s) ||
         failed(cudaGetLastError(), "launch"))
         return PACMAN_RECURRENCE_DEVICE_ERROR;
     return PACMAN_RECURRENCE_OK;
 }
 
-// the largest points-per-warp whose warps still fill a block of 8, else 1
-uint32_t default_log_p(const pacuda_b200_plan *p) {
-    uint32_t best = 0;
-    for (uint32_t lp = 0; lp <= 5; lp++) {
-        int w = tiled_warps(p->kernel, tiled_warp_bytes(p->tiled.host, p->forms, p->kernel, lp));
-        if (w >= 8) best = lp;
-    }
-    return best;
+// the fewest lanes per point whose block of points fits shared memory
+uint32_t default_log_lanes(const pacuda_b200_plan *p) {
+    int lo = tiled_min_log_lanes(p->point_bytes, tiled_threads(p->kernel), tiled_max_smem(p->kernel));
+    return lo < 0 ? 5u : (uint32_t)lo;
 }
 
 }  // namespace
@@ -251,7 +252,8 @@ extern "C" pacuda_b200_plan *pacuda_b200_plan_create(const pacman_recurrence_cal
         pacuda_b200_plan_destroy(p);
         return nullptr;
     }
-    p->log_p = default_log_p(p);
+    p->point_bytes = tiled_point_bytes(p->tiled.host, forms, p->kernel);
+    p->log_lanes = default_log_lanes(p);
     return p;
 }
 
@@ -269,23 +271,24 @@ extern "C" void pacuda_b200_plan_destroy(pacuda_b200_plan *p) {
 
 extern "C" uint64_t pacuda_b200_plan_flops(const pacuda_b200_plan *p) { return p ? p->prog.flops : 0; }
 
-extern "C" int pacuda_b200_plan_set_points_per_warp(pacuda_b200_plan *p, uint32_t per) {
-    if (!p || per > 32 || (per & (per - 1))) return PACMAN_RECURRENCE_INVALID;
-    if (per == 0) {
+extern "C" int pacuda_b200_plan_set_lanes_per_point(pacuda_b200_plan *p, uint32_t lanes) {
+    if (!p || lanes > 512 || (lanes & (lanes - 1))) return PACMAN_RECURRENCE_INVALID;
+    if (lanes == 0) {
         p->fixed = false;
-        p->log_p = default_log_p(p);
+        p->log_lanes = default_log_lanes(p);
         return PACMAN_RECURRENCE_OK;
     }
-    uint32_t lp = 0;
-    while ((1u << lp) < per) lp++;
-    if (tiled_warps(p->kernel, tiled_warp_bytes(p->tiled.host, p->forms, p->kernel, lp)) <= 0)
+    uint32_t lg = 0;
+    while ((1u << lg) < lanes) lg++;
+    int lo = tiled_min_log_lanes(p->point_bytes, tiled_threads(p->kernel), tiled_max_smem(p->kernel));
+    if (lo < 0 || (int)lg < lo || (1 << lg) > tiled_threads(p->kernel) || (lg > 5 && (tiled_threads(p->kernel) >> lg) > 15))
         return PACMAN_RECURRENCE_INVALID;
-    p->log_p = lp;
+    p->log_lanes = lg;
     p->fixed = true;
     return PACMAN_RECURRENCE_OK;
 }
 
-extern "C" uint32_t pacuda_b200_plan_points_per_warp(const pacuda_b200_plan *p) { return p ? 1u << p->log_p : 0; }
+extern "C" uint32_t pacuda_b200_plan_lanes_per_point(const pacuda_b200_plan *p) { return p ? 1u << p->log_lanes : 0; }
 
 extern "C" pacuda_b200_batch *pacuda_b200_batch_create(pacuda_b200_plan *const *plans, uint32_t nplans,
                                                        const double *const *external, const uint32_t *count,
@@ -320,19 +323,31 @@ extern "C" int pacuda_b200_batch_run(pacuda_b200_batch *b, void *stream) {
 extern "C" int pacuda_b200_batch_capture(pacuda_b200_batch *b, void *stream) {
     if (!b) return PACMAN_RECURRENCE_INVALID;
     cudaStream_t s = (cudaStream_t)stream;
+    // the legacy default stream cannot be captured: capture on a stream of the batch's own (the
+    // graph is launched later on whatever stream a run names)
+    cudaStream_t own = nullptr;
+    if (s == nullptr || s == cudaStreamLegacy) {
+        if (failed(cudaStreamCreateWithFlags(&own, cudaStreamNonBlocking), "capture stream")) return PACMAN_RECURRENCE_DEVICE_ERROR;
+        s = own;
+    }
+    int status = PACMAN_RECURRENCE_OK;
     if (b->exec) {
         cudaGraphExecDestroy(b->exec);
         cudaGraphDestroy(b->graph);
         b->exec = nullptr;
         b->graph = nullptr;
     }
-    if (failed(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "capture")) return PACMAN_RECURRENCE_DEVICE_ERROR;
-    int st = launch(b, s);
-    cudaError_t e = cudaStreamEndCapture(s, &b->graph);
-    if (st != PACMAN_RECURRENCE_OK || failed(e, "capture") ||
-        failed(cudaGraphInstantiate(&b->exec, b->graph, 0), "graph instantiation"))
-        return PACMAN_RECURRENCE_DEVICE_ERROR;
-    return PACMAN_RECURRENCE_OK;
+    if (failed(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "capture")) {
+        status = PACMAN_RECURRENCE_DEVICE_ERROR;
+    } else {
+        int st = launch(b, s);
+        cudaError_t e = cudaStreamEndCapture(s, &b->graph);
+        if (st != PACMAN_RECURRENCE_OK || failed(e, "capture") ||
+            failed(cudaGraphInstantiate(&b->exec, b->graph, 0), "graph instantiation"))
+            status = PACMAN_RECURRENCE_DEVICE_ERROR;
+    }
+    if (own) cudaStreamDestroy(own);
+    return status;
 }
 
 extern "C" int pacuda_b200_batch_tune(pacuda_b200_batch *b, void *stream) {
@@ -349,15 +364,13 @@ extern "C" int pacuda_b200_batch_tune(pacuda_b200_batch *b, void *stream) {
         const double *ext[1] = {b->external[k]};
         double *out[1] = {b->output[k]};
         float best = 1e30f;
-        uint32_t best_lp = p->log_p;
-        for (uint32_t lp = 0; lp <= 5; lp++) {
-            if (tiled_warps(p->kernel, tiled_warp_bytes(p->tiled.host, p->forms, p->kernel, lp)) < 2) continue;
-            p->log_p = lp;
-            // the external momenta of the first `sample` points: a plane stride of count[k]
-            // would differ, so the sample is all points when they are few, else the timing
-            // runs on the whole plan
+        uint32_t best_lg = p->log_lanes;
+        int threads = tiled_threads(p->kernel);
+        int lo = tiled_min_log_lanes(p->point_bytes, threads, tiled_max_smem(p->kernel));
+        for (int lg = lo; lo >= 0 && (1 << lg) <= threads; lg++) {
+            if (lg > 5 && (threads >> lg) > 15) continue;
+            p->log_lanes = (uint32_t)lg;
             uint32_t n = b->count[k];
-            (void)sample;
             pacuda_b200_batch *tb = pacuda_b200_batch_create(one, 1, ext, &n, out);
             if (!tb) continue;
             float ms = 0;
@@ -374,10 +387,11 @@ extern "C" int pacuda_b200_batch_tune(pacuda_b200_batch *b, void *stream) {
             pacuda_b200_batch_destroy(tb);
             if (ok && ms < best) {
                 best = ms;
-                best_lp = lp;
+                best_lg = (uint32_t)lg;
             }
         }
-        p->log_p = best_lp;
+        p->log_lanes = best_lg;
+        (void)sample;
     }
     cudaEventDestroy(t0);
     cudaEventDestroy(t1);

@@ -195,7 +195,7 @@ struct Options {
     int block = 0;             // 0: the runner's choice
     bool sort = true;
     int executor = PACUDA_B200_EXECUTOR_AUTO;
-    uint32_t points_per_warp = 0;
+    uint32_t lanes_per_point = 0;
 };
 
 struct Device {
@@ -376,27 +376,18 @@ int onchip_launch(DeviceProgram *prog, const pacman_recurrence_call *c, const Ru
             upload_schedule(prog->tiled, dev.stream))
             prog->tiled_state = 1;
     }
-    // the points per warp: as configured, else the largest that still fills a block of 8 warps
-    uint32_t log_p = 0;
-    int warps = 0;
-    if (prog->tiled_state == 1) {
-        if (current.points_per_warp) {
-            while ((1u << log_p) < current.points_per_warp) log_p++;
-            warps = tiled_warps(kernel, tiled_warp_bytes(prog->tiled.host, forms, kernel, log_p));
-        } else {
-            for (uint32_t lp = 0; lp <= 5; lp++) {
-                int w = tiled_warps(kernel, tiled_warp_bytes(prog->tiled.host, forms, kernel, lp));
-                if (lp == 0 || w >= 8) {
-                    if (w <= 0) break;
-                    log_p = lp;
-                    warps = w;
-                }
-            }
-        }
+    // the lanes per point: as configured, else the fewest whose block of points fits
+    int threads = prog->tiled_state == 1 ? tiled_threads(kernel) : 0;
+    size_t pb = prog->tiled_state == 1 ? tiled_point_bytes(prog->tiled.host, forms, kernel) : 0;
+    int lo = threads ? tiled_min_log_lanes(pb, threads, tiled_max_smem(kernel)) : -1;
+    int log_l = lo;
+    if (lo >= 0 && current.lanes_per_point) {
+        int want = 0;
+        while ((1u << want) < current.lanes_per_point) want++;
+        log_l = (want >= lo && (1 << want) <= threads && !(want > 5 && (threads >> want) > 15)) ? want : -1;
     }
-    if (warps <= 0) return current.executor == PACUDA_B200_EXECUTOR_ONCHIP ? 2 : 0;
-    warps = std::min(warps, 16);
-    size_t wb = tiled_warp_bytes(prog->tiled.host, forms, kernel, log_p);
+    if (log_l < 0) return current.executor == PACUDA_B200_EXECUTOR_ONCHIP ? 2 : 0;
+    size_t smem = (size_t)(threads >> log_l) * pb;
     // descriptors: TiledPlan | item_first[2] | external[1] | count[1] | counter
     const size_t o_items = (sizeof(TiledPlan) + 15) / 16 * 16, o_ext = o_items + 16, o_count = o_ext + 8,
                  o_counter = (o_count + 4 + 15) / 16 * 16, total = o_counter + 16;
@@ -404,7 +395,7 @@ int onchip_launch(DeviceProgram *prog, const pacman_recurrence_call *c, const Ru
     if (!dev.launch_dev.reserve(total, "descriptors")) return -1;
     memset(dev.launch_host, 0, total);
     TiledPlan &p = *(TiledPlan *)dev.launch_host;
-    describe(prog->tiled, forms, log_p, wb, p);
+    describe(prog->tiled, forms, (uint32_t)log_l, pb, p);
     p.s64 = a.s64;
     p.f64 = a.f64;
     p.kconst = a.kconst;
@@ -415,7 +406,8 @@ int onchip_launch(DeviceProgram *prog, const pacman_recurrence_call *c, const Ru
     p.coefficients = a.coefficients;
     unsigned long long *items = (unsigned long long *)(dev.launch_host + o_items);
     items[0] = 0;
-    items[1] = (a.points + (1u << log_p) - 1) >> log_p;
+    uint32_t per = (uint32_t)threads >> log_l;
+    items[1] = (a.points + per - 1) / per;
     *(const double **)(dev.launch_host + o_ext) = a.external;
     *(uint32_t *)(dev.launch_host + o_count) = a.points;
     if (failed(cudaMemcpyAsync(dev.launch_dev.p, dev.launch_host, total, cudaMemcpyHostToDevice, dev.stream),
@@ -437,7 +429,7 @@ int onchip_launch(DeviceProgram *prog, const pacman_recurrence_call *c, const Ru
     L.aim = a.aim;
     L.mom = forms_on_device ? nullptr : a.mom;
     L.ld = a.ld;
-    if (!launch_tiled(kernel, L, warps, wb, dev.sms, dev.stream) || failed(cudaGetLastError(), "launch")) return -1;
+    if (!launch_tiled(kernel, L, threads, smem, dev.sms, dev.stream) || failed(cudaGetLastError(), "launch")) return -1;
     // the host descriptors are read by the copy: wait for it before a later call rewrites them
     return failed(cudaStreamSynchronize(dev.stream), "descriptors") ? -1 : 1;
 }
@@ -858,16 +850,16 @@ extern "C" int pacman_recurrence_v1_configure(const pacman_recurrence_options *o
     n.sort = !o->no_sort;
     if (o->struct_size >= sizeof(pacuda_b200_options)) {
         const pacuda_b200_options *x = (const pacuda_b200_options *)o;
-        if (x->executor > PACUDA_B200_EXECUTOR_ONCHIP || x->points_per_warp > 32 ||
-            (x->points_per_warp & (x->points_per_warp - 1))) {
+        if (x->executor > PACUDA_B200_EXECUTOR_ONCHIP || x->lanes_per_point > 512 ||
+            (x->lanes_per_point & (x->lanes_per_point - 1))) {
             release();
             return PACMAN_RECURRENCE_INVALID;
         }
         n.executor = (int)x->executor;
-        n.points_per_warp = x->points_per_warp;
+        n.lanes_per_point = x->lanes_per_point;
     }
     bool same = n.kernel == current.kernel && n.block == current.block && n.sort == current.sort &&
-                n.executor == current.executor && n.points_per_warp == current.points_per_warp;
+                n.executor == current.executor && n.lanes_per_point == current.lanes_per_point;
     if (runs_started && !same) {
         fprintf(stderr, "%s: another configuration after the first run\n", kTag);
         status = PACMAN_RECURRENCE_INVALID;

@@ -104,8 +104,26 @@ bool build_schedule(const Program &p, uint32_t P, uint32_t A, Schedule &out) {
     const uint32_t G = (uint32_t)gbase.size();
 
     // ---- tasks ----
+    // The sources run first, from the f64 forms, at level 0 (the kernel turns the forms into the
+    // kind's layout after them). Sources that write overlapping planes form one task, so that
+    // they keep their order; others are one task each.
     std::vector<Task> tasks;
+    bool sources_overlap = false;
+    {
+        std::vector<uint8_t> hit(P, 0);
+        for (uint32_t s = 0; s < p.sources && !sources_overlap; s++)
+            for (int k = 0; k < source_components(in[s].y); k++) {
+                if (hit[in[s].a + k]) sources_overlap = true;
+                hit[in[s].a + k] = 1;
+            }
+    }
     size_t n = 0;
+    if (sources_overlap && p.sources) {
+        Task t;
+        t.source = true;
+        for (; n < p.sources; n++) t.ins.push_back(in[n]);
+        tasks.push_back(t);
+    }
     while (n < in.size()) {
         const Ins &i = in[n];
         Task t;
@@ -158,13 +176,14 @@ bool build_schedule(const Program &p, uint32_t P, uint32_t A, Schedule &out) {
     for (Task &t : tasks) {
         std::vector<Range> r, w;
         for (const Ins &i : t.ins) access(i, r, w);
-        int lvl = t.source ? 0 : 1;
+        int lvl = t.source ? 0 : 1;  // sources: 0 (their overlaps are inside one task)
         for (const Range &x : r)
             for (uint32_t k = 0; k < x.count; k++) lvl = std::max(lvl, lw[x.first + k] + 1);
         for (const Range &x : w)
             for (uint32_t k = 0; k < x.count; k++)
                 lvl = std::max(lvl, std::max(lw[x.first + k], lr[x.first + k]) + 1);
         if (t.amplitude != ~0u) lvl = std::max(lvl, std::max(alw[t.amplitude], alr[t.amplitude]) + 1);
+        if (t.source) lvl = 0;
         t.level = lvl;
         for (const Range &x : r)
             for (uint32_t k = 0; k < x.count; k++) lr[x.first + k] = std::max(lr[x.first + k], lvl);

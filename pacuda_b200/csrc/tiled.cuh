@@ -1,11 +1,13 @@
-// The on-chip executor: a persistent kernel whose warps take groups of points; each point's
-// currents, amplitudes and forms live in shared-memory slots (schedule.h), the lanes of a point
-// run the tasks of one dataflow level at a time, and nothing but the external momenta comes in
-// and the outputs go out (in the C ABI's mode also the arena's live-in planes in and its written
+// The on-chip executor: a persistent kernel whose blocks take groups of points; each point's
+// currents, amplitudes and forms live in shared-memory slots (schedule.h), a point's lanes run
+// the tasks of one dataflow level at a time, and nothing but the external momenta comes in and
+// the outputs go out (in the C ABI's mode also the arena's live-in planes in and its written
 // planes out).
 //
-// A warp holds P points (P a power of two) and gives each L = 32 / P lanes. Shared memory per
-// warp: [slot][P] currents (re, im), [amplitude slot][P] amplitudes, [form * 4 + k][P] forms.
+// A point has L lanes (a power of two, 1 .. the block's threads). With L <= 32 a warp holds
+// 32 / L points, interleaved in its shared memory as [slot][point]; with L > 32 a point spans
+// L / 32 warps that meet at a named barrier. A block takes one work item at a time: one plan's
+// next (threads / L) points.
 #pragma once
 #include <stdint.h>
 
@@ -22,8 +24,8 @@ struct TiledPlan {
     const uint32_t *level_first;
     uint32_t levels;
     uint32_t cur_slots, amp_slots, forms;
-    uint32_t log_p;               // P = 1 << log_p points per warp
-    uint32_t warp_bytes;          // shared memory of one warp
+    uint32_t log_lanes;           // L = 1 << log_lanes lanes per point
+    uint32_t point_bytes;         // shared memory of one point
     // constants: f64 (sources), the kind's layout (rows)
     const double *s64, *f64;
     const void *kconst;
@@ -45,7 +47,7 @@ struct TiledPlan {
 struct TiledLaunch {
     const TiledPlan *plans;
     uint32_t nplans;
-    const unsigned long long *item_first;  // nplans + 1 prefix sums of work items (point groups)
+    const unsigned long long *item_first;  // nplans + 1 prefix sums of work items (a block's points)
     const double *const *external;         // per plan: source-major planes [(leg * 4 + k) * count + i]
     const uint32_t *count;                 // per plan: its points
     double *const *output;                 // per plan: [point][outputs] (batch mode)
@@ -66,11 +68,11 @@ template <class K> struct SlotView {
     Amp *are, *aim;
     const Den *mom;
     const Const *sre, *sim, *fre, *fim;
-    uint32_t log_p, pw;
+    uint32_t log_pw, pw;  // points interleaved in the region (1 << log_pw) and this lane's
     // write-back to the global arena (the C ABI's mode), else null
     R *gre, *gim;
     size_t ld, point;
-    __device__ __forceinline__ uint32_t at(uint32_t slot) const { return (slot << log_p) + pw; }
+    __device__ __forceinline__ uint32_t at(uint32_t slot) const { return (slot << log_pw) + pw; }
     __device__ __forceinline__ Cx<R> cur(uint32_t slot) const { return cx(cre[at(slot)], cim[at(slot)]); }
     __device__ __forceinline__ void put(uint32_t slot, Cx<R> v) const {
         cre[at(slot)] = v.re;
@@ -99,6 +101,16 @@ template <class K> struct SlotView {
 __device__ __forceinline__ double to_f64_value(double x) { return x; }
 __device__ __forceinline__ double to_f64_value(D x) { return __dadd_rn((double)x.hi, (double)x.lo); }
 
+// a point's lanes meet: within a warp, or at a named barrier of the point's warps
+__device__ __forceinline__ void point_sync(uint32_t log_lanes) {
+    if (log_lanes <= 5) {
+        __syncwarp();
+    } else {
+        uint32_t id = 1 + (threadIdx.x >> log_lanes), n = 1u << log_lanes;
+        asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory");
+    }
+}
+
 template <class K>
 __global__ void __launch_bounds__(512, 1) run_tiled(TiledLaunch L) {
     typedef typename K::R R;
@@ -106,37 +118,41 @@ __global__ void __launch_bounds__(512, 1) run_tiled(TiledLaunch L) {
     typedef typename K::Amp Amp;
     typedef typename K::Const Const;
     extern __shared__ __align__(16) unsigned char smem[];
-    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    uint32_t max_bytes = 0;
-    for (uint32_t k = 0; k < L.nplans; k++) max_bytes = max(max_bytes, L.plans[k].warp_bytes);
-    unsigned char *base = smem + (size_t)warp * max_bytes;
+    __shared__ unsigned long long next_item;
     const unsigned long long total = L.item_first[L.nplans];
     while (true) {
-        unsigned long long item = 0;
-        if (lane == 0) item = atomicAdd(L.counter, 1ull);
-        item = __shfl_sync(0xffffffffu, item, 0);
+        if (threadIdx.x == 0) next_item = atomicAdd(L.counter, 1ull);
+        __syncthreads();
+        const unsigned long long item = next_item;
+        __syncthreads();  // every thread has the item before the next one replaces it
         if (item >= total) break;
         uint32_t k = 0;
         while (item >= L.item_first[k + 1]) k++;
         const TiledPlan &p = L.plans[k];
-        const uint32_t log_p = p.log_p, lanes = 32u >> log_p;
-        const uint32_t pw = lane / lanes, tl = lane % lanes;
+        const uint32_t log_l = p.log_lanes, lanes = 1u << log_l;
+        const uint32_t log_pw = log_l < 5 ? 5 - log_l : 0;  // points per region
+        const uint32_t tl = threadIdx.x & (lanes - 1);
+        const uint32_t pw = log_l < 5 ? (threadIdx.x & 31) >> log_l : 0;
+        // the region: one warp's points (L <= 32) or one point's warps (L > 32)
+        const uint32_t region = log_l < 5 ? threadIdx.x >> 5 : threadIdx.x >> log_l;
+        unsigned char *base = smem + (size_t)region * ((size_t)p.point_bytes << log_pw);
         const uint32_t count = L.count[k];
-        const size_t first = (size_t)(item - L.item_first[k]) << log_p;
-        const bool valid = first + pw < count;
-        const size_t point = valid ? first + pw : count - 1;  // padding lanes redo the last point, unwritten
+        const size_t first = (size_t)(item - L.item_first[k]) * (blockDim.x >> log_l);
+        const size_t mine = first + (threadIdx.x >> log_l);
+        const bool valid = mine < count;
+        const size_t point = valid ? mine : count - 1;  // padding lanes redo the last point, unwritten
         SlotView<K> v;
         v.cre = (R *)base;
-        v.cim = v.cre + ((size_t)p.cur_slots << log_p);
-        v.are = (Amp *)(v.cim + ((size_t)p.cur_slots << log_p));
-        v.aim = v.are + ((size_t)p.amp_slots << log_p);
-        double *forms64 = (double *)(v.aim + ((size_t)p.amp_slots << log_p));
+        v.cim = v.cre + ((size_t)p.cur_slots << log_pw);
+        v.are = (Amp *)(v.cim + ((size_t)p.cur_slots << log_pw));
+        v.aim = v.are + ((size_t)p.amp_slots << log_pw);
+        double *forms64 = (double *)(v.aim + ((size_t)p.amp_slots << log_pw));
         v.mom = (const Den *)forms64;
         v.sre = (const Const *)p.kconst;
         v.sim = v.sre + p.scales;
         v.fre = v.sim + p.scales;
         v.fim = v.fre + p.factors;
-        v.log_p = log_p;
+        v.log_pw = log_pw;
         v.pw = pw;
         v.gre = (L.abi && valid) ? (R *)L.cre : nullptr;
         v.gim = (R *)L.cim;
@@ -159,29 +175,29 @@ __global__ void __launch_bounds__(512, 1) run_tiled(TiledLaunch L) {
                     val = t == 0 ? __dadd_rn(0.0, term) : __dadd_rn(val, term);
                 }
             }
-            forms64[(q << log_p) + pw] = val;
+            forms64[(q << log_pw) + pw] = val;
         }
         // the C ABI's mode: live-in currents and every amplitude from the global arena
         if (L.abi) {
             for (uint32_t j = 0; j < p.nloads; j++) {
                 uint32_t plane = __ldg(p.loads + 3 * j), slot = __ldg(p.loads + 3 * j + 1), n = __ldg(p.loads + 3 * j + 2);
                 for (uint32_t c = tl; c < n; c += lanes) {
-                    v.cre[((slot + c) << log_p) + pw] = ((const R *)L.cre)[(plane + c) * L.ld + point];
-                    v.cim[((slot + c) << log_p) + pw] = ((const R *)L.cim)[(plane + c) * L.ld + point];
+                    v.cre[((slot + c) << log_pw) + pw] = ((const R *)L.cre)[(plane + c) * L.ld + point];
+                    v.cim[((slot + c) << log_pw) + pw] = ((const R *)L.cim)[(plane + c) * L.ld + point];
                 }
             }
             for (uint32_t a = tl; a < p.amp_slots; a += lanes) {
                 uint32_t plane = __ldg(p.amp_planes + a);
-                v.are[(a << log_p) + pw] = ((const Amp *)L.are)[plane * L.ld + point];
-                v.aim[(a << log_p) + pw] = ((const Amp *)L.aim)[plane * L.ld + point];
+                v.are[(a << log_pw) + pw] = ((const Amp *)L.are)[plane * L.ld + point];
+                v.aim[(a << log_pw) + pw] = ((const Amp *)L.aim)[plane * L.ld + point];
             }
         } else {
             for (uint32_t a = tl; a < p.amp_slots; a += lanes) {
-                v.are[(a << log_p) + pw] = konst<Amp>(0.0);
-                v.aim[(a << log_p) + pw] = konst<Amp>(0.0);
+                v.are[(a << log_pw) + pw] = konst<Amp>(0.0);
+                v.aim[(a << log_pw) + pw] = konst<Amp>(0.0);
             }
         }
-        __syncwarp();
+        point_sync(log_l);
         for (uint32_t lv = 0; lv < p.levels; lv++) {
             uint32_t t0 = __ldg(p.level_first + lv), t1 = __ldg(p.level_first + lv + 1);
             for (uint32_t t = t0 + tl; t < t1; t += lanes) {
@@ -191,7 +207,7 @@ __global__ void __launch_bounds__(512, 1) run_tiled(TiledLaunch L) {
                     for (uint32_t n = i0; n < i1; n++) {
                         Ins o = load_ins(p.ins, n);
                         double mom[4];
-                        for (int c = 0; c < 4; c++) mom[c] = forms64[((o.f * 4 + c) << log_p) + pw];
+                        for (int c = 0; c < 4; c++) mom[c] = forms64[((o.f * 4 + c) << log_pw) + pw];
                         double fr = __ldg(p.f64 + o.x), fi = __ldg(p.f64 + p.factors + o.x), mass = __ldg(p.s64 + o.s);
                         W w[4];
                         int m = source_values(o.y, mass, mom, w);
@@ -210,22 +226,22 @@ __global__ void __launch_bounds__(512, 1) run_tiled(TiledLaunch L) {
                     for (uint32_t n = i0; n < i1; n++) exec_row<K>(v, load_ins(p.ins, n), acc);
                 }
             }
-            __syncwarp();
-            if (lv == 0 && sizeof(Den) == 8 && !is_f64<Den>::value) {
+            point_sync(log_l);
+            if (lv == 0 && !is_f64<Den>::value) {
                 // the forms into df64 pairs, in place
                 for (uint32_t q = tl; q < 4 * p.forms; q += lanes) {
-                    uint32_t at = (q << log_p) + pw;
+                    uint32_t at = (q << log_pw) + pw;
                     reinterpret_cast<D *>(forms64)[at] = narrow<D>(forms64[at]);
                 }
-                __syncwarp();
+                point_sync(log_l);
             }
         }
         if (L.abi) {
             if (valid)
                 for (uint32_t a = tl; a < p.amp_slots; a += lanes) {
                     uint32_t plane = __ldg(p.amp_planes + a);
-                    ((Amp *)L.are)[plane * L.ld + point] = v.are[(a << log_p) + pw];
-                    ((Amp *)L.aim)[plane * L.ld + point] = v.aim[(a << log_p) + pw];
+                    ((Amp *)L.are)[plane * L.ld + point] = v.are[(a << log_pw) + pw];
+                    ((Amp *)L.aim)[plane * L.ld + point] = v.aim[(a << log_pw) + pw];
                 }
         } else if (valid) {
             // the resolved reduction from zero: out[point][o] = 0 + w fma(re, re, im im) + ...
@@ -236,15 +252,15 @@ __global__ void __launch_bounds__(512, 1) run_tiled(TiledLaunch L) {
                     uint32_t s = __ldg(p.red_slots + j);
                     double re = 0.0, im = 0.0;
                     if (s != ~0u) {
-                        re = to_f64_value(v.are[(s << log_p) + pw]);
-                        im = to_f64_value(v.aim[(s << log_p) + pw]);
+                        re = to_f64_value(v.are[(s << log_pw) + pw]);
+                        im = to_f64_value(v.aim[(s << log_pw) + pw]);
                     }
                     acc = __dadd_rn(acc, __dmul_rn(__ldg(p.red_weights + j), __fma_rn(re, re, __dmul_rn(im, im))));
                 }
                 out[o] = acc;
             }
         }
-        __syncwarp();
+        __syncthreads();  // the block's shared memory is free for the next item
     }
 }
 

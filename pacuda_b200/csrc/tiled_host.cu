@@ -46,28 +46,47 @@ bool upload_schedule(TiledDevice &t, cudaStream_t s) {
     return t.ok;
 }
 
-size_t tiled_warp_bytes(const Schedule &s, uint32_t forms, int kernel, uint32_t log_p) {
+size_t tiled_point_bytes(const Schedule &s, uint32_t forms, int kernel) {
     size_t value = kernel == PACMAN_RECURRENCE_KERNEL_MIXED || kernel == PACMAN_RECURRENCE_KERNEL_MIXED64 ? 4 : 8;
     size_t per_point = 2 * value * s.cur_slots + 2 * 8 * s.amp_slots + 8 * 4 * (size_t)forms;
-    per_point = (per_point + 15) / 16 * 16;
-    return per_point << log_p;
+    return (per_point + 15) / 16 * 16;
 }
 
-int tiled_warps(int kernel, size_t warp_bytes) {
+int tiled_threads(int kernel) {
     cudaFuncAttributes attr;
     if (cudaFuncGetAttributes(&attr, kernel_for(kernel)) != cudaSuccess) return 0;
-    int dev = 0, smem = 0, regs = 0;
+    int dev = 0, regs = 0;
     cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     cudaDeviceGetAttribute(&regs, cudaDevAttrMaxRegistersPerBlock, dev);
-    int by_smem = warp_bytes ? (int)((size_t)(smem - attr.sharedSizeBytes) / warp_bytes) : 32;
-    int per_warp_regs = ((attr.numRegs * 32 + 255) / 256) * 256;
-    int by_regs = per_warp_regs ? regs / per_warp_regs : 32;
-    int by_threads = attr.maxThreadsPerBlock / 32;
-    return std::max(0, std::min({32, by_smem, by_regs, by_threads}));
+    int per_warp = ((attr.numRegs * 32 + 255) / 256) * 256;
+    int warps = per_warp ? regs / per_warp : 16;
+    warps = std::min(warps, attr.maxThreadsPerBlock / 32);
+    // a power of two of warps: points (and their barriers) tile the block evenly
+    int w = 1;
+    while (2 * w <= std::min(warps, 16)) w *= 2;
+    return 32 * w;
 }
 
-void describe(const TiledDevice &t, uint32_t forms, uint32_t log_p, size_t warp_bytes, TiledPlan &p) {
+size_t tiled_max_smem(int kernel) {
+    cudaFuncAttributes attr;
+    if (cudaFuncGetAttributes(&attr, kernel_for(kernel)) != cudaSuccess) return 0;
+    int dev = 0, smem = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    return (size_t)smem - attr.sharedSizeBytes;
+}
+
+int tiled_min_log_lanes(size_t point_bytes, int threads, size_t max_smem) {
+    for (int lg = 0; (1 << lg) <= threads; lg++) {
+        // lanes <= 32: a warp's 32 / L points; lanes > 32: one point per L / 32 warps (named
+        // barriers 1 .. 15, so at most 15 points of more than a warp per block)
+        if (lg > 5 && (threads >> lg) > 15) continue;
+        if ((size_t)(threads >> lg) * point_bytes <= max_smem) return lg;
+    }
+    return -1;
+}
+
+void describe(const TiledDevice &t, uint32_t forms, uint32_t log_lanes, size_t point_bytes, TiledPlan &p) {
     p.ins = t.ins;
     p.task_first = t.task_first;
     p.level_first = t.level_first;
@@ -75,19 +94,18 @@ void describe(const TiledDevice &t, uint32_t forms, uint32_t log_p, size_t warp_
     p.cur_slots = t.host.cur_slots;
     p.amp_slots = t.host.amp_slots;
     p.forms = forms;
-    p.log_p = log_p;
-    p.warp_bytes = (uint32_t)warp_bytes;
+    p.log_lanes = log_lanes;
+    p.point_bytes = (uint32_t)point_bytes;
     p.loads = t.loads;
     p.nloads = (uint32_t)t.host.loads.size() / 3;
     p.amp_planes = t.amp_planes;
 }
 
-bool launch_tiled(int kernel, const TiledLaunch &args, int warps, size_t warp_bytes, int sms, cudaStream_t stream) {
+bool launch_tiled(int kernel, const TiledLaunch &args, int threads, size_t smem, int sms, cudaStream_t stream) {
     const void *fn = kernel_for(kernel);
-    size_t smem = warp_bytes * (size_t)warps;
     if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return false;
     void *params[] = {(void *)&args};
-    return cudaLaunchKernel(fn, dim3(sms), dim3(32 * warps), params, smem, stream) == cudaSuccess;
+    return cudaLaunchKernel(fn, dim3(sms), dim3(threads), params, smem, stream) == cudaSuccess;
 }
 
 }  // namespace pacuda

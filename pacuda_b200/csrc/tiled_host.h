@@ -22,16 +22,20 @@ struct TiledDevice {
 // the schedule's arrays on the device
 bool upload_schedule(TiledDevice &t, cudaStream_t stream);
 
-// bytes of shared memory one warp needs for P = 1 << log_p points (kernel: PACMAN_RECURRENCE_KERNEL_*)
-size_t tiled_warp_bytes(const Schedule &s, uint32_t forms, int kernel, uint32_t log_p);
+// bytes of shared memory one point needs (kernel: PACMAN_RECURRENCE_KERNEL_*), 16-aligned
+size_t tiled_point_bytes(const Schedule &s, uint32_t forms, int kernel);
 
-// the warps per block the kernel can run with this much shared memory per warp (0: none fit)
-int tiled_warps(int kernel, size_t warp_bytes);
+// the block's threads (as the kernel's registers allow, at most 512) and its largest shared memory
+int tiled_threads(int kernel);
+size_t tiled_max_smem(int kernel);
+
+// the smallest lanes-per-point exponent whose block of points fits shared memory, or -1
+int tiled_min_log_lanes(size_t point_bytes, int threads, size_t max_smem);
 
 // fills the schedule fields of a plan descriptor
-void describe(const TiledDevice &t, uint32_t forms, uint32_t log_p, size_t warp_bytes, TiledPlan &p);
+void describe(const TiledDevice &t, uint32_t forms, uint32_t log_lanes, size_t point_bytes, TiledPlan &p);
 
-// launches the persistent kernel: `launch` points to device memory holding the TiledLaunch
-bool launch_tiled(int kernel, const TiledLaunch &args, int warps, size_t warp_bytes, int sms, cudaStream_t stream);
+// launches the persistent kernel (one block per SM) with `smem` bytes of shared memory
+bool launch_tiled(int kernel, const TiledLaunch &args, int threads, size_t smem, int sms, cudaStream_t stream);
 
 }  // namespace pacuda

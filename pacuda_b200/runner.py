@@ -42,8 +42,8 @@ class Runner:
         if kernel is not None:
             self.configure(kernel, block, no_sort, stats, executor)
 
-    def configure(self, kernel="f64", block=0, no_sort=False, stats=False, executor=None, points_per_warp=0):
-        o = abi.options(kernel, block, no_sort, stats, executor, points_per_warp)
+    def configure(self, kernel="f64", block=0, no_sort=False, stats=False, executor=None, lanes_per_point=0):
+        o = abi.options(kernel, block, no_sort, stats, executor, lanes_per_point)
         return self.lib.pacman_recurrence_v1_configure(C.addressof(o))
 
     def run(self, call_args):

@@ -1,0 +1,76 @@
+// Test harness (CPU): the product's plan compiler and scheduler (pacuda_b200/csrc/program.cpp,
+// schedule.cpp) driven from Python, for schedule statistics and for the CPU emulation of the
+// on-chip executor's schedule in tests/test_schedule.py.
+#include <stdint.h>
+#include <string.h>
+
+#include "../../pacuda_b200/csrc/program.h"
+#include "../../pacuda_b200/csrc/schedule.h"
+
+using namespace pacuda;
+
+extern "C" {
+
+// stats[0..7] = rows, tasks, levels, cur_slots, amp_slots, max_task_len, live-in groups, max tasks per level
+int schedule_stats(const uint64_t *words, uint32_t count, const uint8_t *width, uint32_t planes, uint32_t amps,
+                   uint32_t forms, uint32_t scales, uint32_t factors, uint32_t *stats) {
+    Program p;
+    Limits lim{planes, amps, forms, scales, factors};
+    BuildError e = build_program(words, count, width, true, lim, p);
+    if (e.status) return e.status;
+    Schedule s;
+    if (!build_schedule(p, planes, amps, s)) return -1;
+    stats[0] = (uint32_t)p.ins.size();
+    stats[1] = (uint32_t)s.task_first.size() - 1;
+    stats[2] = (uint32_t)s.level_first.size() - 1;
+    stats[3] = s.cur_slots;
+    stats[4] = s.amp_slots;
+    stats[5] = s.max_task_len;
+    stats[6] = (uint32_t)s.loads.size() / 3;
+    uint32_t mx = 0;
+    for (size_t l = 0; l + 1 < s.level_first.size(); l++) mx = std::max(mx, s.level_first[l + 1] - s.level_first[l]);
+    stats[7] = mx;
+    return 0;
+}
+
+// the program's instructions (reference order, after the sort): count, then 8 u32 each
+int program_export(const uint64_t *words, uint32_t count, const uint8_t *width, uint32_t planes, uint32_t amps,
+                   uint32_t forms, uint32_t scales, uint32_t factors, uint32_t *n, uint32_t *ins) {
+    Program p;
+    Limits lim{planes, amps, forms, scales, factors};
+    BuildError e = build_program(words, count, width, true, lim, p);
+    if (e.status) return e.status;
+    *n = (uint32_t)p.ins.size();
+    if (ins) memcpy(ins, p.ins.data(), p.ins.size() * sizeof(Ins));
+    return 0;
+}
+
+// the schedule's arrays (for the emulator): sizes first (ins, tasks + 1, levels + 1, loads, amp planes)
+int schedule_export(const uint64_t *words, uint32_t count, const uint8_t *width, uint32_t planes, uint32_t amps,
+                    uint32_t forms, uint32_t scales, uint32_t factors, uint32_t *sizes, uint32_t *ins,
+                    uint32_t *task_first, uint32_t *level_first, uint32_t *loads, uint32_t *amp_planes,
+                    uint32_t *slots) {
+    Program p;
+    Limits lim{planes, amps, forms, scales, factors};
+    BuildError e = build_program(words, count, width, true, lim, p);
+    if (e.status) return e.status;
+    Schedule s;
+    if (!build_schedule(p, planes, amps, s)) return -1;
+    sizes[0] = (uint32_t)s.ins.size();
+    sizes[1] = (uint32_t)s.task_first.size();
+    sizes[2] = (uint32_t)s.level_first.size();
+    sizes[3] = (uint32_t)s.loads.size();
+    sizes[4] = (uint32_t)s.amp_planes.size();
+    sizes[5] = s.cur_slots;
+    sizes[6] = p.sources;
+    if (ins) {
+        memcpy(ins, s.ins.data(), s.ins.size() * sizeof(Ins));
+        memcpy(task_first, s.task_first.data(), s.task_first.size() * 4);
+        memcpy(level_first, s.level_first.data(), s.level_first.size() * 4);
+        memcpy(loads, s.loads.data(), s.loads.size() * 4);
+        memcpy(amp_planes, s.amp_planes.data(), s.amp_planes.size() * 4);
+        (void)slots;
+    }
+    return 0;
+}
+}

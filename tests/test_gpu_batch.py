@@ -47,17 +47,18 @@ def test_batch_matches_oracle_bitwise(kind):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("per", [1, 2, 4, 8, 16, 32])
-def test_every_points_per_warp_gives_the_same_bits(per):
+@pytest.mark.parametrize("lanes", [32, 64, 128, 256, 512])
+def test_every_lanes_per_point_gives_the_same_bits(lanes):
+    """Points over several warps (named barriers) as well as within one."""
     from pacuda_b200 import batch as B
     import torch
 
     plans, ext, out, want = setup("f64", [70, 33, 129, 5])
     for p in plans:
         try:
-            p.points_per_warp = per
+            p.lanes_per_point = lanes
         except Exception:
-            pytest.skip(f"{per} points per warp do not fit")
+            pytest.skip(f"{lanes} lanes per point do not fit")
     b = B.Batch(plans, ext, out)
     b.run()
     torch.cuda.synchronize()
