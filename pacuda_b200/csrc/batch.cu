@@ -63,7 +63,7 @@ struct pacuda_b200_batch {
     unsigned char *host = nullptr, *device = nullptr;
     size_t bytes = 0;
     int threads = 0, sms = 0;
-    size_t smem = 0;
+    size_t smem = 0, const_bytes = 0;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
 };
@@ -116,7 +116,10 @@ bool prepare(pacuda_b200_batch *b) {
     TiledPlan *plans = (TiledPlan *)(b->host + o.plans);
     unsigned long long *items = (unsigned long long *)(b->host + o.items);
     b->threads = tiled_threads(b->plans[0]->kernel);
-    size_t max_smem = tiled_max_smem(b->plans[0]->kernel);
+    b->const_bytes = 0;
+    for (size_t k = 0; k < n; k++)
+        b->const_bytes = std::max(b->const_bytes, tiled_const_bytes(b->plans[k]->scales, b->plans[k]->factors));
+    size_t max_smem = tiled_max_smem(b->plans[0]->kernel) - b->const_bytes;
     b->smem = 0;
     items[0] = 0;
     for (size_t k = 0; k < n; k++) {
@@ -135,6 +138,7 @@ bool prepare(pacuda_b200_batch *b) {
     memcpy(b->host + o.external, b->external.data(), n * 8);
     memcpy(b->host + o.output, b->output.data(), n * 8);
     memcpy(b->host + o.count, b->count.data(), n * 4);
+    b->smem += b->const_bytes;
     return true;
 }
 
@@ -151,6 +155,7 @@ TiledLaunch launch_args(const pacuda_b200_batch *b) {
     L.count = (const uint32_t *)(b->device + o.count);
     L.counter = (unsigned long long *)(b->device + o.counter);
     L.abi = false;
+    L.const_bytes = (uint32_t)b->const_bytes;
     return L;
 }
 
@@ -165,7 +170,8 @@ int launch(pacuda_b200_batch *b, cudaStream_t s) {
 
 // the fewest lanes per point whose block of points fits shared memory
 uint32_t default_log_lanes(const pacuda_b200_plan *p) {
-    int lo = tiled_min_log_lanes(p->point_bytes, tiled_threads(p->kernel), tiled_max_smem(p->kernel));
+    int lo = tiled_min_log_lanes(p->point_bytes, tiled_threads(p->kernel),
+                                 tiled_max_smem(p->kernel) - tiled_const_bytes(p->scales, p->factors));
     return lo < 0 ? 5u : (uint32_t)lo;
 }
 
@@ -280,7 +286,8 @@ extern "C" int pacuda_b200_plan_set_lanes_per_point(pacuda_b200_plan *p, uint32_
     }
     uint32_t lg = 0;
     while ((1u << lg) < lanes) lg++;
-    int lo = tiled_min_log_lanes(p->point_bytes, tiled_threads(p->kernel), tiled_max_smem(p->kernel));
+    int lo = tiled_min_log_lanes(p->point_bytes, tiled_threads(p->kernel),
+                                 tiled_max_smem(p->kernel) - tiled_const_bytes(p->scales, p->factors));
     if (lo < 0 || (int)lg < lo || (1 << lg) > tiled_threads(p->kernel) || (lg > 5 && (tiled_threads(p->kernel) >> lg) > 15))
         return PACMAN_RECURRENCE_INVALID;
     p->log_lanes = lg;
@@ -366,7 +373,8 @@ extern "C" int pacuda_b200_batch_tune(pacuda_b200_batch *b, void *stream) {
         float best = 1e30f;
         uint32_t best_lg = p->log_lanes;
         int threads = tiled_threads(p->kernel);
-        int lo = tiled_min_log_lanes(p->point_bytes, threads, tiled_max_smem(p->kernel));
+        int lo = tiled_min_log_lanes(p->point_bytes, threads,
+                                     tiled_max_smem(p->kernel) - tiled_const_bytes(p->scales, p->factors));
         for (int lg = lo; lo >= 0 && (1 << lg) <= threads; lg++) {
             if (lg > 5 && (threads >> lg) > 15) continue;
             p->log_lanes = (uint32_t)lg;

@@ -92,8 +92,9 @@ __device__ __forceinline__ void exec_contribution(const V &v, const Ins &o, Cx<t
         else acc[k] = v.cur(o.c + k) + c;
     }
     if (flags & F_LAST) {
+        if (!(flags & 32))  // else the sums stay in registers for the task's closures
 #pragma unroll
-        for (int k = 0; k < cd; k++) v.put(o.c + k, acc[k]);
+            for (int k = 0; k < cd; k++) v.put(o.c + k, acc[k]);
         if (flags & 8) v.writeback(o.y, acc, cd);
     }
 }
@@ -122,16 +123,29 @@ __device__ __forceinline__ void exec_propagator(const V &v, const Ins &o) {
 }
 
 template <class K, class V>
-__device__ __forceinline__ void exec_closure(const V &v, const Ins &o) {
+__device__ __forceinline__ void exec_closure(const V &v, const Ins &o, const Cx<typename K::R> *acc) {
     typedef typename K::R R;
     typedef typename K::Amp Amp;
     Cx<R> f = v.factor(o.x);
     Amp dr, di;
     v.amp(o.c, dr, di);
-    for (uint32_t k = 0; k < o.s; k++) {
-        Cx<R> t = closure_term(v.cur(o.a + k), v.cur(o.b + k), cast<R>(v.fre[o.y + k]), cast<R>(v.fim[o.y + k]), f.re, f.im);
-        dr = dr + amp_of(t.re, (Amp *)nullptr);
-        di = di + amp_of(t.im, (Amp *)nullptr);
+    if (ins_flags(o) & 16) {
+        // parent 0 is the task's sums (at most 6 components): indices known at compile time keep
+        // the sums in registers
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+            if ((uint32_t)k >= o.s) break;
+            Cx<R> t = closure_term(acc[k], v.cur(o.b + k), cast<R>(v.fre[o.y + k]), cast<R>(v.fim[o.y + k]), f.re, f.im);
+            dr = dr + amp_of(t.re, (Amp *)nullptr);
+            di = di + amp_of(t.im, (Amp *)nullptr);
+        }
+    } else {
+        for (uint32_t k = 0; k < o.s; k++) {
+            Cx<R> t = closure_term(v.cur(o.a + k), v.cur(o.b + k), cast<R>(v.fre[o.y + k]), cast<R>(v.fim[o.y + k]), f.re,
+                                   f.im);
+            dr = dr + amp_of(t.re, (Amp *)nullptr);
+            di = di + amp_of(t.im, (Amp *)nullptr);
+        }
     }
     v.put_amp(o.c, dr, di);
 }
@@ -174,7 +188,7 @@ __device__ __forceinline__ void exec_row(const V &v, const Ins &o, Cx<typename K
         else if (op == 8) exec_propagator<K, 8>(v, o);
         else exec_propagator<K, 9>(v, o);
     } else if (kind == K_CLOSURE) {
-        exec_closure<K>(v, o);
+        exec_closure<K>(v, o, acc);
     } else if (kind == K_IDENTITY) {
         exec_identity<K>(v, o);
     } else if (kind == K_CLEAR) {

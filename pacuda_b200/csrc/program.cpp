@@ -154,6 +154,8 @@ uint32_t row_flops(const Ins &i) {
 
 }  // namespace
 
+uint32_t ins_flops(const Ins &i) { return row_flops(i); }
+
 BuildError build_program(const uint64_t *words, uint32_t count, const uint8_t *width, bool sort,
                          const Limits &lim, Program &out) {
     BuildError err;

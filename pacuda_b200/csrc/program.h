@@ -84,4 +84,7 @@ void sort_contribution_runs(std::vector<Row> &rows);
 
 void contribution_shape(int op, int *c0, int *c1, int *cd);
 
+// an instruction's algorithmic flops (fixed per-op counts)
+uint32_t ins_flops(const Ins &i);
+
 }  // namespace pacuda

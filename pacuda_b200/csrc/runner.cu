@@ -379,7 +379,8 @@ int onchip_launch(DeviceProgram *prog, const pacman_recurrence_call *c, const Ru
     // the lanes per point: as configured, else the fewest whose block of points fits
     int threads = prog->tiled_state == 1 ? tiled_threads(kernel) : 0;
     size_t pb = prog->tiled_state == 1 ? tiled_point_bytes(prog->tiled.host, forms, kernel) : 0;
-    int lo = threads ? tiled_min_log_lanes(pb, threads, tiled_max_smem(kernel)) : -1;
+    size_t cb = tiled_const_bytes(c->scale_count, c->factor_count);
+    int lo = threads ? tiled_min_log_lanes(pb, threads, tiled_max_smem(kernel) - cb) : -1;
     int log_l = lo;
     if (lo >= 0 && current.lanes_per_point) {
         int want = 0;
@@ -387,7 +388,7 @@ int onchip_launch(DeviceProgram *prog, const pacman_recurrence_call *c, const Ru
         log_l = (want >= lo && (1 << want) <= threads && !(want > 5 && (threads >> want) > 15)) ? want : -1;
     }
     if (log_l < 0) return current.executor == PACUDA_B200_EXECUTOR_ONCHIP ? 2 : 0;
-    size_t smem = (size_t)(threads >> log_l) * pb;
+    size_t smem = cb + (size_t)(threads >> log_l) * pb;
     // descriptors: TiledPlan | item_first[2] | external[1] | count[1] | counter
     const size_t o_items = (sizeof(TiledPlan) + 15) / 16 * 16, o_ext = o_items + 16, o_count = o_ext + 8,
                  o_counter = (o_count + 4 + 15) / 16 * 16, total = o_counter + 16;
@@ -429,6 +430,7 @@ int onchip_launch(DeviceProgram *prog, const pacman_recurrence_call *c, const Ru
     L.aim = a.aim;
     L.mom = forms_on_device ? nullptr : a.mom;
     L.ld = a.ld;
+    L.const_bytes = (uint32_t)cb;
     if (!launch_tiled(kernel, L, threads, smem, dev.sms, dev.stream) || failed(cudaGetLastError(), "launch")) return -1;
     // the host descriptors are read by the copy: wait for it before a later call rewrites them
     return failed(cudaStreamSynchronize(dev.stream), "descriptors") ? -1 : 1;

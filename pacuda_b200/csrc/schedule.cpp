@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <map>
 #include <numeric>
+#include <queue>
 
 namespace pacuda {
 namespace {
@@ -59,7 +60,8 @@ struct Task {
     std::vector<Ins> ins;
     int level = 0;
     bool source = false;
-    uint32_t amplitude = ~0u;  // closures: their amplitude plane
+    uint32_t amplitude = ~0u;           // closures: their amplitude plane
+    std::vector<uint32_t> amplitudes;   // closures fused into a current's task: their amplitudes
 };
 
 }  // namespace
@@ -170,6 +172,74 @@ bool build_schedule(const Program &p, uint32_t P, uint32_t A, Schedule &out) {
         tasks.push_back(t);
     }
 
+    // ---- closures fused into the task of their closing current ----
+    // A closing current read by nothing but closures, whose amplitudes receive no other closure,
+    // is computed, closed and forgotten by one task: the closures read its sums in registers and
+    // it needs no slot. (Its values still go to the global arena in the C ABI's mode.)
+    std::vector<uint8_t> in_register(G, 0);
+    {
+        std::vector<int> closure_tasks_of(A, 0);
+        for (const Task &t : tasks)
+            if (t.amplitude != ~0u) closure_tasks_of[t.amplitude]++;
+        // per group: its tasks that read or write it
+        std::vector<std::vector<uint32_t>> readers(G), writers(G);
+        for (uint32_t ti = 0; ti < tasks.size(); ti++) {
+            std::vector<Range> r, w;
+            for (const Ins &i : tasks[ti].ins) access(i, r, w);
+            for (const Range &x : r)
+                for (uint32_t k = 0; k < x.count; k++) {
+                    auto &v = readers[group_of[x.first + k]];
+                    if (v.empty() || v.back() != ti) v.push_back(ti);
+                }
+            for (const Range &x : w)
+                for (uint32_t k = 0; k < x.count; k++) {
+                    auto &v = writers[group_of[x.first + k]];
+                    if (v.empty() || v.back() != ti) v.push_back(ti);
+                }
+        }
+        std::vector<uint8_t> merged(tasks.size(), 0);
+        for (uint32_t g = 0; g < G; g++) {
+            if (writers[g].size() != 1 || readers[g].empty()) continue;
+            uint32_t pt = writers[g][0];
+            Task &prod = tasks[pt];
+            const Ins &last = prod.ins.back();
+            int c0, c1, cd;
+            if (ins_kind(last) != K_CONTRIB || !(ins_flags(last) & F_LAST)) continue;
+            contribution_shape(ins_op(last), &c0, &c1, &cd);
+            if (last.c != gbase[g] || (uint32_t)cd != gsize[g] || !(ins_flags(prod.ins.front()) & F_INIT)) continue;
+            bool ok = true;
+            for (const Ins &i : prod.ins) {  // every row of the run writes the same components
+                int a0, a1, ad;
+                contribution_shape(ins_op(i), &a0, &a1, &ad);
+                if (ins_kind(i) != K_CONTRIB || ad != cd) ok = false;
+            }
+            for (uint32_t rt : readers[g]) {
+                const Task &t = tasks[rt];
+                if (rt == pt || t.amplitude == ~0u || closure_tasks_of[t.amplitude] != 1 || rt < pt) ok = false;
+                for (const Ins &i : t.ins)
+                    if (ins_kind(i) != K_CLOSURE || i.a != gbase[g] || i.s > gsize[g] ||
+                        (i.b < gbase[g] + gsize[g] && i.b + i.s > gbase[g]))
+                        ok = false;
+            }
+            if (!ok) continue;
+            for (uint32_t rt : readers[g]) {
+                for (Ins i : tasks[rt].ins) {
+                    i.head |= F_ACC0 << 8;
+                    prod.ins.push_back(i);
+                }
+                prod.amplitudes.push_back(tasks[rt].amplitude);
+                merged[rt] = 1;
+            }
+            for (Ins &i : prod.ins)
+                if (ins_kind(i) == K_CONTRIB && (ins_flags(i) & F_LAST)) i.head |= F_NOSTORE << 8;
+            in_register[g] = 1;
+        }
+        std::vector<Task> kept;
+        for (uint32_t ti = 0; ti < tasks.size(); ti++)
+            if (!merged[ti]) kept.push_back(std::move(tasks[ti]));
+        tasks.swap(kept);
+    }
+
     // ---- levels ----
     std::vector<int> lw(P, -1), lr(P, -1), alw(A, -1), alr(A, -1);
     int levels = 1;
@@ -183,6 +253,7 @@ bool build_schedule(const Program &p, uint32_t P, uint32_t A, Schedule &out) {
             for (uint32_t k = 0; k < x.count; k++)
                 lvl = std::max(lvl, std::max(lw[x.first + k], lr[x.first + k]) + 1);
         if (t.amplitude != ~0u) lvl = std::max(lvl, std::max(alw[t.amplitude], alr[t.amplitude]) + 1);
+        for (uint32_t a : t.amplitudes) lvl = std::max(lvl, std::max(alw[a], alr[a]) + 1);
         if (t.source) lvl = 0;
         t.level = lvl;
         for (const Range &x : r)
@@ -193,6 +264,7 @@ bool build_schedule(const Program &p, uint32_t P, uint32_t A, Schedule &out) {
                 lr[x.first + k] = -1;
             }
         if (t.amplitude != ~0u) alw[t.amplitude] = lvl;
+        for (uint32_t a : t.amplitudes) alw[a] = lvl;
         levels = std::max(levels, lvl + 1);
     }
 
@@ -252,6 +324,7 @@ bool build_schedule(const Program &p, uint32_t P, uint32_t A, Schedule &out) {
         }
     };
     for (uint32_t g : order) {
+        if (in_register[g]) continue;  // kept in a task's registers
         // a slot is reused only after the last level that touches its previous occupant
         while (!active.empty() && active.begin()->first < gfirst[g]) {
             release(active.begin()->second.first, active.begin()->second.second);
@@ -274,7 +347,10 @@ bool build_schedule(const Program &p, uint32_t P, uint32_t A, Schedule &out) {
         active.emplace(glast[g], std::make_pair(slot, gsize[g]));
     }
     out.cur_slots = top;
-    auto slot_of = [&](uint32_t plane) { return gslot[group_of[plane]] + (plane - gbase[group_of[plane]]); };
+    auto slot_of = [&](uint32_t plane) {
+        uint32_t g = group_of[plane];
+        return in_register[g] ? 0u : gslot[g] + (plane - gbase[g]);
+    };
     for (uint32_t g = 0; g < G; g++)
         if (live_in[g]) {
             out.loads.push_back(gbase[g]);
@@ -284,10 +360,11 @@ bool build_schedule(const Program &p, uint32_t P, uint32_t A, Schedule &out) {
     // amplitude slots: one per amplitude a closure accumulates into, for the whole run
     out.amp_slot_of.assign(A, ~0u);
     for (const Task &t : tasks)
-        if (t.amplitude != ~0u && out.amp_slot_of[t.amplitude] == ~0u) {
-            out.amp_slot_of[t.amplitude] = (uint32_t)out.amp_planes.size();
-            out.amp_planes.push_back(t.amplitude);
-        }
+        for (const Ins &i : t.ins)
+            if (ins_kind(i) == K_CLOSURE && out.amp_slot_of[i.c] == ~0u) {
+                out.amp_slot_of[i.c] = (uint32_t)out.amp_planes.size();
+                out.amp_planes.push_back(i.c);
+            }
     out.amp_slots = (uint32_t)out.amp_planes.size();
 
     // ---- emit: levels in order; within a level the tasks sorted by their ops ----
@@ -324,8 +401,38 @@ bool build_schedule(const Program &p, uint32_t P, uint32_t A, Schedule &out) {
         }
         out.task_first.push_back((uint32_t)out.ins.size());
         out.max_task_len = std::max<uint32_t>(out.max_task_len, (uint32_t)tasks[t].ins.size());
+        uint32_t cost = 0;
+        for (const Ins &i : tasks[t].ins) cost += ins_flops(i) + 8;  // + its fetch and decode
+        out.task_cost.push_back(cost);
     }
     return true;
+}
+
+void lane_order(const Schedule &s, uint32_t log_lanes, std::vector<uint32_t> &order, std::vector<uint32_t> &level_first) {
+    const uint32_t L = 1u << log_lanes;
+    order.clear();
+    level_first.assign(1, 0);
+    for (size_t lv = 0; lv + 1 < s.level_first.size(); lv++) {
+        std::vector<uint32_t> ts;
+        for (uint32_t t = s.level_first[lv]; t < s.level_first[lv + 1]; t++) ts.push_back(t);
+        std::stable_sort(ts.begin(), ts.end(), [&](uint32_t x, uint32_t y) { return s.task_cost[x] > s.task_cost[y]; });
+        // longest first onto the least loaded lane (ties: the lowest lane)
+        std::vector<std::vector<uint32_t>> lane(L);
+        typedef std::pair<uint64_t, uint32_t> Load;
+        std::priority_queue<Load, std::vector<Load>, std::greater<Load>> heap;
+        for (uint32_t l = 0; l < L; l++) heap.push({0, l});
+        for (uint32_t t : ts) {
+            Load top = heap.top();
+            heap.pop();
+            lane[top.second].push_back(t);
+            heap.push({top.first + s.task_cost[t], top.second});
+        }
+        size_t rounds = 0;
+        for (auto &v : lane) rounds = std::max(rounds, v.size());
+        for (size_t r = 0; r < rounds; r++)
+            for (uint32_t l = 0; l < L; l++) order.push_back(r < lane[l].size() ? lane[l][r] : ~0u);
+        level_first.push_back((uint32_t)order.size());
+    }
 }
 
 }  // namespace pacuda

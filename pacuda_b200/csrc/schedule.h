@@ -17,7 +17,11 @@
 
 namespace pacuda {
 
-enum : uint32_t { F_WB = 8 };  // the instruction's written values also go to the global arena
+enum : uint32_t {
+    F_WB = 8,        // the instruction's written values also go to the global arena
+    F_ACC0 = 16,     // a closure whose parent 0 is the task's sums (its closing current, in registers)
+    F_NOSTORE = 32,  // a destination run's last row keeps its sums in registers (no slot)
+};
 
 struct Schedule {
     std::vector<Ins> ins;               // task instructions; operands are slots
@@ -29,8 +33,14 @@ struct Schedule {
     std::vector<uint32_t> amp_planes;   // per amplitude slot, its global amplitude plane
     std::vector<uint32_t> amp_slot_of;  // per global amplitude plane, its slot or ~0u
     uint32_t max_task_len = 0;
+    std::vector<uint32_t> task_cost;    // per task, its algorithmic flops
     std::string why;                    // empty when the schedule exists
 };
+
+// The order in which a point's L = 1 << log_lanes lanes take a level's tasks: position j of a
+// level goes to lane j % L, so each level is padded to whole rounds of L with ~0u (no task). The
+// tasks of a level are assigned longest first to the least loaded lane.
+void lane_order(const Schedule &s, uint32_t log_lanes, std::vector<uint32_t> &order, std::vector<uint32_t> &level_first);
 
 // builds the schedule of a program; `forms` is the plan's momentum form count
 bool build_schedule(const Program &p, uint32_t current_planes, uint32_t amplitude_planes, Schedule &out);

@@ -20,8 +20,9 @@ namespace pacuda {
 struct TiledPlan {
     // the schedule
     const Ins *ins;
-    const uint32_t *task_first;
-    const uint32_t *level_first;
+    const uint32_t *task_first;   // per task, its instructions (tasks + 1 entries)
+    const uint32_t *order;        // per level position, its task's (first, end) instructions; lane = position % L
+    const uint32_t *level_first;  // levels + 1 entries into order
     uint32_t levels;
     uint32_t cur_slots, amp_slots, forms;
     uint32_t log_lanes;           // L = 1 << log_lanes lanes per point
@@ -57,44 +58,58 @@ struct TiledLaunch {
     void *cre, *cim, *are, *aim;
     const double *mom;                     // uploaded forms (f64 planes), or null
     size_t ld;
+    uint32_t const_bytes;                  // shared memory kept for a plan's constants
 };
 
-template <class K> struct SlotView {
+// a complex value as shared memory holds it: (re, im) side by side, one 8- or 16-byte access
+template <class R> struct alignas(2 * sizeof(R)) Pair {
+    R re, im;
+};
+
+template <class K, bool ABI> struct SlotView {
     typedef typename K::R R;
     typedef typename K::Den Den;
     typedef typename K::Amp Amp;
     typedef typename K::Const Const;
-    R *cre, *cim;
-    Amp *are, *aim;
+    Pair<R> *cur_;        // [slot][points of the region]
+    Pair<Amp> *amp_;      // [amplitude slot][points of the region]
     const Den *mom;
-    const Const *sre, *sim, *fre, *fim;
+    const Const *sre, *sim, *fre, *fim;  // the plan's constants, in shared memory
     uint32_t log_pw, pw;  // points interleaved in the region (1 << log_pw) and this lane's
     // write-back to the global arena (the C ABI's mode), else null
     R *gre, *gim;
     size_t ld, point;
     __device__ __forceinline__ uint32_t at(uint32_t slot) const { return (slot << log_pw) + pw; }
-    __device__ __forceinline__ Cx<R> cur(uint32_t slot) const { return cx(cre[at(slot)], cim[at(slot)]); }
+    __device__ __forceinline__ Cx<R> cur(uint32_t slot) const {
+        Pair<R> v = cur_[at(slot)];
+        return cx(v.re, v.im);
+    }
     __device__ __forceinline__ void put(uint32_t slot, Cx<R> v) const {
-        cre[at(slot)] = v.re;
-        cim[at(slot)] = v.im;
+        Pair<R> x;
+        x.re = v.re;
+        x.im = v.im;
+        cur_[at(slot)] = x;
     }
     __device__ __forceinline__ Den form(uint32_t f, int k) const { return mom[at(f * 4 + k)]; }
     __device__ __forceinline__ Cx<R> scale(uint32_t s) const { return cx(cast<R>(sre[s]), cast<R>(sim[s])); }
     __device__ __forceinline__ Cx<R> factor(uint32_t x) const { return cx(cast<R>(fre[x]), cast<R>(fim[x])); }
     __device__ __forceinline__ void amp(uint32_t a, Amp &re, Amp &im) const {
-        re = are[at(a)];
-        im = aim[at(a)];
+        Pair<Amp> v = amp_[at(a)];
+        re = v.re;
+        im = v.im;
     }
     __device__ __forceinline__ void put_amp(uint32_t a, Amp re, Amp im) const {
-        are[at(a)] = re;
-        aim[at(a)] = im;
+        Pair<Amp> x;
+        x.re = re;
+        x.im = im;
+        amp_[at(a)] = x;
     }
     __device__ __forceinline__ void writeback(uint32_t plane, const Cx<R> *v, int n) const {
-        if (!gre) return;
-        for (int k = 0; k < n; k++) {
-            gre[(plane + k) * ld + point] = v[k].re;
-            gim[(plane + k) * ld + point] = v[k].im;
-        }
+        if (ABI && gre)
+            for (int k = 0; k < n; k++) {
+                gre[(plane + k) * ld + point] = v[k].re;
+                gim[(plane + k) * ld + point] = v[k].im;
+            }
     }
 };
 
@@ -111,7 +126,8 @@ __device__ __forceinline__ void point_sync(uint32_t log_lanes) {
     }
 }
 
-template <class K>
+// ABI: the C ABI's mode (arena in and out) or a batch's (outputs only)
+template <class K, bool ABI>
 __global__ void __launch_bounds__(512, 1) run_tiled(TiledLaunch L) {
     typedef typename K::R R;
     typedef typename K::Den Den;
@@ -124,46 +140,50 @@ __global__ void __launch_bounds__(512, 1) run_tiled(TiledLaunch L) {
         if (threadIdx.x == 0) next_item = atomicAdd(L.counter, 1ull);
         __syncthreads();
         const unsigned long long item = next_item;
-        __syncthreads();  // every thread has the item before the next one replaces it
         if (item >= total) break;
         uint32_t k = 0;
         while (item >= L.item_first[k + 1]) k++;
         const TiledPlan &p = L.plans[k];
-        const uint32_t log_l = p.log_lanes, lanes = 1u << log_l;
+        // the plan's constants (the kind's layout) into shared memory
+        Const *consts = (Const *)smem;
+        const uint32_t nconst = 2 * (p.scales + p.factors);
+        for (uint32_t c = threadIdx.x; c < nconst; c += blockDim.x) consts[c] = ((const Const *)p.kconst)[c];
+        __syncthreads();  // the constants are in, and every thread has the item
+        const uint32_t log_l = p.log_lanes, lanes = 1u << log_l, levels = p.levels;
         const uint32_t log_pw = log_l < 5 ? 5 - log_l : 0;  // points per region
         const uint32_t tl = threadIdx.x & (lanes - 1);
         const uint32_t pw = log_l < 5 ? (threadIdx.x & 31) >> log_l : 0;
         // the region: one warp's points (L <= 32) or one point's warps (L > 32)
         const uint32_t region = log_l < 5 ? threadIdx.x >> 5 : threadIdx.x >> log_l;
-        unsigned char *base = smem + (size_t)region * ((size_t)p.point_bytes << log_pw);
+        unsigned char *base = smem + L.const_bytes + (size_t)region * ((size_t)p.point_bytes << log_pw);
         const uint32_t count = L.count[k];
         const size_t first = (size_t)(item - L.item_first[k]) * (blockDim.x >> log_l);
         const size_t mine = first + (threadIdx.x >> log_l);
         const bool valid = mine < count;
         const size_t point = valid ? mine : count - 1;  // padding lanes redo the last point, unwritten
-        SlotView<K> v;
-        v.cre = (R *)base;
-        v.cim = v.cre + ((size_t)p.cur_slots << log_pw);
-        v.are = (Amp *)(v.cim + ((size_t)p.cur_slots << log_pw));
-        v.aim = v.are + ((size_t)p.amp_slots << log_pw);
-        double *forms64 = (double *)(v.aim + ((size_t)p.amp_slots << log_pw));
+        SlotView<K, ABI> v;
+        v.cur_ = (Pair<R> *)base;
+        v.amp_ = (Pair<Amp> *)(v.cur_ + ((size_t)p.cur_slots << log_pw));
+        double *forms64 = (double *)(v.amp_ + ((size_t)p.amp_slots << log_pw));
         v.mom = (const Den *)forms64;
-        v.sre = (const Const *)p.kconst;
+        v.sre = consts;
         v.sim = v.sre + p.scales;
         v.fre = v.sim + p.scales;
         v.fim = v.fre + p.factors;
         v.log_pw = log_pw;
         v.pw = pw;
-        v.gre = (L.abi && valid) ? (R *)L.cre : nullptr;
-        v.gim = (R *)L.cim;
-        v.ld = L.ld;
-        v.point = point;
+        if (ABI) {
+            v.gre = valid ? (R *)L.cre : nullptr;
+            v.gim = (R *)L.cim;
+            v.ld = L.ld;
+            v.point = point;
+        }
         // forms, f64: from the external momenta (0.0 + c0 p + c1 p + ..., in term order), or the
         // uploaded planes
         for (uint32_t q = tl; q < 4 * p.forms; q += lanes) {
             uint32_t f = q >> 2, c = q & 3;
             double val;
-            if (L.mom) {
+            if (ABI && L.mom) {
                 val = L.mom[(size_t)q * L.ld + point];
             } else {
                 uint32_t t0 = __ldg(p.form_terms + 2 * f), n = __ldg(p.form_terms + 2 * f + 1);
@@ -178,34 +198,31 @@ __global__ void __launch_bounds__(512, 1) run_tiled(TiledLaunch L) {
             forms64[(q << log_pw) + pw] = val;
         }
         // the C ABI's mode: live-in currents and every amplitude from the global arena
-        if (L.abi) {
+        if (ABI) {
             for (uint32_t j = 0; j < p.nloads; j++) {
                 uint32_t plane = __ldg(p.loads + 3 * j), slot = __ldg(p.loads + 3 * j + 1), n = __ldg(p.loads + 3 * j + 2);
-                for (uint32_t c = tl; c < n; c += lanes) {
-                    v.cre[((slot + c) << log_pw) + pw] = ((const R *)L.cre)[(plane + c) * L.ld + point];
-                    v.cim[((slot + c) << log_pw) + pw] = ((const R *)L.cim)[(plane + c) * L.ld + point];
-                }
+                for (uint32_t c = tl; c < n; c += lanes)
+                    v.put(slot + c, cx(((const R *)L.cre)[(plane + c) * L.ld + point],
+                                       ((const R *)L.cim)[(plane + c) * L.ld + point]));
             }
             for (uint32_t a = tl; a < p.amp_slots; a += lanes) {
                 uint32_t plane = __ldg(p.amp_planes + a);
-                v.are[(a << log_pw) + pw] = ((const Amp *)L.are)[plane * L.ld + point];
-                v.aim[(a << log_pw) + pw] = ((const Amp *)L.aim)[plane * L.ld + point];
+                v.put_amp(a, ((const Amp *)L.are)[plane * L.ld + point], ((const Amp *)L.aim)[plane * L.ld + point]);
             }
         } else {
-            for (uint32_t a = tl; a < p.amp_slots; a += lanes) {
-                v.are[(a << log_pw) + pw] = konst<Amp>(0.0);
-                v.aim[(a << log_pw) + pw] = konst<Amp>(0.0);
-            }
+            for (uint32_t a = tl; a < p.amp_slots; a += lanes) v.put_amp(a, konst<Amp>(0.0), konst<Amp>(0.0));
         }
         point_sync(log_l);
-        for (uint32_t lv = 0; lv < p.levels; lv++) {
-            uint32_t t0 = __ldg(p.level_first + lv), t1 = __ldg(p.level_first + lv + 1);
-            for (uint32_t t = t0 + tl; t < t1; t += lanes) {
-                uint32_t i0 = __ldg(p.task_first + t), i1 = __ldg(p.task_first + t + 1);
-                if (lv == 0) {
+        const Ins *ins = p.ins;
+        const uint2 *order = reinterpret_cast<const uint2 *>(p.order);
+        for (uint32_t lv = 0; lv < levels; lv++) {
+            uint32_t j0 = __ldg(p.level_first + lv), j1 = __ldg(p.level_first + lv + 1);
+            if (lv == 0) {
+                for (uint32_t j = j0 + tl; j < j1; j += lanes) {
+                    uint2 r = __ldg(order + j);
                     // sources: f64 wavefunctions from the f64 forms and constants, narrowed
-                    for (uint32_t n = i0; n < i1; n++) {
-                        Ins o = load_ins(p.ins, n);
+                    for (uint32_t n = r.x; n < r.y; n++) {
+                        Ins o = load_ins(ins, n);
                         double mom[4];
                         for (int c = 0; c < 4; c++) mom[c] = forms64[((o.f * 4 + c) << log_pw) + pw];
                         double fr = __ldg(p.f64 + o.x), fi = __ldg(p.f64 + p.factors + o.x), mass = __ldg(p.s64 + o.s);
@@ -219,11 +236,21 @@ __global__ void __launch_bounds__(512, 1) run_tiled(TiledLaunch L) {
                         }
                         if (ins_flags(o) & 8) v.writeback(o.c, vals, m);
                     }
-                } else {
+                }
+            } else {
+                // the next task's range is fetched while a task runs, and each next instruction
+                // while its predecessor runs
+                uint32_t j = j0 + tl;
+                uint2 r = j < j1 ? __ldg(order + j) : make_uint2(0, 0);
+                while (j < j1) {
+                    uint2 cur = r;
+                    j += lanes;
+                    if (j < j1) r = __ldg(order + j);
+                    if (cur.x == cur.y) continue;
                     Cx<R> acc[6];
 #pragma unroll
                     for (int c = 0; c < 6; c++) acc[c] = cx(konst<R>(0.0), konst<R>(0.0));
-                    for (uint32_t n = i0; n < i1; n++) exec_row<K>(v, load_ins(p.ins, n), acc);
+                    for (uint32_t n = cur.x; n < cur.y; n++) exec_row<K>(v, load_ins(ins, n), acc);
                 }
             }
             point_sync(log_l);
@@ -236,12 +263,14 @@ __global__ void __launch_bounds__(512, 1) run_tiled(TiledLaunch L) {
                 point_sync(log_l);
             }
         }
-        if (L.abi) {
+        if (ABI) {
             if (valid)
                 for (uint32_t a = tl; a < p.amp_slots; a += lanes) {
                     uint32_t plane = __ldg(p.amp_planes + a);
-                    ((Amp *)L.are)[plane * L.ld + point] = v.are[(a << log_pw) + pw];
-                    ((Amp *)L.aim)[plane * L.ld + point] = v.aim[(a << log_pw) + pw];
+                    Amp re, im;
+                    v.amp(a, re, im);
+                    ((Amp *)L.are)[plane * L.ld + point] = re;
+                    ((Amp *)L.aim)[plane * L.ld + point] = im;
                 }
         } else if (valid) {
             // the resolved reduction from zero: out[point][o] = 0 + w fma(re, re, im im) + ...
@@ -252,8 +281,10 @@ __global__ void __launch_bounds__(512, 1) run_tiled(TiledLaunch L) {
                     uint32_t s = __ldg(p.red_slots + j);
                     double re = 0.0, im = 0.0;
                     if (s != ~0u) {
-                        re = to_f64_value(v.are[(s << log_pw) + pw]);
-                        im = to_f64_value(v.aim[(s << log_pw) + pw]);
+                        Amp ar, ai;
+                        v.amp(s, ar, ai);
+                        re = to_f64_value(ar);
+                        im = to_f64_value(ai);
                     }
                     acc = __dadd_rn(acc, __dmul_rn(__ldg(p.red_weights + j), __fma_rn(re, re, __dmul_rn(im, im))));
                 }

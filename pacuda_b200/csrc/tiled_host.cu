@@ -16,14 +16,16 @@ template <class T> bool put(T **dst, const std::vector<T> &v, cudaStream_t s) {
     return v.empty() || cudaMemcpyAsync(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s) == cudaSuccess;
 }
 
-template <class K> const void *kernel_of() { return (const void *)run_tiled<K>; }
+template <class K> const void *kernel_of(bool abi) {
+    return abi ? (const void *)run_tiled<K, true> : (const void *)run_tiled<K, false>;
+}
 
-const void *kernel_for(int kernel) {
+const void *kernel_for(int kernel, bool abi = false) {
     switch (kernel) {
-    case PACMAN_RECURRENCE_KERNEL_F64: return kernel_of<KindF64>();
-    case PACMAN_RECURRENCE_KERNEL_MIXED: return kernel_of<KindMixed>();
-    case PACMAN_RECURRENCE_KERNEL_MIXED64: return kernel_of<KindMixed64>();
-    default: return kernel_of<KindDF64>();
+    case PACMAN_RECURRENCE_KERNEL_F64: return kernel_of<KindF64>(abi);
+    case PACMAN_RECURRENCE_KERNEL_MIXED: return kernel_of<KindMixed>(abi);
+    case PACMAN_RECURRENCE_KERNEL_MIXED64: return kernel_of<KindMixed64>(abi);
+    default: return kernel_of<KindDF64>(abi);
     }
 }
 }  // namespace
@@ -31,20 +33,39 @@ const void *kernel_for(int kernel) {
 void TiledDevice::release() {
     cudaFree(ins);
     cudaFree(task_first);
-    cudaFree(level_first);
     cudaFree(loads);
     cudaFree(amp_planes);
+    for (int k = 0; k < 10; k++) {
+        cudaFree(order[k]);
+        cudaFree(level_first[k]);
+        order[k] = level_first[k] = nullptr;
+    }
     ins = nullptr;
-    task_first = level_first = loads = amp_planes = nullptr;
+    task_first = loads = amp_planes = nullptr;
     ok = false;
 }
 
 bool upload_schedule(TiledDevice &t, cudaStream_t s) {
-    t.ok = put(&t.ins, t.host.ins, s) && put(&t.task_first, t.host.task_first, s) &&
-           put(&t.level_first, t.host.level_first, s) && put(&t.loads, t.host.loads, s) &&
+    t.ok = put(&t.ins, t.host.ins, s) && put(&t.task_first, t.host.task_first, s) && put(&t.loads, t.host.loads, s) &&
            put(&t.amp_planes, t.host.amp_planes, s);
+    t.levels = (uint32_t)t.host.level_first.size() - 1;
+    for (int k = 0; t.ok && k < 10; k++) {
+        std::vector<uint32_t> order, lf, ranges;
+        lane_order(t.host, (uint32_t)k, order, lf);
+        // each position holds its task's instruction range (first, end); (0, 0) for none
+        ranges.reserve(2 * order.size());
+        for (uint32_t task : order) {
+            ranges.push_back(task == ~0u ? 0 : t.host.task_first[task]);
+            ranges.push_back(task == ~0u ? 0 : t.host.task_first[task + 1]);
+        }
+        t.ok = put(&t.order[k], ranges, s) && put(&t.level_first[k], lf, s);
+    }
+    // the host vectors must outlive the asynchronous copies
+    cudaStreamSynchronize(s);
     return t.ok;
 }
+
+size_t tiled_const_bytes(uint32_t scales, uint32_t factors) { return ((2 * (size_t)scales + 2 * factors) * 8 + 15) / 16 * 16; }
 
 size_t tiled_point_bytes(const Schedule &s, uint32_t forms, int kernel) {
     size_t value = kernel == PACMAN_RECURRENCE_KERNEL_MIXED || kernel == PACMAN_RECURRENCE_KERNEL_MIXED64 ? 4 : 8;
@@ -53,8 +74,12 @@ size_t tiled_point_bytes(const Schedule &s, uint32_t forms, int kernel) {
 }
 
 int tiled_threads(int kernel) {
-    cudaFuncAttributes attr;
-    if (cudaFuncGetAttributes(&attr, kernel_for(kernel)) != cudaSuccess) return 0;
+    cudaFuncAttributes attr, abi;
+    if (cudaFuncGetAttributes(&attr, kernel_for(kernel, false)) != cudaSuccess ||
+        cudaFuncGetAttributes(&abi, kernel_for(kernel, true)) != cudaSuccess)
+        return 0;
+    attr.numRegs = std::max(attr.numRegs, abi.numRegs);
+    attr.maxThreadsPerBlock = std::min(attr.maxThreadsPerBlock, abi.maxThreadsPerBlock);
     int dev = 0, regs = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&regs, cudaDevAttrMaxRegistersPerBlock, dev);
@@ -68,8 +93,11 @@ int tiled_threads(int kernel) {
 }
 
 size_t tiled_max_smem(int kernel) {
-    cudaFuncAttributes attr;
-    if (cudaFuncGetAttributes(&attr, kernel_for(kernel)) != cudaSuccess) return 0;
+    cudaFuncAttributes attr, abi;
+    if (cudaFuncGetAttributes(&attr, kernel_for(kernel, false)) != cudaSuccess ||
+        cudaFuncGetAttributes(&abi, kernel_for(kernel, true)) != cudaSuccess)
+        return 0;
+    attr.sharedSizeBytes = std::max(attr.sharedSizeBytes, abi.sharedSizeBytes);
     int dev = 0, smem = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
@@ -89,8 +117,9 @@ int tiled_min_log_lanes(size_t point_bytes, int threads, size_t max_smem) {
 void describe(const TiledDevice &t, uint32_t forms, uint32_t log_lanes, size_t point_bytes, TiledPlan &p) {
     p.ins = t.ins;
     p.task_first = t.task_first;
-    p.level_first = t.level_first;
-    p.levels = (uint32_t)t.host.level_first.size() - 1;
+    p.order = t.order[log_lanes];
+    p.level_first = t.level_first[log_lanes];
+    p.levels = t.levels;
     p.cur_slots = t.host.cur_slots;
     p.amp_slots = t.host.amp_slots;
     p.forms = forms;
@@ -102,7 +131,7 @@ void describe(const TiledDevice &t, uint32_t forms, uint32_t log_lanes, size_t p
 }
 
 bool launch_tiled(int kernel, const TiledLaunch &args, int threads, size_t smem, int sms, cudaStream_t stream) {
-    const void *fn = kernel_for(kernel);
+    const void *fn = kernel_for(kernel, args.abi);
     if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return false;
     void *params[] = {(void *)&args};
     return cudaLaunchKernel(fn, dim3(sms), dim3(threads), params, smem, stream) == cudaSuccess;

@@ -14,10 +14,16 @@ struct TiledLaunch;
 struct TiledDevice {
     Schedule host;
     Ins *ins = nullptr;
-    uint32_t *task_first = nullptr, *level_first = nullptr, *loads = nullptr, *amp_planes = nullptr;
+    uint32_t *task_first = nullptr, *loads = nullptr, *amp_planes = nullptr;
+    // per lanes-per-point exponent 0 .. 9: the tasks' order and its level boundaries
+    uint32_t *order[10] = {nullptr}, *level_first[10] = {nullptr};
+    uint32_t levels = 0;
     bool ok = false;
     void release();
 };
+
+// bytes of shared memory a block needs for one plan's constants (scales and factors, re and im)
+size_t tiled_const_bytes(uint32_t scales, uint32_t factors);
 
 // the schedule's arrays on the device
 bool upload_schedule(TiledDevice &t, cudaStream_t stream);

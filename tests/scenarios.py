@@ -77,7 +77,7 @@ def fuzz_case(seed, points=37, stride=40):
     kw = dict(words=words, width=width, stride=stride, points=points, current_planes=planes, amplitude_planes=amps,
               momentum_planes=4 * forms, scales=(rng.uniform(-0.6, 0.6, scales), rng.uniform(-0.6, 0.6, scales)),
               factors=(rng.uniform(-0.6, 0.6, factors), rng.uniform(-0.6, 0.6, factors)),
-              upload_current=[0, planes], upload_amplitude=[0, amps - 1], zero_amplitude=[amps - 1, 1],
+              upload_current=upload_runs(rows, planes), upload_amplitude=[0, amps - 1], zero_amplitude=[amps - 1, 1],
               download_amplitude=[0, amps], download_current=[0, planes], words_key=0,
               current=(cre, cim), amplitude=(are, aim))
     ext = None
@@ -101,6 +101,28 @@ def fuzz_case(seed, points=37, stride=40):
         kw.update(external=ext, external_count=legs, form_terms=terms, term_slots=slots, term_coefficients=coef,
                   flags=abi.FORMS_ON_DEVICE, momenta=np.zeros(4 * forms * stride))
     return kw
+
+
+def upload_runs(rows, planes):
+    """Every plane but those the plan's source rows write, as (first, count) runs: a call does not
+    upload what its own sources compute (the reference converts such an upload after the sources
+    ran, which is not a meaningful call)."""
+    written = np.zeros(planes, dtype=bool)
+    for r in rows:
+        if r[0] == 12:
+            n = 1 if r[5] & 7 == 0 else 2 if r[5] & 7 == 1 else 4
+            written[r[1]:r[1] + n] = True
+    runs, p = [], 0
+    while p < planes:
+        if written[p]:
+            p += 1
+            continue
+        q = p
+        while q < planes and not written[q]:
+            q += 1
+        runs += [p, q - p]
+        p = q
+    return runs
 
 
 def fuzz_args(seed):

@@ -20,7 +20,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 HARNESS = os.path.join(HERE, "harness")
 LIB = os.path.join(HARNESS, "libschedule_harness.so")
 K_CONTRIB, K_PROP, K_IDENTITY, K_CLEAR, K_CLOSURE, K_SOURCE = 1, 2, 3, 4, 5, 6
-F_INIT, F_FIRST, F_LAST, F_WB = 1, 2, 4, 8
+F_INIT, F_FIRST, F_LAST, F_WB, F_ACC0, F_NOSTORE = 1, 2, 4, 8, 16, 32
 _lib = None
 
 
@@ -110,8 +110,9 @@ def _row(store, i, acc, wb=None):
             else:
                 acc[k] = hash(("add", store.get(c + k), val))
         if flags & F_LAST:
-            for k in range(cd):
-                store.put(c + k, acc[k])
+            if not flags & F_NOSTORE:
+                for k in range(cd):
+                    store.put(c + k, acc[k])
             if wb and flags & F_WB:
                 wb(y, [acc[k] for k in range(cd)])
     elif kind == K_PROP:
@@ -136,7 +137,8 @@ def _row(store, i, acc, wb=None):
     elif kind == K_CLOSURE:
         v = store.amp_get(c)
         for k in range(s):
-            v = hash(("closure", x, y + k, store.get(a + k), store.get(b + k), v))
+            left = acc[k] if flags & F_ACC0 else store.get(a + k)
+            v = hash(("closure", x, y + k, left, store.get(b + k), v))
         store.amp_put(c, v)
     elif kind == K_SOURCE:
         out = [hash(("source", y, f, x, s, k)) for k in range(_src_comps(y))]
