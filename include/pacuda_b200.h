@@ -64,6 +64,20 @@ int pacuda_b200_batch_capture(pacuda_b200_batch *batch, void *stream);
 uint32_t pacuda_b200_batch_launches(const pacuda_b200_batch *batch);
 void pacuda_b200_batch_destroy(pacuda_b200_batch *batch);
 
+/* Evaluates plans as a batch of them would, without a batch object and without allocating
+ * anything: the launch's descriptors and its work-item counter live in a fixed array of this
+ * library in device memory (one per device), which a small setup kernel fills and zeroes on
+ * `stream` before the executor's launch (2 kernel launches). No counterpart in the reference.
+ * For callers that cannot allocate device or pinned memory when they evaluate.
+ * Limits: 1 to PACUDA_B200_STATIC_MAX_PLANS plans, else INVALID (with a message on stderr). Calls
+ * on one device must not overlap in time (they share the array): use one stream, or order them.
+ * The first call on each device, with that device current, looks up the array's address (which
+ * may load the library's device code); make it before capturing any stream on that device. Each
+ * plan runs with its own lanes per point when the launch's shared memory allows, as in a batch. */
+#define PACUDA_B200_STATIC_MAX_PLANS 8
+int pacuda_b200_run_static(pacuda_b200_plan *const *plans, uint32_t nplans, const double *const *external,
+                           const uint32_t *count, double *const *output, void *stream);
+
 /* Measurement: launches blocks x threads threads that each run 8 independent chains of
  * `iterations` f64 fused multiply-adds (2 flops each) on `stream`; the caller times it. `sink`
  * is a device array of at least *blocks doubles (never written in practice). */

@@ -5,6 +5,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <mutex>
 #include <vector>
 
 #include "../../include/pacuda_b200.h"
@@ -415,4 +416,137 @@ extern "C" void pacuda_b200_batch_destroy(pacuda_b200_batch *b) {
     cudaFreeHost(b->host);
     cudaFree(b->device);
     delete b;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Evaluation without allocation (pacuda_b200_run_static).
+//
+// pacuda_b200_batch_create allocates a pinned and a device descriptor block. Some callers cannot
+// allocate when they evaluate: an integrand callback that runs inside a host framework which owns
+// the device's memory pool (an allocation there bypasses the pool, can fail once the pool has
+// taken the device's memory, and stalls the device while the driver maps it), or a caller that is
+// recording the surrounding work into a CUDA graph, where a cudaMalloc is no stream operation at
+// all. For them this entry point keeps the descriptors of one launch and its work-item counter in
+// a fixed array of this library in device memory. It allocates nothing; the plans' own arrays were
+// allocated when they were created.
+//
+// Limits: at most PACUDA_B200_STATIC_MAX_PLANS plans per call (more are INVALID). The array is one
+// per device: calls on one device must not overlap (the second call's setup would overwrite the
+// first's descriptors and counter while the first runs), so issue them on one stream or order
+// them with events.
+
+namespace {
+
+constexpr uint32_t kStaticPlans = PACUDA_B200_STATIC_MAX_PLANS;
+constexpr int kStaticDevices = 64;
+
+// the launch's descriptors; the setup kernel receives them as its parameter (under 4 KB)
+struct StaticBlock {
+    TiledPlan plans[kStaticPlans];
+    unsigned long long items[kStaticPlans + 1];
+    const double *external[kStaticPlans];
+    double *output[kStaticPlans];
+    uint32_t count[kStaticPlans];
+};
+constexpr size_t kStaticCounter = (sizeof(StaticBlock) + 255) / 256 * 256;
+constexpr size_t kStaticBytes = 4096;
+static_assert(kStaticCounter + sizeof(unsigned long long) <= kStaticBytes, "the static scratch is too small");
+static_assert(sizeof(StaticBlock) <= 4000, "the descriptors exceed a kernel parameter");
+
+// the scratch: StaticBlock at 0; the work-item counter at kStaticCounter, which must be zero when
+// the executor starts (the setup kernel of every call zeroes it); nothing else needs a start value
+__device__ __align__(256) unsigned char g_static_scratch[kStaticBytes];
+
+__global__ void static_setup(StaticBlock block, unsigned char *scratch) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        *(StaticBlock *)scratch = block;
+        *(unsigned long long *)(scratch + kStaticCounter) = 0;
+    }
+}
+
+std::mutex g_static_mutex;
+void *g_static_address[kStaticDevices] = {nullptr};
+
+// the scratch's address on the current device, looked up on the first call with that device
+// current (the lookup may load this library's device code; later calls only read the cache)
+unsigned char *static_scratch() {
+    int dev = -1;
+    if (failed(cudaGetDevice(&dev), "current device")) return nullptr;
+    if (dev < 0 || dev >= kStaticDevices) {
+        fprintf(stderr, "%s: run_static: device %d beyond the %d this entry point serves\n", kTag, dev, kStaticDevices);
+        return nullptr;
+    }
+    std::lock_guard<std::mutex> lock(g_static_mutex);
+    if (!g_static_address[dev]) {
+        void *address = nullptr;
+        if (failed(cudaGetSymbolAddress(&address, g_static_scratch), "static scratch address") || !address)
+            return nullptr;
+        g_static_address[dev] = address;
+    }
+    return (unsigned char *)g_static_address[dev];
+}
+
+}  // namespace
+
+extern "C" int pacuda_b200_run_static(pacuda_b200_plan *const *plans, uint32_t nplans, const double *const *external,
+                                      const uint32_t *count, double *const *output, void *stream) {
+    if (nplans == 0 || nplans > kStaticPlans) {
+        fprintf(stderr, "%s: run_static: %u plans; this entry point takes 1 to %u\n", kTag, nplans, kStaticPlans);
+        return PACMAN_RECURRENCE_INVALID;
+    }
+    if (!plans || !external || !count || !output) return PACMAN_RECURRENCE_INVALID;
+    for (uint32_t k = 0; k < nplans; k++)
+        if (!plans[k] || plans[k]->kernel != plans[0]->kernel || !count[k] || !external[k] || !output[k]) {
+            fprintf(stderr, "%s: run_static: plan %u: a missing plan, array or point count, or another kernel kind\n",
+                    kTag, k);
+            return PACMAN_RECURRENCE_INVALID;
+        }
+    unsigned char *scratch = static_scratch();
+    if (!scratch) return PACMAN_RECURRENCE_DEVICE_ERROR;
+    // the launch's shape as a batch of these plans has it; the plans' own choices are not changed
+    int kernel = plans[0]->kernel;
+    int threads = tiled_threads(kernel);
+    size_t const_bytes = 0;
+    for (uint32_t k = 0; k < nplans; k++)
+        const_bytes = std::max(const_bytes, tiled_const_bytes(plans[k]->scales, plans[k]->factors));
+    size_t max_smem = tiled_max_smem(kernel) - const_bytes;
+    StaticBlock block;
+    memset(&block, 0, sizeof block);
+    size_t smem = 0;
+    for (uint32_t k = 0; k < nplans; k++) {
+        const pacuda_b200_plan *p = plans[k];
+        int lo = tiled_min_log_lanes(p->point_bytes, threads, max_smem);
+        if (lo < 0) {
+            fprintf(stderr, "%s: run_static: a plan's point does not fit a block's shared memory\n", kTag);
+            return PACMAN_RECURRENCE_INVALID;
+        }
+        uint32_t lg = ((int)p->log_lanes < lo || (1 << p->log_lanes) > threads) ? (uint32_t)lo : p->log_lanes;
+        fill_plan(p, block.plans[k]);
+        describe(p->tiled, p->forms, lg, p->point_bytes, block.plans[k]);
+        uint32_t per = (uint32_t)threads >> lg;
+        smem = std::max<size_t>(smem, (size_t)per * p->point_bytes);
+        block.items[k + 1] = block.items[k] + (count[k] + per - 1) / per;
+        block.external[k] = external[k];
+        block.output[k] = output[k];
+        block.count[k] = count[k];
+    }
+    smem += const_bytes;
+    cudaStream_t s = (cudaStream_t)stream;
+    static_setup<<<1, 32, 0, s>>>(block, scratch);
+    if (failed(cudaGetLastError(), "run_static setup")) return PACMAN_RECURRENCE_DEVICE_ERROR;
+    const StaticBlock *d = (const StaticBlock *)scratch;
+    TiledLaunch L;
+    memset(&L, 0, sizeof L);
+    L.plans = d->plans;
+    L.nplans = nplans;
+    L.item_first = d->items;
+    L.external = d->external;
+    L.output = d->output;
+    L.count = d->count;
+    L.counter = (unsigned long long *)(scratch + kStaticCounter);
+    L.abi = false;
+    L.const_bytes = (uint32_t)const_bytes;
+    if (!launch_tiled(kernel, L, threads, smem, device_sms(), s) || failed(cudaGetLastError(), "run_static launch"))
+        return PACMAN_RECURRENCE_DEVICE_ERROR;
+    return PACMAN_RECURRENCE_OK;
 }
