@@ -48,7 +48,7 @@ struct pacuda_b200_plan {
     double *coefficients = nullptr;
     uint32_t *red_offsets = nullptr, *red_slots = nullptr;
     double *red_weights = nullptr;
-    uint32_t log_lanes = 5;   // lanes per point, as an exponent
+    uint32_t lanes = 32;      // lanes per point (tiled_host.h: 1 .. 16 or a multiple of 32)
     size_t point_bytes = 0;
     bool fixed = false;
 };
@@ -73,7 +73,7 @@ namespace {
 
 void fill_plan(const pacuda_b200_plan *p, TiledPlan &d) {
     memset(&d, 0, sizeof d);
-    describe(p->tiled, p->forms, p->log_lanes, p->point_bytes, d);
+    describe(p->tiled, p->forms, p->lanes, p->point_bytes, d);
     d.s64 = p->consts;
     d.f64 = p->consts + 2 * p->scales;
     d.kconst = p->consts + 2 * (p->scales + p->factors);
@@ -125,14 +125,14 @@ bool prepare(pacuda_b200_batch *b) {
     items[0] = 0;
     for (size_t k = 0; k < n; k++) {
         pacuda_b200_plan *p = b->plans[k];
-        int lo = tiled_min_log_lanes(p->point_bytes, b->threads, max_smem);
-        if (lo < 0) {
+        uint32_t lo = tiled_min_lanes(p->point_bytes, b->threads, max_smem);
+        if (!lo) {
             fprintf(stderr, "%s: a plan's point does not fit a block's shared memory\n", kTag);
             return false;
         }
-        if ((int)p->log_lanes < lo || (1 << p->log_lanes) > b->threads) p->log_lanes = (uint32_t)lo;
+        if (!tiled_lanes_fit(p->lanes, p->point_bytes, b->threads, max_smem)) p->lanes = lo;
         fill_plan(p, plans[k]);
-        uint32_t per = (uint32_t)b->threads >> p->log_lanes;
+        uint32_t per = (uint32_t)b->threads / p->lanes;
         b->smem = std::max<size_t>(b->smem, (size_t)per * p->point_bytes);
         items[k + 1] = items[k] + (b->count[k] + per - 1) / per;
     }
@@ -169,11 +169,15 @@ int launch(pacuda_b200_batch *b, cudaStream_t s) {
     return PACMAN_RECURRENCE_OK;
 }
 
+// the shared memory a block has for one plan's points
+size_t point_smem(const pacuda_b200_plan *p) {
+    return tiled_max_smem(p->kernel) - tiled_const_bytes(p->scales, p->factors);
+}
+
 // the fewest lanes per point whose block of points fits shared memory
-uint32_t default_log_lanes(const pacuda_b200_plan *p) {
-    int lo = tiled_min_log_lanes(p->point_bytes, tiled_threads(p->kernel),
-                                 tiled_max_smem(p->kernel) - tiled_const_bytes(p->scales, p->factors));
-    return lo < 0 ? 5u : (uint32_t)lo;
+uint32_t default_lanes(const pacuda_b200_plan *p) {
+    uint32_t lo = tiled_min_lanes(p->point_bytes, tiled_threads(p->kernel), point_smem(p));
+    return lo ? lo : 32u;
 }
 
 }  // namespace
@@ -260,7 +264,7 @@ extern "C" pacuda_b200_plan *pacuda_b200_plan_create(const pacman_recurrence_cal
         return nullptr;
     }
     p->point_bytes = tiled_point_bytes(p->tiled.host, forms, p->kernel);
-    p->log_lanes = default_log_lanes(p);
+    p->lanes = default_lanes(p);
     return p;
 }
 
@@ -279,24 +283,19 @@ extern "C" void pacuda_b200_plan_destroy(pacuda_b200_plan *p) {
 extern "C" uint64_t pacuda_b200_plan_flops(const pacuda_b200_plan *p) { return p ? p->prog.flops : 0; }
 
 extern "C" int pacuda_b200_plan_set_lanes_per_point(pacuda_b200_plan *p, uint32_t lanes) {
-    if (!p || lanes > 512 || (lanes & (lanes - 1))) return PACMAN_RECURRENCE_INVALID;
+    if (!p) return PACMAN_RECURRENCE_INVALID;
     if (lanes == 0) {
         p->fixed = false;
-        p->log_lanes = default_log_lanes(p);
+        p->lanes = default_lanes(p);
         return PACMAN_RECURRENCE_OK;
     }
-    uint32_t lg = 0;
-    while ((1u << lg) < lanes) lg++;
-    int lo = tiled_min_log_lanes(p->point_bytes, tiled_threads(p->kernel),
-                                 tiled_max_smem(p->kernel) - tiled_const_bytes(p->scales, p->factors));
-    if (lo < 0 || (int)lg < lo || (1 << lg) > tiled_threads(p->kernel) || (lg > 5 && (tiled_threads(p->kernel) >> lg) > 15))
-        return PACMAN_RECURRENCE_INVALID;
-    p->log_lanes = lg;
+    if (!tiled_lanes_fit(lanes, p->point_bytes, tiled_threads(p->kernel), point_smem(p))) return PACMAN_RECURRENCE_INVALID;
+    p->lanes = lanes;
     p->fixed = true;
     return PACMAN_RECURRENCE_OK;
 }
 
-extern "C" uint32_t pacuda_b200_plan_lanes_per_point(const pacuda_b200_plan *p) { return p ? 1u << p->log_lanes : 0; }
+extern "C" uint32_t pacuda_b200_plan_lanes_per_point(const pacuda_b200_plan *p) { return p ? p->lanes : 0; }
 
 extern "C" pacuda_b200_batch *pacuda_b200_batch_create(pacuda_b200_plan *const *plans, uint32_t nplans,
                                                        const double *const *external, const uint32_t *count,
@@ -372,13 +371,12 @@ extern "C" int pacuda_b200_batch_tune(pacuda_b200_batch *b, void *stream) {
         const double *ext[1] = {b->external[k]};
         double *out[1] = {b->output[k]};
         float best = 1e30f;
-        uint32_t best_lg = p->log_lanes;
+        uint32_t best_lanes = p->lanes;
         int threads = tiled_threads(p->kernel);
-        int lo = tiled_min_log_lanes(p->point_bytes, threads,
-                                     tiled_max_smem(p->kernel) - tiled_const_bytes(p->scales, p->factors));
-        for (int lg = lo; lo >= 0 && (1 << lg) <= threads; lg++) {
-            if (lg > 5 && (threads >> lg) > 15) continue;
-            p->log_lanes = (uint32_t)lg;
+        for (int choice = 0; choice < kLaneChoices; choice++) {
+            uint32_t lanes = lanes_of_choice(choice);
+            if (!tiled_lanes_fit(lanes, p->point_bytes, threads, point_smem(p))) continue;
+            p->lanes = lanes;
             uint32_t n = b->count[k];
             pacuda_b200_batch *tb = pacuda_b200_batch_create(one, 1, ext, &n, out);
             if (!tb) continue;
@@ -396,10 +394,10 @@ extern "C" int pacuda_b200_batch_tune(pacuda_b200_batch *b, void *stream) {
             pacuda_b200_batch_destroy(tb);
             if (ok && ms < best) {
                 best = ms;
-                best_lg = (uint32_t)lg;
+                best_lanes = lanes;
             }
         }
-        p->log_lanes = best_lg;
+        p->lanes = best_lanes;
         (void)sample;
     }
     cudaEventDestroy(t0);
@@ -515,15 +513,15 @@ extern "C" int pacuda_b200_run_static(pacuda_b200_plan *const *plans, uint32_t n
     size_t smem = 0;
     for (uint32_t k = 0; k < nplans; k++) {
         const pacuda_b200_plan *p = plans[k];
-        int lo = tiled_min_log_lanes(p->point_bytes, threads, max_smem);
-        if (lo < 0) {
+        uint32_t lo = tiled_min_lanes(p->point_bytes, threads, max_smem);
+        if (!lo) {
             fprintf(stderr, "%s: run_static: a plan's point does not fit a block's shared memory\n", kTag);
             return PACMAN_RECURRENCE_INVALID;
         }
-        uint32_t lg = ((int)p->log_lanes < lo || (1 << p->log_lanes) > threads) ? (uint32_t)lo : p->log_lanes;
+        uint32_t lanes = tiled_lanes_fit(p->lanes, p->point_bytes, threads, max_smem) ? p->lanes : lo;
         fill_plan(p, block.plans[k]);
-        describe(p->tiled, p->forms, lg, p->point_bytes, block.plans[k]);
-        uint32_t per = (uint32_t)threads >> lg;
+        describe(p->tiled, p->forms, lanes, p->point_bytes, block.plans[k]);
+        uint32_t per = (uint32_t)threads / lanes;
         smem = std::max<size_t>(smem, (size_t)per * p->point_bytes);
         block.items[k + 1] = block.items[k] + (count[k] + per - 1) / per;
         block.external[k] = external[k];

@@ -380,15 +380,12 @@ int onchip_launch(DeviceProgram *prog, const pacman_recurrence_call *c, const Ru
     int threads = prog->tiled_state == 1 ? tiled_threads(kernel) : 0;
     size_t pb = prog->tiled_state == 1 ? tiled_point_bytes(prog->tiled.host, forms, kernel) : 0;
     size_t cb = tiled_const_bytes(c->scale_count, c->factor_count);
-    int lo = threads ? tiled_min_log_lanes(pb, threads, tiled_max_smem(kernel) - cb) : -1;
-    int log_l = lo;
-    if (lo >= 0 && current.lanes_per_point) {
-        int want = 0;
-        while ((1u << want) < current.lanes_per_point) want++;
-        log_l = (want >= lo && (1 << want) <= threads && !(want > 5 && (threads >> want) > 15)) ? want : -1;
-    }
-    if (log_l < 0) return current.executor == PACUDA_B200_EXECUTOR_ONCHIP ? 2 : 0;
-    size_t smem = cb + (size_t)(threads >> log_l) * pb;
+    size_t room = threads ? tiled_max_smem(kernel) - cb : 0;
+    uint32_t lanes = threads ? tiled_min_lanes(pb, threads, room) : 0;
+    if (lanes && current.lanes_per_point)
+        lanes = tiled_lanes_fit(current.lanes_per_point, pb, threads, room) ? current.lanes_per_point : 0;
+    if (!lanes) return current.executor == PACUDA_B200_EXECUTOR_ONCHIP ? 2 : 0;
+    size_t smem = cb + (size_t)(threads / lanes) * pb;
     // descriptors: TiledPlan | item_first[2] | external[1] | count[1] | counter
     const size_t o_items = (sizeof(TiledPlan) + 15) / 16 * 16, o_ext = o_items + 16, o_count = o_ext + 8,
                  o_counter = (o_count + 4 + 15) / 16 * 16, total = o_counter + 16;
@@ -396,7 +393,7 @@ int onchip_launch(DeviceProgram *prog, const pacman_recurrence_call *c, const Ru
     if (!dev.launch_dev.reserve(total, "descriptors")) return -1;
     memset(dev.launch_host, 0, total);
     TiledPlan &p = *(TiledPlan *)dev.launch_host;
-    describe(prog->tiled, forms, (uint32_t)log_l, pb, p);
+    describe(prog->tiled, forms, lanes, pb, p);
     p.s64 = a.s64;
     p.f64 = a.f64;
     p.kconst = a.kconst;
@@ -407,7 +404,7 @@ int onchip_launch(DeviceProgram *prog, const pacman_recurrence_call *c, const Ru
     p.coefficients = a.coefficients;
     unsigned long long *items = (unsigned long long *)(dev.launch_host + o_items);
     items[0] = 0;
-    uint32_t per = (uint32_t)threads >> log_l;
+    uint32_t per = (uint32_t)threads / lanes;
     items[1] = (a.points + per - 1) / per;
     *(const double **)(dev.launch_host + o_ext) = a.external;
     *(uint32_t *)(dev.launch_host + o_count) = a.points;
@@ -852,8 +849,7 @@ extern "C" int pacman_recurrence_v1_configure(const pacman_recurrence_options *o
     n.sort = !o->no_sort;
     if (o->struct_size >= sizeof(pacuda_b200_options)) {
         const pacuda_b200_options *x = (const pacuda_b200_options *)o;
-        if (x->executor > PACUDA_B200_EXECUTOR_ONCHIP || x->lanes_per_point > 512 ||
-            (x->lanes_per_point & (x->lanes_per_point - 1))) {
+        if (x->executor > PACUDA_B200_EXECUTOR_ONCHIP || (x->lanes_per_point && lane_choice(x->lanes_per_point) < 0)) {
             release();
             return PACMAN_RECURRENCE_INVALID;
         }

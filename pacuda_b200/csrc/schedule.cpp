@@ -408,8 +408,8 @@ bool build_schedule(const Program &p, uint32_t P, uint32_t A, Schedule &out) {
     return true;
 }
 
-void lane_order(const Schedule &s, uint32_t log_lanes, std::vector<uint32_t> &order, std::vector<uint32_t> &level_first) {
-    const uint32_t L = 1u << log_lanes;
+void lane_order(const Schedule &s, uint32_t lanes, std::vector<uint32_t> &order, std::vector<uint32_t> &level_first) {
+    const uint32_t L = lanes;
     order.clear();
     level_first.assign(1, 0);
     for (size_t lv = 0; lv + 1 < s.level_first.size(); lv++) {

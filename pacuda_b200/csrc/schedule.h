@@ -37,10 +37,10 @@ struct Schedule {
     std::string why;                    // empty when the schedule exists
 };
 
-// The order in which a point's L = 1 << log_lanes lanes take a level's tasks: position j of a
+// The order in which a point's L lanes take a level's tasks: position j of a
 // level goes to lane j % L, so each level is padded to whole rounds of L with ~0u (no task). The
 // tasks of a level are assigned longest first to the least loaded lane.
-void lane_order(const Schedule &s, uint32_t log_lanes, std::vector<uint32_t> &order, std::vector<uint32_t> &level_first);
+void lane_order(const Schedule &s, uint32_t lanes, std::vector<uint32_t> &order, std::vector<uint32_t> &level_first);
 
 // builds the schedule of a program; `forms` is the plan's momentum form count
 bool build_schedule(const Program &p, uint32_t current_planes, uint32_t amplitude_planes, Schedule &out);

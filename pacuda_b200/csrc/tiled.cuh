@@ -25,7 +25,8 @@ struct TiledPlan {
     const uint32_t *level_first;  // levels + 1 entries into order
     uint32_t levels;
     uint32_t cur_slots, amp_slots, forms;
-    uint32_t log_lanes;           // L = 1 << log_lanes lanes per point
+    uint32_t lanes;               // L lanes per point: 1, 2, 4, 8, 16 or a multiple of 32
+    uint32_t log_lanes;           // log2(L) when L < 32, else 5
     uint32_t point_bytes;         // shared memory of one point
     // constants: f64 (sources), the kind's layout (rows)
     const double *s64, *f64;
@@ -116,13 +117,14 @@ template <class K, bool ABI> struct SlotView {
 __device__ __forceinline__ double to_f64_value(double x) { return x; }
 __device__ __forceinline__ double to_f64_value(D x) { return __dadd_rn((double)x.hi, (double)x.lo); }
 
-// a point's lanes meet: within a warp, or at a named barrier of the point's warps
-__device__ __forceinline__ void point_sync(uint32_t log_lanes) {
-    if (log_lanes <= 5) {
+// a point's lanes meet: within a warp, or at the named barrier of the block's point `slot`
+// (barriers 1 .. 15; 0 is the block's), which its L / 32 warps arrive at
+__device__ __forceinline__ void point_sync(uint32_t lanes, uint32_t slot) {
+    if (lanes <= 32) {
         __syncwarp();
     } else {
-        uint32_t id = 1 + (threadIdx.x >> log_lanes), n = 1u << log_lanes;
-        asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory");
+        uint32_t id = 1 + slot;
+        asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(lanes) : "memory");
     }
 }
 
@@ -149,146 +151,153 @@ __global__ void __launch_bounds__(512, 1) run_tiled(TiledLaunch L) {
         const uint32_t nconst = 2 * (p.scales + p.factors);
         for (uint32_t c = threadIdx.x; c < nconst; c += blockDim.x) consts[c] = ((const Const *)p.kconst)[c];
         __syncthreads();  // the constants are in, and every thread has the item
-        const uint32_t log_l = p.log_lanes, lanes = 1u << log_l, levels = p.levels;
-        const uint32_t log_pw = log_l < 5 ? 5 - log_l : 0;  // points per region
-        const uint32_t tl = threadIdx.x & (lanes - 1);
-        const uint32_t pw = log_l < 5 ? (threadIdx.x & 31) >> log_l : 0;
-        // the region: one warp's points (L <= 32) or one point's warps (L > 32)
-        const uint32_t region = log_l < 5 ? threadIdx.x >> 5 : threadIdx.x >> log_l;
-        unsigned char *base = smem + L.const_bytes + (size_t)region * ((size_t)p.point_bytes << log_pw);
-        const uint32_t count = L.count[k];
-        const size_t first = (size_t)(item - L.item_first[k]) * (blockDim.x >> log_l);
-        const size_t mine = first + (threadIdx.x >> log_l);
-        const bool valid = mine < count;
-        const size_t point = valid ? mine : count - 1;  // padding lanes redo the last point, unwritten
-        SlotView<K, ABI> v;
-        v.cur_ = (Pair<R> *)base;
-        v.amp_ = (Pair<Amp> *)(v.cur_ + ((size_t)p.cur_slots << log_pw));
-        double *forms64 = (double *)(v.amp_ + ((size_t)p.amp_slots << log_pw));
-        v.mom = (const Den *)forms64;
-        v.sre = consts;
-        v.sim = v.sre + p.scales;
-        v.fre = v.sim + p.scales;
-        v.fim = v.fre + p.factors;
-        v.log_pw = log_pw;
-        v.pw = pw;
-        if (ABI) {
-            v.gre = valid ? (R *)L.cre : nullptr;
-            v.gim = (R *)L.cim;
-            v.ld = L.ld;
-            v.point = point;
-        }
-        // forms, f64: from the external momenta (0.0 + c0 p + c1 p + ..., in term order), or the
-        // uploaded planes
-        for (uint32_t q = tl; q < 4 * p.forms; q += lanes) {
-            uint32_t f = q >> 2, c = q & 3;
-            double val;
-            if (ABI && L.mom) {
-                val = L.mom[(size_t)q * L.ld + point];
-            } else {
-                uint32_t t0 = __ldg(p.form_terms + 2 * f), n = __ldg(p.form_terms + 2 * f + 1);
-                const double *ext = L.external[k];
-                val = 0.0;
-                for (uint32_t t = 0; t < n; t++) {
-                    double term = __dmul_rn(__ldg(p.coefficients + t0 + t),
-                                            ext[((size_t)__ldg(p.term_slots + t0 + t) * 4 + c) * count + point]);
-                    val = t == 0 ? __dadd_rn(0.0, term) : __dadd_rn(val, term);
-                }
+        // the item's geometry: L lanes per point, `per` points per block; with L < 32 a warp
+        // interleaves 32 / L points in its region, with L >= 32 a point's warps share one; the
+        // threads beyond per * L (when L does not divide the block) idle until the item's end
+        const uint32_t lanes = p.lanes, log_l = p.log_lanes, levels = p.levels;
+        const bool packed = lanes < 32;
+        const uint32_t log_pw = packed ? 5 - log_l : 0;
+        const uint32_t slot = packed ? threadIdx.x >> log_l : threadIdx.x / lanes;
+        const uint32_t tl = packed ? threadIdx.x & (lanes - 1) : threadIdx.x - slot * lanes;
+        const uint32_t pw = packed ? (threadIdx.x & 31) >> log_l : 0;
+        const uint32_t region = packed ? threadIdx.x >> 5 : slot;
+        const uint32_t per = blockDim.x / lanes;
+        if (slot < per) {
+            unsigned char *base = smem + L.const_bytes + (size_t)region * ((size_t)p.point_bytes << log_pw);
+            const uint32_t count = L.count[k];
+            const size_t first = (size_t)(item - L.item_first[k]) * per;
+            const size_t mine = first + slot;
+            const bool valid = mine < count;
+            const size_t point = valid ? mine : count - 1;  // padding lanes redo the last point, unwritten
+            SlotView<K, ABI> v;
+            v.cur_ = (Pair<R> *)base;
+            v.amp_ = (Pair<Amp> *)(v.cur_ + ((size_t)p.cur_slots << log_pw));
+            double *forms64 = (double *)(v.amp_ + ((size_t)p.amp_slots << log_pw));
+            v.mom = (const Den *)forms64;
+            v.sre = consts;
+            v.sim = v.sre + p.scales;
+            v.fre = v.sim + p.scales;
+            v.fim = v.fre + p.factors;
+            v.log_pw = log_pw;
+            v.pw = pw;
+            if (ABI) {
+                v.gre = valid ? (R *)L.cre : nullptr;
+                v.gim = (R *)L.cim;
+                v.ld = L.ld;
+                v.point = point;
             }
-            forms64[(q << log_pw) + pw] = val;
-        }
-        // the C ABI's mode: live-in currents and every amplitude from the global arena
-        if (ABI) {
-            for (uint32_t j = 0; j < p.nloads; j++) {
-                uint32_t plane = __ldg(p.loads + 3 * j), slot = __ldg(p.loads + 3 * j + 1), n = __ldg(p.loads + 3 * j + 2);
-                for (uint32_t c = tl; c < n; c += lanes)
-                    v.put(slot + c, cx(((const R *)L.cre)[(plane + c) * L.ld + point],
-                                       ((const R *)L.cim)[(plane + c) * L.ld + point]));
-            }
-            for (uint32_t a = tl; a < p.amp_slots; a += lanes) {
-                uint32_t plane = __ldg(p.amp_planes + a);
-                v.put_amp(a, ((const Amp *)L.are)[plane * L.ld + point], ((const Amp *)L.aim)[plane * L.ld + point]);
-            }
-        } else {
-            for (uint32_t a = tl; a < p.amp_slots; a += lanes) v.put_amp(a, konst<Amp>(0.0), konst<Amp>(0.0));
-        }
-        point_sync(log_l);
-        const Ins *ins = p.ins;
-        const uint2 *order = reinterpret_cast<const uint2 *>(p.order);
-        for (uint32_t lv = 0; lv < levels; lv++) {
-            uint32_t j0 = __ldg(p.level_first + lv), j1 = __ldg(p.level_first + lv + 1);
-            if (lv == 0) {
-                for (uint32_t j = j0 + tl; j < j1; j += lanes) {
-                    uint2 r = __ldg(order + j);
-                    // sources: f64 wavefunctions from the f64 forms and constants, narrowed
-                    for (uint32_t n = r.x; n < r.y; n++) {
-                        Ins o = load_ins(ins, n);
-                        double mom[4];
-                        for (int c = 0; c < 4; c++) mom[c] = forms64[((o.f * 4 + c) << log_pw) + pw];
-                        double fr = __ldg(p.f64 + o.x), fi = __ldg(p.f64 + p.factors + o.x), mass = __ldg(p.s64 + o.s);
-                        W w[4];
-                        int m = source_values(o.y, mass, mom, w);
-                        Cx<R> vals[4];
-                        for (int c = 0; c < m; c++) {
-                            double sr = fr * w[c].re - fi * w[c].im, si = fr * w[c].im + fi * w[c].re;
-                            vals[c] = cx(narrow<R>(sr), narrow<R>(si));
-                            v.put(o.a + c, vals[c]);
-                        }
-                        if (ins_flags(o) & 8) v.writeback(o.c, vals, m);
+            // forms, f64: from the external momenta (0.0 + c0 p + c1 p + ..., in term order), or the
+            // uploaded planes
+            for (uint32_t q = tl; q < 4 * p.forms; q += lanes) {
+                uint32_t f = q >> 2, c = q & 3;
+                double val;
+                if (ABI && L.mom) {
+                    val = L.mom[(size_t)q * L.ld + point];
+                } else {
+                    uint32_t t0 = __ldg(p.form_terms + 2 * f), n = __ldg(p.form_terms + 2 * f + 1);
+                    const double *ext = L.external[k];
+                    val = 0.0;
+                    for (uint32_t t = 0; t < n; t++) {
+                        double term = __dmul_rn(__ldg(p.coefficients + t0 + t),
+                                                ext[((size_t)__ldg(p.term_slots + t0 + t) * 4 + c) * count + point]);
+                        val = t == 0 ? __dadd_rn(0.0, term) : __dadd_rn(val, term);
                     }
                 }
-            } else {
-                // the next task's range is fetched while a task runs, and each next instruction
-                // while its predecessor runs
-                uint32_t j = j0 + tl;
-                uint2 r = j < j1 ? __ldg(order + j) : make_uint2(0, 0);
-                while (j < j1) {
-                    uint2 cur = r;
-                    j += lanes;
-                    if (j < j1) r = __ldg(order + j);
-                    if (cur.x == cur.y) continue;
-                    Cx<R> acc[6];
-#pragma unroll
-                    for (int c = 0; c < 6; c++) acc[c] = cx(konst<R>(0.0), konst<R>(0.0));
-                    for (uint32_t n = cur.x; n < cur.y; n++) exec_row<K>(v, load_ins(ins, n), acc);
-                }
+                forms64[(q << log_pw) + pw] = val;
             }
-            point_sync(log_l);
-            if (lv == 0 && !is_f64<Den>::value) {
-                // the forms into df64 pairs, in place
-                for (uint32_t q = tl; q < 4 * p.forms; q += lanes) {
-                    uint32_t at = (q << log_pw) + pw;
-                    reinterpret_cast<D *>(forms64)[at] = narrow<D>(forms64[at]);
+            // the C ABI's mode: live-in currents and every amplitude from the global arena
+            if (ABI) {
+                for (uint32_t j = 0; j < p.nloads; j++) {
+                    uint32_t plane = __ldg(p.loads + 3 * j), slot = __ldg(p.loads + 3 * j + 1), n = __ldg(p.loads + 3 * j + 2);
+                    for (uint32_t c = tl; c < n; c += lanes)
+                        v.put(slot + c, cx(((const R *)L.cre)[(plane + c) * L.ld + point],
+                                           ((const R *)L.cim)[(plane + c) * L.ld + point]));
                 }
-                point_sync(log_l);
-            }
-        }
-        if (ABI) {
-            if (valid)
                 for (uint32_t a = tl; a < p.amp_slots; a += lanes) {
                     uint32_t plane = __ldg(p.amp_planes + a);
-                    Amp re, im;
-                    v.amp(a, re, im);
-                    ((Amp *)L.are)[plane * L.ld + point] = re;
-                    ((Amp *)L.aim)[plane * L.ld + point] = im;
+                    v.put_amp(a, ((const Amp *)L.are)[plane * L.ld + point], ((const Amp *)L.aim)[plane * L.ld + point]);
                 }
-        } else if (valid) {
-            // the resolved reduction from zero: out[point][o] = 0 + w fma(re, re, im im) + ...
-            double *out = L.output[k] + point * p.outputs;
-            for (uint32_t o = tl; o < p.outputs; o += lanes) {
-                double acc = 0.0;
-                for (uint32_t j = __ldg(p.red_offsets + o), e = __ldg(p.red_offsets + o + 1); j < e; j++) {
-                    uint32_t s = __ldg(p.red_slots + j);
-                    double re = 0.0, im = 0.0;
-                    if (s != ~0u) {
-                        Amp ar, ai;
-                        v.amp(s, ar, ai);
-                        re = to_f64_value(ar);
-                        im = to_f64_value(ai);
+            } else {
+                for (uint32_t a = tl; a < p.amp_slots; a += lanes) v.put_amp(a, konst<Amp>(0.0), konst<Amp>(0.0));
+            }
+            point_sync(lanes, slot);
+            const Ins *ins = p.ins;
+            const uint2 *order = reinterpret_cast<const uint2 *>(p.order);
+            for (uint32_t lv = 0; lv < levels; lv++) {
+                uint32_t j0 = __ldg(p.level_first + lv), j1 = __ldg(p.level_first + lv + 1);
+                if (lv == 0) {
+                    for (uint32_t j = j0 + tl; j < j1; j += lanes) {
+                        uint2 r = __ldg(order + j);
+                        // sources: f64 wavefunctions from the f64 forms and constants, narrowed
+                        for (uint32_t n = r.x; n < r.y; n++) {
+                            Ins o = load_ins(ins, n);
+                            double mom[4];
+                            for (int c = 0; c < 4; c++) mom[c] = forms64[((o.f * 4 + c) << log_pw) + pw];
+                            double fr = __ldg(p.f64 + o.x), fi = __ldg(p.f64 + p.factors + o.x), mass = __ldg(p.s64 + o.s);
+                            W w[4];
+                            int m = source_values(o.y, mass, mom, w);
+                            Cx<R> vals[4];
+                            for (int c = 0; c < m; c++) {
+                                double sr = fr * w[c].re - fi * w[c].im, si = fr * w[c].im + fi * w[c].re;
+                                vals[c] = cx(narrow<R>(sr), narrow<R>(si));
+                                v.put(o.a + c, vals[c]);
+                            }
+                            if (ins_flags(o) & 8) v.writeback(o.c, vals, m);
+                        }
                     }
-                    acc = __dadd_rn(acc, __dmul_rn(__ldg(p.red_weights + j), __fma_rn(re, re, __dmul_rn(im, im))));
+                } else {
+                    // the next task's range is fetched while a task runs, and each next instruction
+                    // while its predecessor runs
+                    uint32_t j = j0 + tl;
+                    uint2 r = j < j1 ? __ldg(order + j) : make_uint2(0, 0);
+                    while (j < j1) {
+                        uint2 cur = r;
+                        j += lanes;
+                        if (j < j1) r = __ldg(order + j);
+                        if (cur.x == cur.y) continue;
+                        Cx<R> acc[6];
+    #pragma unroll
+                        for (int c = 0; c < 6; c++) acc[c] = cx(konst<R>(0.0), konst<R>(0.0));
+                        for (uint32_t n = cur.x; n < cur.y; n++) exec_row<K>(v, load_ins(ins, n), acc);
+                    }
                 }
-                out[o] = acc;
+                point_sync(lanes, slot);
+                if (lv == 0 && !is_f64<Den>::value) {
+                    // the forms into df64 pairs, in place
+                    for (uint32_t q = tl; q < 4 * p.forms; q += lanes) {
+                        uint32_t at = (q << log_pw) + pw;
+                        reinterpret_cast<D *>(forms64)[at] = narrow<D>(forms64[at]);
+                    }
+                    point_sync(lanes, slot);
+                }
+            }
+            if (ABI) {
+                if (valid)
+                    for (uint32_t a = tl; a < p.amp_slots; a += lanes) {
+                        uint32_t plane = __ldg(p.amp_planes + a);
+                        Amp re, im;
+                        v.amp(a, re, im);
+                        ((Amp *)L.are)[plane * L.ld + point] = re;
+                        ((Amp *)L.aim)[plane * L.ld + point] = im;
+                    }
+            } else if (valid) {
+                // the resolved reduction from zero: out[point][o] = 0 + w fma(re, re, im im) + ...
+                double *out = L.output[k] + point * p.outputs;
+                for (uint32_t o = tl; o < p.outputs; o += lanes) {
+                    double acc = 0.0;
+                    for (uint32_t j = __ldg(p.red_offsets + o), e = __ldg(p.red_offsets + o + 1); j < e; j++) {
+                        uint32_t s = __ldg(p.red_slots + j);
+                        double re = 0.0, im = 0.0;
+                        if (s != ~0u) {
+                            Amp ar, ai;
+                            v.amp(s, ar, ai);
+                            re = to_f64_value(ar);
+                            im = to_f64_value(ai);
+                        }
+                        acc = __dadd_rn(acc, __dmul_rn(__ldg(p.red_weights + j), __fma_rn(re, re, __dmul_rn(im, im))));
+                    }
+                    out[o] = acc;
+                }
             }
         }
         __syncthreads();  // the block's shared memory is free for the next item

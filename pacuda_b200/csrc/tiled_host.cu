@@ -35,7 +35,7 @@ void TiledDevice::release() {
     cudaFree(task_first);
     cudaFree(loads);
     cudaFree(amp_planes);
-    for (int k = 0; k < 10; k++) {
+    for (int k = 0; k < kLaneChoices; k++) {
         cudaFree(order[k]);
         cudaFree(level_first[k]);
         order[k] = level_first[k] = nullptr;
@@ -49,9 +49,9 @@ bool upload_schedule(TiledDevice &t, cudaStream_t s) {
     t.ok = put(&t.ins, t.host.ins, s) && put(&t.task_first, t.host.task_first, s) && put(&t.loads, t.host.loads, s) &&
            put(&t.amp_planes, t.host.amp_planes, s);
     t.levels = (uint32_t)t.host.level_first.size() - 1;
-    for (int k = 0; t.ok && k < 10; k++) {
+    for (int k = 0; t.ok && k < kLaneChoices; k++) {
         std::vector<uint32_t> order, lf, ranges;
-        lane_order(t.host, (uint32_t)k, order, lf);
+        lane_order(t.host, lanes_of_choice(k), order, lf);
         // each position holds its task's instruction range (first, end); (0, 0) for none
         ranges.reserve(2 * order.size());
         for (uint32_t task : order) {
@@ -104,26 +104,32 @@ size_t tiled_max_smem(int kernel) {
     return (size_t)smem - attr.sharedSizeBytes;
 }
 
-int tiled_min_log_lanes(size_t point_bytes, int threads, size_t max_smem) {
-    for (int lg = 0; (1 << lg) <= threads; lg++) {
-        // lanes <= 32: a warp's 32 / L points; lanes > 32: one point per L / 32 warps (named
-        // barriers 1 .. 15, so at most 15 points of more than a warp per block)
-        if (lg > 5 && (threads >> lg) > 15) continue;
-        if ((size_t)(threads >> lg) * point_bytes <= max_smem) return lg;
-    }
-    return -1;
+bool tiled_lanes_fit(uint32_t lanes, size_t point_bytes, int threads, size_t max_smem) {
+    if (lane_choice(lanes) < 0 || threads <= 0 || lanes > (uint32_t)threads) return false;
+    // lanes < 32: a warp's 32 / L points; lanes >= 32: one point per L / 32 warps
+    uint32_t per = (uint32_t)threads / lanes;
+    if (lanes > 32 && per > 15) return false;
+    return (size_t)per * point_bytes <= max_smem;
 }
 
-void describe(const TiledDevice &t, uint32_t forms, uint32_t log_lanes, size_t point_bytes, TiledPlan &p) {
+uint32_t tiled_min_lanes(size_t point_bytes, int threads, size_t max_smem) {
+    for (int c = 0; c < kLaneChoices; c++)
+        if (tiled_lanes_fit(lanes_of_choice(c), point_bytes, threads, max_smem)) return lanes_of_choice(c);
+    return 0;
+}
+
+void describe(const TiledDevice &t, uint32_t forms, uint32_t lanes, size_t point_bytes, TiledPlan &p) {
+    int choice = lane_choice(lanes);
     p.ins = t.ins;
     p.task_first = t.task_first;
-    p.order = t.order[log_lanes];
-    p.level_first = t.level_first[log_lanes];
+    p.order = t.order[choice];
+    p.level_first = t.level_first[choice];
     p.levels = t.levels;
     p.cur_slots = t.host.cur_slots;
     p.amp_slots = t.host.amp_slots;
     p.forms = forms;
-    p.log_lanes = log_lanes;
+    p.lanes = lanes;
+    p.log_lanes = lanes < 32 ? (uint32_t)choice : 5;
     p.point_bytes = (uint32_t)point_bytes;
     p.loads = t.loads;
     p.nloads = (uint32_t)t.host.loads.size() / 3;
