@@ -22,7 +22,8 @@ extern "C" {
  * reference's fields, then the executor of runs (0: the on-chip executor when a block of the
  * plan's points fits shared memory, else the global-arena one; 1: always the global-arena executor;
  * 2: the on-chip executor, or INVALID at run time when it does not fit) and the on-chip
- * executor's lanes per point (0: automatic). A runner given the reference's struct keeps the
+ * executor's lanes per point (0: automatic; as pacuda_b200_plan_set_lanes_per_point). A runner
+ * given the reference's struct keeps the
  * defaults. */
 typedef struct {
     pacman_recurrence_options base;
@@ -44,9 +45,10 @@ pacuda_b200_plan *pacuda_b200_plan_create(const pacman_recurrence_call *call, co
 void pacuda_b200_plan_destroy(pacuda_b200_plan *plan);
 /* the plan's algorithmic flops per point (fixed per-op counts) */
 uint64_t pacuda_b200_plan_flops(const pacuda_b200_plan *plan);
-/* the lanes that run one point's tasks (1, 2, 4, 8, 16, or a multiple of 32 up to 512: above 32
- * a point spans several warps), or 0 for the tuned or default choice (the fewest whose block of
- * points fits shared memory); INVALID when the block's points do not fit */
+/* the lanes that run one point's tasks: a block then runs P = threads / lanes of the plan's points
+ * at once (1 .. 64) and each gets threads / P lanes (at least `lanes`, which that returns); 0 for
+ * the tuned or default choice (the most points whose shared memory fits); INVALID when P points
+ * do not fit */
 int pacuda_b200_plan_set_lanes_per_point(pacuda_b200_plan *plan, uint32_t lanes);
 uint32_t pacuda_b200_plan_lanes_per_point(const pacuda_b200_plan *plan);
 

@@ -48,7 +48,7 @@ struct pacuda_b200_plan {
     double *coefficients = nullptr;
     uint32_t *red_offsets = nullptr, *red_slots = nullptr;
     double *red_weights = nullptr;
-    uint32_t lanes = 32;      // lanes per point (tiled_host.h: 1 .. 16 or a multiple of 32)
+    uint32_t points = 1;      // points per block (a point has the block's threads / points lanes)
     size_t point_bytes = 0;
     bool fixed = false;
 };
@@ -73,7 +73,7 @@ namespace {
 
 void fill_plan(const pacuda_b200_plan *p, TiledPlan &d) {
     memset(&d, 0, sizeof d);
-    describe(p->tiled, p->forms, p->lanes, p->point_bytes, d);
+    describe(p->tiled, p->forms, p->points, p->point_bytes, d);
     d.s64 = p->consts;
     d.f64 = p->consts + 2 * p->scales;
     d.kconst = p->consts + 2 * (p->scales + p->factors);
@@ -125,14 +125,14 @@ bool prepare(pacuda_b200_batch *b) {
     items[0] = 0;
     for (size_t k = 0; k < n; k++) {
         pacuda_b200_plan *p = b->plans[k];
-        uint32_t lo = tiled_min_lanes(p->point_bytes, b->threads, max_smem);
-        if (!lo) {
+        uint32_t most = tiled_max_points(p->point_bytes, b->threads, max_smem);
+        if (!most || p->tiled.threads != b->threads) {
             fprintf(stderr, "%s: a plan's point does not fit a block's shared memory\n", kTag);
             return false;
         }
-        if (!tiled_lanes_fit(p->lanes, p->point_bytes, b->threads, max_smem)) p->lanes = lo;
+        if (!tiled_points_fit(p->points, p->point_bytes, b->threads, max_smem)) p->points = most;
         fill_plan(p, plans[k]);
-        uint32_t per = (uint32_t)b->threads / p->lanes;
+        uint32_t per = p->points;
         b->smem = std::max<size_t>(b->smem, (size_t)per * p->point_bytes);
         items[k + 1] = items[k] + (b->count[k] + per - 1) / per;
     }
@@ -174,10 +174,10 @@ size_t point_smem(const pacuda_b200_plan *p) {
     return tiled_max_smem(p->kernel) - tiled_const_bytes(p->scales, p->factors);
 }
 
-// the fewest lanes per point whose block of points fits shared memory
-uint32_t default_lanes(const pacuda_b200_plan *p) {
-    uint32_t lo = tiled_min_lanes(p->point_bytes, tiled_threads(p->kernel), point_smem(p));
-    return lo ? lo : 32u;
+// the most points per block that fit shared memory (the fewest lanes per point)
+uint32_t default_points(const pacuda_b200_plan *p) {
+    uint32_t most = tiled_max_points(p->point_bytes, tiled_threads(p->kernel), point_smem(p));
+    return most ? most : 1u;
 }
 
 }  // namespace
@@ -257,14 +257,14 @@ extern "C" pacuda_b200_plan *pacuda_b200_plan_create(const pacman_recurrence_cal
               to_device(&p->coefficients, c->term_coefficients, c->term_count) &&
               to_device(&p->red_offsets, offsets, (size_t)outputs + 1) &&
               to_device(&p->red_slots, slots.data(), slots.size()) &&
-              to_device(&p->red_weights, weights, offsets[outputs]) && upload_schedule(p->tiled, 0) &&
+              to_device(&p->red_weights, weights, offsets[outputs]) && upload_schedule(p->tiled, tiled_threads(p->kernel), 0) &&
               !failed(cudaDeviceSynchronize(), "plan upload");
     if (!ok) {
         pacuda_b200_plan_destroy(p);
         return nullptr;
     }
     p->point_bytes = tiled_point_bytes(p->tiled.host, forms, p->kernel);
-    p->lanes = default_lanes(p);
+    p->points = default_points(p);
     return p;
 }
 
@@ -286,16 +286,20 @@ extern "C" int pacuda_b200_plan_set_lanes_per_point(pacuda_b200_plan *p, uint32_
     if (!p) return PACMAN_RECURRENCE_INVALID;
     if (lanes == 0) {
         p->fixed = false;
-        p->lanes = default_lanes(p);
+        p->points = default_points(p);
         return PACMAN_RECURRENCE_OK;
     }
-    if (!tiled_lanes_fit(lanes, p->point_bytes, tiled_threads(p->kernel), point_smem(p))) return PACMAN_RECURRENCE_INVALID;
-    p->lanes = lanes;
+    int threads = tiled_threads(p->kernel);
+    uint32_t points = lanes <= (uint32_t)threads ? (uint32_t)threads / lanes : 0;
+    if (!tiled_points_fit(points, p->point_bytes, threads, point_smem(p))) return PACMAN_RECURRENCE_INVALID;
+    p->points = points;
     p->fixed = true;
     return PACMAN_RECURRENCE_OK;
 }
 
-extern "C" uint32_t pacuda_b200_plan_lanes_per_point(const pacuda_b200_plan *p) { return p ? p->lanes : 0; }
+extern "C" uint32_t pacuda_b200_plan_lanes_per_point(const pacuda_b200_plan *p) {
+    return p ? (uint32_t)p->tiled.threads / p->points : 0;
+}
 
 extern "C" pacuda_b200_batch *pacuda_b200_batch_create(pacuda_b200_plan *const *plans, uint32_t nplans,
                                                        const double *const *external, const uint32_t *count,
@@ -371,12 +375,13 @@ extern "C" int pacuda_b200_batch_tune(pacuda_b200_batch *b, void *stream) {
         const double *ext[1] = {b->external[k]};
         double *out[1] = {b->output[k]};
         float best = 1e30f;
-        uint32_t best_lanes = p->lanes;
+        uint32_t best_points = p->points;
         int threads = tiled_threads(p->kernel);
-        for (int choice = 0; choice < kLaneChoices; choice++) {
-            uint32_t lanes = lanes_of_choice(choice);
-            if (!tiled_lanes_fit(lanes, p->point_bytes, threads, point_smem(p))) continue;
-            p->lanes = lanes;
+        // from the most points per block that fit down to half of them (fewer points leave more
+        // of the block's lanes idle at the levels' barriers)
+        uint32_t most = tiled_max_points(p->point_bytes, threads, point_smem(p));
+        for (uint32_t points = most; points >= 1 && 2 * points >= most; points--) {
+            p->points = points;
             uint32_t n = b->count[k];
             pacuda_b200_batch *tb = pacuda_b200_batch_create(one, 1, ext, &n, out);
             if (!tb) continue;
@@ -394,10 +399,10 @@ extern "C" int pacuda_b200_batch_tune(pacuda_b200_batch *b, void *stream) {
             pacuda_b200_batch_destroy(tb);
             if (ok && ms < best) {
                 best = ms;
-                best_lanes = lanes;
+                best_points = points;
             }
         }
-        p->lanes = best_lanes;
+        p->points = best_points;
         (void)sample;
     }
     cudaEventDestroy(t0);
@@ -513,15 +518,14 @@ extern "C" int pacuda_b200_run_static(pacuda_b200_plan *const *plans, uint32_t n
     size_t smem = 0;
     for (uint32_t k = 0; k < nplans; k++) {
         const pacuda_b200_plan *p = plans[k];
-        uint32_t lo = tiled_min_lanes(p->point_bytes, threads, max_smem);
-        if (!lo) {
+        uint32_t most = tiled_max_points(p->point_bytes, threads, max_smem);
+        if (!most || p->tiled.threads != threads) {
             fprintf(stderr, "%s: run_static: a plan's point does not fit a block's shared memory\n", kTag);
             return PACMAN_RECURRENCE_INVALID;
         }
-        uint32_t lanes = tiled_lanes_fit(p->lanes, p->point_bytes, threads, max_smem) ? p->lanes : lo;
+        uint32_t per = tiled_points_fit(p->points, p->point_bytes, threads, max_smem) ? p->points : most;
         fill_plan(p, block.plans[k]);
-        describe(p->tiled, p->forms, lanes, p->point_bytes, block.plans[k]);
-        uint32_t per = (uint32_t)threads / lanes;
+        describe(p->tiled, p->forms, per, p->point_bytes, block.plans[k]);
         smem = std::max<size_t>(smem, (size_t)per * p->point_bytes);
         block.items[k + 1] = block.items[k] + (count[k] + per - 1) / per;
         block.external[k] = external[k];

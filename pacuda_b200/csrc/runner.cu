@@ -373,7 +373,7 @@ int onchip_launch(DeviceProgram *prog, const pacman_recurrence_call *c, const Ru
     if (prog->tiled_state == 0) {
         prog->tiled_state = -1;
         if (build_schedule(prog->host, c->current_planes, c->amplitude_planes, prog->tiled.host) &&
-            upload_schedule(prog->tiled, dev.stream))
+            upload_schedule(prog->tiled, tiled_threads(kernel), dev.stream))
             prog->tiled_state = 1;
     }
     // the lanes per point: as configured, else the fewest whose block of points fits
@@ -381,11 +381,13 @@ int onchip_launch(DeviceProgram *prog, const pacman_recurrence_call *c, const Ru
     size_t pb = prog->tiled_state == 1 ? tiled_point_bytes(prog->tiled.host, forms, kernel) : 0;
     size_t cb = tiled_const_bytes(c->scale_count, c->factor_count);
     size_t room = threads ? tiled_max_smem(kernel) - cb : 0;
-    uint32_t lanes = threads ? tiled_min_lanes(pb, threads, room) : 0;
-    if (lanes && current.lanes_per_point)
-        lanes = tiled_lanes_fit(current.lanes_per_point, pb, threads, room) ? current.lanes_per_point : 0;
-    if (!lanes) return current.executor == PACUDA_B200_EXECUTOR_ONCHIP ? 2 : 0;
-    size_t smem = cb + (size_t)(threads / lanes) * pb;
+    uint32_t np = threads && prog->tiled.threads == threads ? tiled_max_points(pb, threads, room) : 0;
+    if (np && current.lanes_per_point) {
+        uint32_t want = current.lanes_per_point <= (uint32_t)threads ? (uint32_t)threads / current.lanes_per_point : 0;
+        np = tiled_points_fit(want, pb, threads, room) ? want : 0;
+    }
+    if (!np) return current.executor == PACUDA_B200_EXECUTOR_ONCHIP ? 2 : 0;
+    size_t smem = cb + (size_t)np * pb;
     // descriptors: TiledPlan | item_first[2] | external[1] | count[1] | counter
     const size_t o_items = (sizeof(TiledPlan) + 15) / 16 * 16, o_ext = o_items + 16, o_count = o_ext + 8,
                  o_counter = (o_count + 4 + 15) / 16 * 16, total = o_counter + 16;
@@ -393,7 +395,7 @@ int onchip_launch(DeviceProgram *prog, const pacman_recurrence_call *c, const Ru
     if (!dev.launch_dev.reserve(total, "descriptors")) return -1;
     memset(dev.launch_host, 0, total);
     TiledPlan &p = *(TiledPlan *)dev.launch_host;
-    describe(prog->tiled, forms, lanes, pb, p);
+    describe(prog->tiled, forms, np, pb, p);
     p.s64 = a.s64;
     p.f64 = a.f64;
     p.kconst = a.kconst;
@@ -404,7 +406,7 @@ int onchip_launch(DeviceProgram *prog, const pacman_recurrence_call *c, const Ru
     p.coefficients = a.coefficients;
     unsigned long long *items = (unsigned long long *)(dev.launch_host + o_items);
     items[0] = 0;
-    uint32_t per = (uint32_t)threads / lanes;
+    uint32_t per = np;
     items[1] = (a.points + per - 1) / per;
     *(const double **)(dev.launch_host + o_ext) = a.external;
     *(uint32_t *)(dev.launch_host + o_count) = a.points;
@@ -849,7 +851,7 @@ extern "C" int pacman_recurrence_v1_configure(const pacman_recurrence_options *o
     n.sort = !o->no_sort;
     if (o->struct_size >= sizeof(pacuda_b200_options)) {
         const pacuda_b200_options *x = (const pacuda_b200_options *)o;
-        if (x->executor > PACUDA_B200_EXECUTOR_ONCHIP || (x->lanes_per_point && lane_choice(x->lanes_per_point) < 0)) {
+        if (x->executor > PACUDA_B200_EXECUTOR_ONCHIP || x->lanes_per_point > 512) {
             release();
             return PACMAN_RECURRENCE_INVALID;
         }

@@ -4,10 +4,12 @@
 // the outputs go out (in the C ABI's mode also the arena's live-in planes in and its written
 // planes out).
 //
-// A point has L lanes (a power of two, 1 .. the block's threads). With L <= 32 a warp holds
-// 32 / L points, interleaved in its shared memory as [slot][point]; with L > 32 a point spans
-// L / 32 warps that meet at a named barrier. A block takes one work item at a time: one plan's
-// next (threads / L) points.
+// A block runs P points at once with G = threads / P lanes each. Thread t serves point t % P as
+// lane t / P: the P threads of a lane run the same task on consecutive points, so their
+// instruction fetches are one broadcast, their shared-memory values ([slot][P], interleaved) are
+// contiguous, and their global stores cover P consecutive points of a plane. All points take the
+// same lane order, so a block's points move through the levels together and meet at the block's
+// barrier. A block takes one work item at a time: one plan's next P points.
 #pragma once
 #include <stdint.h>
 
@@ -21,12 +23,12 @@ struct TiledPlan {
     // the schedule
     const Ins *ins;
     const uint32_t *task_first;   // per task, its instructions (tasks + 1 entries)
-    const uint32_t *order;        // per level position, its task's (first, end) instructions; lane = position % L
+    const uint32_t *order;        // per level position, its task's (first, end) instructions; lane = position % G
     const uint32_t *level_first;  // levels + 1 entries into order
     uint32_t levels;
     uint32_t cur_slots, amp_slots, forms;
-    uint32_t lanes;               // L lanes per point: 1, 2, 4, 8, 16 or a multiple of 32
-    uint32_t log_lanes;           // log2(L) when L < 32, else 5
+    uint32_t points;              // P points per block
+    uint32_t lanes;               // G lanes per point (the block's threads / P)
     uint32_t point_bytes;         // shared memory of one point
     // constants: f64 (sources), the kind's layout (rows)
     const double *s64, *f64;
@@ -67,6 +69,16 @@ template <class R> struct alignas(2 * sizeof(R)) Pair {
     R re, im;
 };
 
+// the C ABI's mode: where an item's points write their planes back (thread 0 sets it per item;
+// in shared memory so that no lane holds these in registers through its tasks)
+struct AbiItem {
+    void *cre, *cim;
+    size_t ld;
+    unsigned long long first;  // the item's first point
+    uint32_t count;            // the plan's points
+};
+static __shared__ AbiItem abi_item;
+
 template <class K, bool ABI> struct SlotView {
     typedef typename K::R R;
     typedef typename K::Den Den;
@@ -76,11 +88,8 @@ template <class K, bool ABI> struct SlotView {
     Pair<Amp> *amp_;      // [amplitude slot][points of the region]
     const Den *mom;
     const Const *sre, *sim, *fre, *fim;  // the plan's constants, in shared memory
-    uint32_t log_pw, pw;  // points interleaved in the region (1 << log_pw) and this lane's
-    // write-back to the global arena (the C ABI's mode), else null
-    R *gre, *gim;
-    size_t ld, point;
-    __device__ __forceinline__ uint32_t at(uint32_t slot) const { return (slot << log_pw) + pw; }
+    uint32_t np, pw;      // the block's points (interleaved) and this thread's
+    __device__ __forceinline__ uint32_t at(uint32_t slot) const { return slot * np + pw; }
     __device__ __forceinline__ Cx<R> cur(uint32_t slot) const {
         Pair<R> v = cur_[at(slot)];
         return cx(v.re, v.im);
@@ -106,27 +115,22 @@ template <class K, bool ABI> struct SlotView {
         amp_[at(a)] = x;
     }
     __device__ __forceinline__ void writeback(uint32_t plane, const Cx<R> *v, int n) const {
-        if (ABI && gre)
-            for (int k = 0; k < n; k++) {
-                gre[(plane + k) * ld + point] = v[k].re;
-                gim[(plane + k) * ld + point] = v[k].im;
+        if (ABI) {
+            const unsigned long long point = abi_item.first + pw;
+            if (point < abi_item.count) {
+                R *re = (R *)abi_item.cre, *im = (R *)abi_item.cim;
+                const size_t ld = abi_item.ld;
+                for (int k = 0; k < n; k++) {
+                    re[(plane + k) * ld + point] = v[k].re;
+                    im[(plane + k) * ld + point] = v[k].im;
+                }
             }
+        }
     }
 };
 
 __device__ __forceinline__ double to_f64_value(double x) { return x; }
 __device__ __forceinline__ double to_f64_value(D x) { return __dadd_rn((double)x.hi, (double)x.lo); }
-
-// a point's lanes meet: within a warp, or at the named barrier of the block's point `slot`
-// (barriers 1 .. 15; 0 is the block's), which its L / 32 warps arrive at
-__device__ __forceinline__ void point_sync(uint32_t lanes, uint32_t slot) {
-    if (lanes <= 32) {
-        __syncwarp();
-    } else {
-        uint32_t id = 1 + slot;
-        asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(lanes) : "memory");
-    }
-}
 
 // ABI: the C ABI's mode (arena in and out) or a batch's (outputs only)
 template <class K, bool ABI>
@@ -146,48 +150,38 @@ __global__ void __launch_bounds__(512, 1) run_tiled(TiledLaunch L) {
         uint32_t k = 0;
         while (item >= L.item_first[k + 1]) k++;
         const TiledPlan &p = L.plans[k];
+        const uint32_t np = p.points, lanes = p.lanes, levels = p.levels;
+        if (ABI && threadIdx.x == 0) {
+            abi_item.cre = L.cre;
+            abi_item.cim = L.cim;
+            abi_item.ld = L.ld;
+            abi_item.first = (item - L.item_first[k]) * np;
+            abi_item.count = L.count[k];
+        }
         // the plan's constants (the kind's layout) into shared memory
         Const *consts = (Const *)smem;
         const uint32_t nconst = 2 * (p.scales + p.factors);
         for (uint32_t c = threadIdx.x; c < nconst; c += blockDim.x) consts[c] = ((const Const *)p.kconst)[c];
-        __syncthreads();  // the constants are in, and every thread has the item
-        // the item's geometry: L lanes per point, `per` points per block; with L < 32 a warp
-        // interleaves 32 / L points in its region, with L >= 32 a point's warps share one; the
-        // threads beyond per * L (when L does not divide the block) idle until the item's end
-        const uint32_t lanes = p.lanes, log_l = p.log_lanes, levels = p.levels;
-        const bool packed = lanes < 32;
-        const uint32_t log_pw = packed ? 5 - log_l : 0;
-        const uint32_t slot = packed ? threadIdx.x >> log_l : threadIdx.x / lanes;
-        const uint32_t tl = packed ? threadIdx.x & (lanes - 1) : threadIdx.x - slot * lanes;
-        const uint32_t pw = packed ? (threadIdx.x & 31) >> log_l : 0;
-        const uint32_t region = packed ? threadIdx.x >> 5 : slot;
-        const uint32_t per = blockDim.x / lanes;
-        if (slot < per) {
-            unsigned char *base = smem + L.const_bytes + (size_t)region * ((size_t)p.point_bytes << log_pw);
+        // this thread: lane tl of point pw; the threads beyond np * lanes only meet the barriers
+        const uint32_t tl = threadIdx.x / np, pw = threadIdx.x - tl * np;
+        const bool active = tl < lanes;
+        SlotView<K, ABI> v;
+        v.cur_ = (Pair<R> *)(smem + L.const_bytes);
+        v.amp_ = (Pair<Amp> *)(v.cur_ + (size_t)p.cur_slots * np);
+        double *forms64 = (double *)(v.amp_ + (size_t)p.amp_slots * np);
+        v.mom = (const Den *)forms64;
+        v.sre = consts;
+        v.sim = v.sre + p.scales;
+        v.fre = v.sim + p.scales;
+        v.fim = v.fre + p.factors;
+        v.np = np;
+        v.pw = pw;
+        if (active) {
             const uint32_t count = L.count[k];
-            const size_t first = (size_t)(item - L.item_first[k]) * per;
-            const size_t mine = first + slot;
-            const bool valid = mine < count;
-            const size_t point = valid ? mine : count - 1;  // padding lanes redo the last point, unwritten
-            SlotView<K, ABI> v;
-            v.cur_ = (Pair<R> *)base;
-            v.amp_ = (Pair<Amp> *)(v.cur_ + ((size_t)p.cur_slots << log_pw));
-            double *forms64 = (double *)(v.amp_ + ((size_t)p.amp_slots << log_pw));
-            v.mom = (const Den *)forms64;
-            v.sre = consts;
-            v.sim = v.sre + p.scales;
-            v.fre = v.sim + p.scales;
-            v.fim = v.fre + p.factors;
-            v.log_pw = log_pw;
-            v.pw = pw;
-            if (ABI) {
-                v.gre = valid ? (R *)L.cre : nullptr;
-                v.gim = (R *)L.cim;
-                v.ld = L.ld;
-                v.point = point;
-            }
-            // forms, f64: from the external momenta (0.0 + c0 p + c1 p + ..., in term order), or the
-            // uploaded planes
+            const size_t mine = (size_t)(item - L.item_first[k]) * np + pw;
+            const size_t point = mine < count ? mine : count - 1;  // padding points redo the last point, unwritten
+            // forms, f64: from the external momenta (0.0 + c0 p + c1 p + ..., in term order), or
+            // the uploaded planes
             for (uint32_t q = tl; q < 4 * p.forms; q += lanes) {
                 uint32_t f = q >> 2, c = q & 3;
                 double val;
@@ -203,7 +197,7 @@ __global__ void __launch_bounds__(512, 1) run_tiled(TiledLaunch L) {
                         val = t == 0 ? __dadd_rn(0.0, term) : __dadd_rn(val, term);
                     }
                 }
-                forms64[(q << log_pw) + pw] = val;
+                forms64[q * np + pw] = val;
             }
             // the C ABI's mode: live-in currents and every amplitude from the global arena
             if (ABI) {
@@ -220,84 +214,87 @@ __global__ void __launch_bounds__(512, 1) run_tiled(TiledLaunch L) {
             } else {
                 for (uint32_t a = tl; a < p.amp_slots; a += lanes) v.put_amp(a, konst<Amp>(0.0), konst<Amp>(0.0));
             }
-            point_sync(lanes, slot);
-            const Ins *ins = p.ins;
-            const uint2 *order = reinterpret_cast<const uint2 *>(p.order);
-            for (uint32_t lv = 0; lv < levels; lv++) {
-                uint32_t j0 = __ldg(p.level_first + lv), j1 = __ldg(p.level_first + lv + 1);
-                if (lv == 0) {
-                    for (uint32_t j = j0 + tl; j < j1; j += lanes) {
-                        uint2 r = __ldg(order + j);
-                        // sources: f64 wavefunctions from the f64 forms and constants, narrowed
-                        for (uint32_t n = r.x; n < r.y; n++) {
-                            Ins o = load_ins(ins, n);
-                            double mom[4];
-                            for (int c = 0; c < 4; c++) mom[c] = forms64[((o.f * 4 + c) << log_pw) + pw];
-                            double fr = __ldg(p.f64 + o.x), fi = __ldg(p.f64 + p.factors + o.x), mass = __ldg(p.s64 + o.s);
-                            W w[4];
-                            int m = source_values(o.y, mass, mom, w);
-                            Cx<R> vals[4];
-                            for (int c = 0; c < m; c++) {
-                                double sr = fr * w[c].re - fi * w[c].im, si = fr * w[c].im + fi * w[c].re;
-                                vals[c] = cx(narrow<R>(sr), narrow<R>(si));
-                                v.put(o.a + c, vals[c]);
-                            }
-                            if (ins_flags(o) & 8) v.writeback(o.c, vals, m);
+        }
+        __syncthreads();  // the constants, forms and live-in values are in
+        const Ins *ins = p.ins;
+        const uint2 *order = reinterpret_cast<const uint2 *>(p.order);
+        for (uint32_t lv = 0; lv < levels; lv++) {
+            const uint32_t j0 = __ldg(p.level_first + lv), j1 = active ? __ldg(p.level_first + lv + 1) : 0;
+            if (lv == 0) {
+                for (uint32_t j = j0 + tl; j < j1; j += lanes) {
+                    uint2 r = __ldg(order + j);
+                    // sources: f64 wavefunctions from the f64 forms and constants, narrowed
+                    for (uint32_t n = r.x; n < r.y; n++) {
+                        Ins o = load_ins(ins, n);
+                        double mom[4];
+                        for (int c = 0; c < 4; c++) mom[c] = forms64[(o.f * 4 + c) * np + pw];
+                        double fr = __ldg(p.f64 + o.x), fi = __ldg(p.f64 + p.factors + o.x), mass = __ldg(p.s64 + o.s);
+                        W w[4];
+                        int m = source_values(o.y, mass, mom, w);
+                        Cx<R> vals[4];
+                        for (int c = 0; c < m; c++) {
+                            double sr = fr * w[c].re - fi * w[c].im, si = fr * w[c].im + fi * w[c].re;
+                            vals[c] = cx(narrow<R>(sr), narrow<R>(si));
+                            v.put(o.a + c, vals[c]);
                         }
-                    }
-                } else {
-                    // the next task's range is fetched while a task runs, and each next instruction
-                    // while its predecessor runs
-                    uint32_t j = j0 + tl;
-                    uint2 r = j < j1 ? __ldg(order + j) : make_uint2(0, 0);
-                    while (j < j1) {
-                        uint2 cur = r;
-                        j += lanes;
-                        if (j < j1) r = __ldg(order + j);
-                        if (cur.x == cur.y) continue;
-                        Cx<R> acc[6];
-    #pragma unroll
-                        for (int c = 0; c < 6; c++) acc[c] = cx(konst<R>(0.0), konst<R>(0.0));
-                        for (uint32_t n = cur.x; n < cur.y; n++) exec_row<K>(v, load_ins(ins, n), acc);
+                        if (ins_flags(o) & 8) v.writeback(o.c, vals, m);
                     }
                 }
-                point_sync(lanes, slot);
-                if (lv == 0 && !is_f64<Den>::value) {
-                    // the forms into df64 pairs, in place
-                    for (uint32_t q = tl; q < 4 * p.forms; q += lanes) {
-                        uint32_t at = (q << log_pw) + pw;
-                        reinterpret_cast<D *>(forms64)[at] = narrow<D>(forms64[at]);
-                    }
-                    point_sync(lanes, slot);
+            } else {
+                // the next task's range is fetched while a task runs
+                uint32_t j = j0 + tl;
+                uint2 r = j < j1 ? __ldg(order + j) : make_uint2(0, 0);
+                while (j < j1) {
+                    uint2 cur = r;
+                    j += lanes;
+                    if (j < j1) r = __ldg(order + j);
+                    if (cur.x == cur.y) continue;
+                    Cx<R> acc[6];
+#pragma unroll
+                    for (int c = 0; c < 6; c++) acc[c] = cx(konst<R>(0.0), konst<R>(0.0));
+                    for (uint32_t n = cur.x; n < cur.y; n++) exec_row<K>(v, load_ins(ins, n), acc);
                 }
             }
-            if (ABI) {
-                if (valid)
-                    for (uint32_t a = tl; a < p.amp_slots; a += lanes) {
-                        uint32_t plane = __ldg(p.amp_planes + a);
-                        Amp re, im;
-                        v.amp(a, re, im);
-                        ((Amp *)L.are)[plane * L.ld + point] = re;
-                        ((Amp *)L.aim)[plane * L.ld + point] = im;
+            __syncthreads();
+            if (lv == 0 && !is_f64<Den>::value) {
+                // the forms into df64 pairs, in place
+                if (active)
+                    for (uint32_t q = tl; q < 4 * p.forms; q += lanes) {
+                        uint32_t at = q * np + pw;
+                        reinterpret_cast<D *>(forms64)[at] = narrow<D>(forms64[at]);
                     }
-            } else if (valid) {
-                // the resolved reduction from zero: out[point][o] = 0 + w fma(re, re, im im) + ...
-                double *out = L.output[k] + point * p.outputs;
-                for (uint32_t o = tl; o < p.outputs; o += lanes) {
-                    double acc = 0.0;
-                    for (uint32_t j = __ldg(p.red_offsets + o), e = __ldg(p.red_offsets + o + 1); j < e; j++) {
-                        uint32_t s = __ldg(p.red_slots + j);
-                        double re = 0.0, im = 0.0;
-                        if (s != ~0u) {
-                            Amp ar, ai;
-                            v.amp(s, ar, ai);
-                            re = to_f64_value(ar);
-                            im = to_f64_value(ai);
-                        }
-                        acc = __dadd_rn(acc, __dmul_rn(__ldg(p.red_weights + j), __fma_rn(re, re, __dmul_rn(im, im))));
-                    }
-                    out[o] = acc;
+                __syncthreads();
+            }
+        }
+        if (ABI) {
+            // (the point again from the item: nothing of it stays in registers through the levels)
+            const unsigned long long at = abi_item.first + pw;
+            if (active && at < abi_item.count)
+                for (uint32_t a = tl; a < p.amp_slots; a += lanes) {
+                    uint32_t plane = __ldg(p.amp_planes + a);
+                    Amp re, im;
+                    v.amp(a, re, im);
+                    ((Amp *)L.are)[plane * L.ld + at] = re;
+                    ((Amp *)L.aim)[plane * L.ld + at] = im;
                 }
+        } else if (active && (size_t)(item - L.item_first[k]) * np + pw < L.count[k]) {
+            // the resolved reduction from zero: out[point][o] = 0 + w fma(re, re, im im) + ...
+            const size_t point = (size_t)(item - L.item_first[k]) * np + pw;
+            double *out = L.output[k] + point * p.outputs;
+            for (uint32_t o = tl; o < p.outputs; o += lanes) {
+                double acc = 0.0;
+                for (uint32_t j = __ldg(p.red_offsets + o), e = __ldg(p.red_offsets + o + 1); j < e; j++) {
+                    uint32_t s = __ldg(p.red_slots + j);
+                    double re = 0.0, im = 0.0;
+                    if (s != ~0u) {
+                        Amp ar, ai;
+                        v.amp(s, ar, ai);
+                        re = to_f64_value(ar);
+                        im = to_f64_value(ai);
+                    }
+                    acc = __dadd_rn(acc, __dmul_rn(__ldg(p.red_weights + j), __fma_rn(re, re, __dmul_rn(im, im))));
+                }
+                out[o] = acc;
             }
         }
         __syncthreads();  // the block's shared memory is free for the next item

@@ -35,31 +35,32 @@ void TiledDevice::release() {
     cudaFree(task_first);
     cudaFree(loads);
     cudaFree(amp_planes);
-    for (int k = 0; k < kLaneChoices; k++) {
-        cudaFree(order[k]);
-        cudaFree(level_first[k]);
-        order[k] = level_first[k] = nullptr;
-    }
+    cudaFree(orders);
+    cudaFree(level_firsts);
     ins = nullptr;
-    task_first = loads = amp_planes = nullptr;
+    task_first = loads = amp_planes = orders = level_firsts = nullptr;
     ok = false;
 }
 
-bool upload_schedule(TiledDevice &t, cudaStream_t s) {
-    t.ok = put(&t.ins, t.host.ins, s) && put(&t.task_first, t.host.task_first, s) && put(&t.loads, t.host.loads, s) &&
-           put(&t.amp_planes, t.host.amp_planes, s);
+bool upload_schedule(TiledDevice &t, int threads, cudaStream_t s) {
+    t.ok = threads > 0 && put(&t.ins, t.host.ins, s) && put(&t.task_first, t.host.task_first, s) &&
+           put(&t.loads, t.host.loads, s) && put(&t.amp_planes, t.host.amp_planes, s);
     t.levels = (uint32_t)t.host.level_first.size() - 1;
-    for (int k = 0; t.ok && k < kLaneChoices; k++) {
-        std::vector<uint32_t> order, lf, ranges;
-        lane_order(t.host, lanes_of_choice(k), order, lf);
+    t.threads = threads;
+    std::vector<uint32_t> ranges, firsts;
+    for (uint32_t np = 1; t.ok && np <= kMaxPoints; np++) {
+        std::vector<uint32_t> order, lf;
+        lane_order(t.host, std::max(1u, (uint32_t)threads / np), order, lf);
         // each position holds its task's instruction range (first, end); (0, 0) for none
-        ranges.reserve(2 * order.size());
+        t.order_at[np - 1] = ranges.size();
+        t.level_at[np - 1] = firsts.size();
         for (uint32_t task : order) {
             ranges.push_back(task == ~0u ? 0 : t.host.task_first[task]);
             ranges.push_back(task == ~0u ? 0 : t.host.task_first[task + 1]);
         }
-        t.ok = put(&t.order[k], ranges, s) && put(&t.level_first[k], lf, s);
+        firsts.insert(firsts.end(), lf.begin(), lf.end());
     }
+    t.ok = t.ok && put(&t.orders, ranges, s) && put(&t.level_firsts, firsts, s);
     // the host vectors must outlive the asynchronous copies
     cudaStreamSynchronize(s);
     return t.ok;
@@ -86,10 +87,7 @@ int tiled_threads(int kernel) {
     int per_warp = ((attr.numRegs * 32 + 255) / 256) * 256;
     int warps = per_warp ? regs / per_warp : 16;
     warps = std::min(warps, attr.maxThreadsPerBlock / 32);
-    // a power of two of warps: points (and their barriers) tile the block evenly
-    int w = 1;
-    while (2 * w <= std::min(warps, 16)) w *= 2;
-    return 32 * w;
+    return 32 * std::max(1, std::min(warps, 16));
 }
 
 size_t tiled_max_smem(int kernel) {
@@ -104,32 +102,28 @@ size_t tiled_max_smem(int kernel) {
     return (size_t)smem - attr.sharedSizeBytes;
 }
 
-bool tiled_lanes_fit(uint32_t lanes, size_t point_bytes, int threads, size_t max_smem) {
-    if (lane_choice(lanes) < 0 || threads <= 0 || lanes > (uint32_t)threads) return false;
-    // lanes < 32: a warp's 32 / L points; lanes >= 32: one point per L / 32 warps
-    uint32_t per = (uint32_t)threads / lanes;
-    if (lanes > 32 && per > 15) return false;
-    return (size_t)per * point_bytes <= max_smem;
+bool tiled_points_fit(uint32_t points, size_t point_bytes, int threads, size_t max_smem) {
+    return points >= 1 && points <= kMaxPoints && threads > 0 && points <= (uint32_t)threads &&
+           (size_t)points * point_bytes <= max_smem;
 }
 
-uint32_t tiled_min_lanes(size_t point_bytes, int threads, size_t max_smem) {
-    for (int c = 0; c < kLaneChoices; c++)
-        if (tiled_lanes_fit(lanes_of_choice(c), point_bytes, threads, max_smem)) return lanes_of_choice(c);
+uint32_t tiled_max_points(size_t point_bytes, int threads, size_t max_smem) {
+    for (uint32_t np = kMaxPoints; np >= 1; np--)
+        if (tiled_points_fit(np, point_bytes, threads, max_smem)) return np;
     return 0;
 }
 
-void describe(const TiledDevice &t, uint32_t forms, uint32_t lanes, size_t point_bytes, TiledPlan &p) {
-    int choice = lane_choice(lanes);
+void describe(const TiledDevice &t, uint32_t forms, uint32_t points, size_t point_bytes, TiledPlan &p) {
     p.ins = t.ins;
     p.task_first = t.task_first;
-    p.order = t.order[choice];
-    p.level_first = t.level_first[choice];
+    p.order = t.orders + t.order_at[points - 1];
+    p.level_first = t.level_firsts + t.level_at[points - 1];
     p.levels = t.levels;
     p.cur_slots = t.host.cur_slots;
     p.amp_slots = t.host.amp_slots;
     p.forms = forms;
-    p.lanes = lanes;
-    p.log_lanes = lanes < 32 ? (uint32_t)choice : 5;
+    p.points = points;
+    p.lanes = std::max(1u, (uint32_t)t.threads / points);
     p.point_bytes = (uint32_t)point_bytes;
     p.loads = t.loads;
     p.nloads = (uint32_t)t.host.loads.size() / 3;

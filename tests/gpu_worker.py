@@ -1,6 +1,6 @@
 """Runs the shared scenarios on a runner library in this process and saves what came back.
 
-usage: python tests/gpu_worker.py LIB KERNEL OUT.npz [nosort] [arena|onchip]
+usage: python tests/gpu_worker.py LIB KERNEL OUT.npz [nosort] [arena|onchip] [lanes=N]
 
 One process per kernel kind, since a runner takes its configuration once, before its first run.
 LIB is this package's librecurrence.so or the reference runner built from its sources.
@@ -20,8 +20,12 @@ def main():
     lib, kernel, path = sys.argv[1], sys.argv[2], sys.argv[3]
     no_sort = "nosort" in sys.argv[4:]
     executor = "arena" if "arena" in sys.argv[4:] else "onchip" if "onchip" in sys.argv[4:] else None
+    lanes = [int(a[6:]) for a in sys.argv[4:] if a.startswith("lanes=")]
     r = Runner(lib)
-    assert r.configure(kernel, no_sort=no_sort, executor=executor) == 0
+    if lanes:
+        assert r.configure(kernel, no_sort=no_sort, executor=executor, lanes_per_point=lanes[0]) == 0
+    else:
+        assert r.configure(kernel, no_sort=no_sort, executor=executor) == 0
     res = {}
     for seed in S.FUZZ_SEEDS:
         a = S.fuzz_args(seed)

@@ -24,14 +24,15 @@ KINDS = ["f64", "df64", "mixed", "mixed64"]
 _cache = {}
 
 
-def worker(lib, kind, nosort=False, executor=None):
-    key = (lib, kind, nosort, executor)
+def worker(lib, kind, nosort=False, executor=None, lanes=0):
+    key = (lib, kind, nosort, executor, lanes)
     if key not in _cache:
-        tag = f"{os.path.basename(os.path.dirname(lib))}_{kind}{'_nosort' if nosort else ''}{'_' + executor if executor else ''}"
+        tag = f"{os.path.basename(os.path.dirname(lib))}_{kind}{'_nosort' if nosort else ''}{'_' + executor if executor else ''}" \
+            f"{f'_lanes{lanes}' if lanes else ''}"
         out = os.path.join(ROOT, "gpurun_out", f"parity_{tag}.npz") if os.path.isdir(os.path.join(ROOT, "gpurun_out")) \
             else f"/tmp/parity_{tag}.npz"
         cmd = [sys.executable, os.path.join(ROOT, "tests", "gpu_worker.py"), lib, kind, out] + (["nosort"] if nosort else []) \
-            + ([executor] if executor else [])
+            + ([executor] if executor else []) + ([f"lanes={lanes}"] if lanes else [])
         subprocess.run(cmd, check=True, timeout=600)
         _cache[key] = dict(np.load(out))
     return _cache[key]
@@ -117,6 +118,14 @@ def test_runner_matches_oracle_bitwise(kind):
 @pytest.mark.parametrize("executor", ["arena", "onchip"])
 def test_each_executor_matches_oracle_bitwise(kind, executor):
     compare(worker(LIB, kind, executor=executor), oracle_results(kind), f"runner {kind} ({executor}) vs oracle")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("lanes", [8, 100, 512])
+def test_configured_lanes_per_point_match_oracle_bitwise(lanes):
+    """The C ABI's on-chip runs at 64, 5 and 1 points per block (plans whose points do not fit
+    run on the global-arena executor)."""
+    compare(worker(LIB, "f64", lanes=lanes), oracle_results("f64"), f"runner f64 ({lanes} lanes) vs oracle")
 
 
 @pytest.mark.gpu
