@@ -45,10 +45,11 @@ pacuda_b200_plan *pacuda_b200_plan_create(const pacman_recurrence_call *call, co
 void pacuda_b200_plan_destroy(pacuda_b200_plan *plan);
 /* the plan's algorithmic flops per point (fixed per-op counts) */
 uint64_t pacuda_b200_plan_flops(const pacuda_b200_plan *plan);
-/* the lanes that run one point's tasks: a block then runs P = threads / lanes of the plan's points
- * at once (1 .. 64) and each gets threads / P lanes (at least `lanes`, which that returns); 0 for
- * the tuned or default choice (the most points whose shared memory fits); INVALID when P points
- * do not fit */
+/* the lanes that run one point's tasks: a block runs P of the plan's points at once (1 .. 32),
+ * each with warps * floor(32 / P) lanes; this picks the largest P whose lanes are at least
+ * `lanes` (pacuda_b200_plan_lanes_per_point returns the lanes it gives); 0 for the tuned or
+ * default choice (of the point counts whose shared memory fits, the one that leaves the fewest
+ * threads idle, the larger on ties); INVALID when P points do not fit */
 int pacuda_b200_plan_set_lanes_per_point(pacuda_b200_plan *plan, uint32_t lanes);
 uint32_t pacuda_b200_plan_lanes_per_point(const pacuda_b200_plan *plan);
 

@@ -130,7 +130,8 @@ bool prepare(pacuda_b200_batch *b) {
             fprintf(stderr, "%s: a plan's point does not fit a block's shared memory\n", kTag);
             return false;
         }
-        if (!tiled_points_fit(p->points, p->point_bytes, b->threads, max_smem)) p->points = most;
+        if (!tiled_points_fit(p->points, p->point_bytes, b->threads, max_smem))
+            p->points = tiled_default_points(p->point_bytes, b->threads, max_smem);
         fill_plan(p, plans[k]);
         uint32_t per = p->points;
         b->smem = std::max<size_t>(b->smem, (size_t)per * p->point_bytes);
@@ -174,10 +175,10 @@ size_t point_smem(const pacuda_b200_plan *p) {
     return tiled_max_smem(p->kernel) - tiled_const_bytes(p->scales, p->factors);
 }
 
-// the most points per block that fit shared memory (the fewest lanes per point)
+// the default points per block (tiled_default_points)
 uint32_t default_points(const pacuda_b200_plan *p) {
-    uint32_t most = tiled_max_points(p->point_bytes, tiled_threads(p->kernel), point_smem(p));
-    return most ? most : 1u;
+    uint32_t np = tiled_default_points(p->point_bytes, tiled_threads(p->kernel), point_smem(p));
+    return np ? np : 1u;
 }
 
 }  // namespace
@@ -290,7 +291,10 @@ extern "C" int pacuda_b200_plan_set_lanes_per_point(pacuda_b200_plan *p, uint32_
         return PACMAN_RECURRENCE_OK;
     }
     int threads = tiled_threads(p->kernel);
-    uint32_t points = lanes <= (uint32_t)threads ? (uint32_t)threads / lanes : 0;
+    // the most points per block whose lanes are still at least `lanes`
+    uint32_t points = 0;
+    for (uint32_t np = 1; np <= kMaxPoints; np++)
+        if (tiled_lanes(np, threads) >= lanes) points = np;
     if (!tiled_points_fit(points, p->point_bytes, threads, point_smem(p))) return PACMAN_RECURRENCE_INVALID;
     p->points = points;
     p->fixed = true;
@@ -298,7 +302,7 @@ extern "C" int pacuda_b200_plan_set_lanes_per_point(pacuda_b200_plan *p, uint32_
 }
 
 extern "C" uint32_t pacuda_b200_plan_lanes_per_point(const pacuda_b200_plan *p) {
-    return p ? (uint32_t)p->tiled.threads / p->points : 0;
+    return p ? tiled_lanes(p->points, p->tiled.threads) : 0;
 }
 
 extern "C" pacuda_b200_batch *pacuda_b200_batch_create(pacuda_b200_plan *const *plans, uint32_t nplans,
@@ -523,7 +527,9 @@ extern "C" int pacuda_b200_run_static(pacuda_b200_plan *const *plans, uint32_t n
             fprintf(stderr, "%s: run_static: a plan's point does not fit a block's shared memory\n", kTag);
             return PACMAN_RECURRENCE_INVALID;
         }
-        uint32_t per = tiled_points_fit(p->points, p->point_bytes, threads, max_smem) ? p->points : most;
+        uint32_t per = tiled_points_fit(p->points, p->point_bytes, threads, max_smem)
+                           ? p->points
+                           : tiled_default_points(p->point_bytes, threads, max_smem);
         fill_plan(p, block.plans[k]);
         describe(p->tiled, p->forms, per, p->point_bytes, block.plans[k]);
         smem = std::max<size_t>(smem, (size_t)per * p->point_bytes);

@@ -381,9 +381,11 @@ int onchip_launch(DeviceProgram *prog, const pacman_recurrence_call *c, const Ru
     size_t pb = prog->tiled_state == 1 ? tiled_point_bytes(prog->tiled.host, forms, kernel) : 0;
     size_t cb = tiled_const_bytes(c->scale_count, c->factor_count);
     size_t room = threads ? tiled_max_smem(kernel) - cb : 0;
-    uint32_t np = threads && prog->tiled.threads == threads ? tiled_max_points(pb, threads, room) : 0;
+    uint32_t np = threads && prog->tiled.threads == threads ? tiled_default_points(pb, threads, room) : 0;
     if (np && current.lanes_per_point) {
-        uint32_t want = current.lanes_per_point <= (uint32_t)threads ? (uint32_t)threads / current.lanes_per_point : 0;
+        uint32_t want = 0;  // the most points per block whose lanes are at least the configured count
+        for (uint32_t n = 1; n <= kMaxPoints; n++)
+            if (tiled_lanes(n, threads) >= current.lanes_per_point) want = n;
         np = tiled_points_fit(want, pb, threads, room) ? want : 0;
     }
     if (!np) return current.executor == PACUDA_B200_EXECUTOR_ONCHIP ? 2 : 0;

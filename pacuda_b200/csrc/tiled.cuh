@@ -4,12 +4,14 @@
 // the outputs go out (in the C ABI's mode also the arena's live-in planes in and its written
 // planes out).
 //
-// A block runs P points at once with G = threads / P lanes each. Thread t serves point t % P as
-// lane t / P: the P threads of a lane run the same task on consecutive points, so their
-// instruction fetches are one broadcast, their shared-memory values ([slot][P], interleaved) are
-// contiguous, and their global stores cover P consecutive points of a plane. All points take the
-// same lane order, so a block's points move through the levels together and meet at the block's
-// barrier. A block takes one work item at a time: one plan's next P points.
+// A block runs P points at once (1 .. 32). A lane of all P points is a group of P adjacent
+// threads of one warp (floor(32 / P) groups per warp, the warp's other threads idle), so each
+// point has G = warps * floor(32 / P) lanes. The P threads of a group run the same task on
+// consecutive points: their instruction fetches are one broadcast, their shared-memory values
+// ([slot][P], interleaved) are contiguous, and their global stores cover P consecutive points of
+// a plane. All points take the same lane order, so a block's points move through the levels
+// together and meet at the block's barrier. A block takes one work item at a time: one plan's
+// next P points.
 #pragma once
 #include <stdint.h>
 
@@ -28,7 +30,7 @@ struct TiledPlan {
     uint32_t levels;
     uint32_t cur_slots, amp_slots, forms;
     uint32_t points;              // P points per block
-    uint32_t lanes;               // G lanes per point (the block's threads / P)
+    uint32_t lanes;               // G lanes per point: warps * floor(32 / P)
     uint32_t point_bytes;         // shared memory of one point
     // constants: f64 (sources), the kind's layout (rows)
     const double *s64, *f64;
@@ -162,9 +164,10 @@ __global__ void __launch_bounds__(512, 1) run_tiled(TiledLaunch L) {
         Const *consts = (Const *)smem;
         const uint32_t nconst = 2 * (p.scales + p.factors);
         for (uint32_t c = threadIdx.x; c < nconst; c += blockDim.x) consts[c] = ((const Const *)p.kconst)[c];
-        // this thread: lane tl of point pw; the threads beyond np * lanes only meet the barriers
-        const uint32_t tl = threadIdx.x / np, pw = threadIdx.x - tl * np;
-        const bool active = tl < lanes;
+        // this thread: lane tl of point pw; the threads of no group only meet the barriers
+        const uint32_t groups = 32 / np, x = threadIdx.x & 31, q = x / np, pw = x - q * np;
+        const uint32_t tl = (threadIdx.x >> 5) * groups + q;
+        const bool active = q < groups;
         SlotView<K, ABI> v;
         v.cur_ = (Pair<R> *)(smem + L.const_bytes);
         v.amp_ = (Pair<Amp> *)(v.cur_ + (size_t)p.cur_slots * np);

@@ -50,7 +50,7 @@ bool upload_schedule(TiledDevice &t, int threads, cudaStream_t s) {
     std::vector<uint32_t> ranges, firsts;
     for (uint32_t np = 1; t.ok && np <= kMaxPoints; np++) {
         std::vector<uint32_t> order, lf;
-        lane_order(t.host, std::max(1u, (uint32_t)threads / np), order, lf);
+        lane_order(t.host, tiled_lanes(np, threads), order, lf);
         // each position holds its task's instruction range (first, end); (0, 0) for none
         t.order_at[np - 1] = ranges.size();
         t.level_at[np - 1] = firsts.size();
@@ -103,14 +103,21 @@ size_t tiled_max_smem(int kernel) {
 }
 
 bool tiled_points_fit(uint32_t points, size_t point_bytes, int threads, size_t max_smem) {
-    return points >= 1 && points <= kMaxPoints && threads > 0 && points <= (uint32_t)threads &&
-           (size_t)points * point_bytes <= max_smem;
+    return points >= 1 && points <= kMaxPoints && threads >= 32 && (size_t)points * point_bytes <= max_smem;
 }
 
 uint32_t tiled_max_points(size_t point_bytes, int threads, size_t max_smem) {
     for (uint32_t np = kMaxPoints; np >= 1; np--)
         if (tiled_points_fit(np, point_bytes, threads, max_smem)) return np;
     return 0;
+}
+
+uint32_t tiled_default_points(size_t point_bytes, int threads, size_t max_smem) {
+    uint32_t best = 0;
+    for (uint32_t np = 1; np <= kMaxPoints; np++)
+        if (tiled_points_fit(np, point_bytes, threads, max_smem) && (!best || np * (32 / np) >= best * (32 / best)))
+            best = np;
+    return best;
 }
 
 void describe(const TiledDevice &t, uint32_t forms, uint32_t points, size_t point_bytes, TiledPlan &p) {
@@ -123,7 +130,7 @@ void describe(const TiledDevice &t, uint32_t forms, uint32_t points, size_t poin
     p.amp_slots = t.host.amp_slots;
     p.forms = forms;
     p.points = points;
-    p.lanes = std::max(1u, (uint32_t)t.threads / points);
+    p.lanes = tiled_lanes(points, t.threads);
     p.point_bytes = (uint32_t)point_bytes;
     p.loads = t.loads;
     p.nloads = (uint32_t)t.host.loads.size() / 3;

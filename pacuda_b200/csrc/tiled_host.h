@@ -11,8 +11,10 @@ namespace pacuda {
 struct TiledPlan;
 struct TiledLaunch;
 
-// points per block: 1 .. kMaxPoints; a point then has threads / P lanes
-constexpr uint32_t kMaxPoints = 64;
+// points per block: 1 .. kMaxPoints; a point then has warps * floor(32 / P) lanes (a lane of all
+// P points is P adjacent threads of one warp)
+constexpr uint32_t kMaxPoints = 32;
+inline uint32_t tiled_lanes(uint32_t points, int threads) { return (uint32_t)(threads / 32) * (32 / points); }
 
 struct TiledDevice {
     Schedule host;
@@ -46,6 +48,9 @@ size_t tiled_max_smem(int kernel);
 bool tiled_points_fit(uint32_t points, size_t point_bytes, int threads, size_t max_smem);
 // the most points per block that fit, or 0
 uint32_t tiled_max_points(size_t point_bytes, int threads, size_t max_smem);
+// the default points per block: of those that fit, the count that leaves the fewest threads of a
+// warp without a lane (P * floor(32 / P) largest), the larger on ties; 0 when none fits
+uint32_t tiled_default_points(size_t point_bytes, int threads, size_t max_smem);
 
 // fills the schedule fields of a plan descriptor for `points` points per block
 void describe(const TiledDevice &t, uint32_t forms, uint32_t points, size_t point_bytes, TiledPlan &p);

@@ -49,7 +49,7 @@ def test_batch_matches_oracle_bitwise(kind):
 @pytest.mark.gpu
 @pytest.mark.parametrize("lanes", [8, 16, 25, 32, 64, 96, 128, 170, 256, 512])
 def test_every_lanes_per_point_gives_the_same_bits(lanes):
-    """Blocks of 1 to 64 points, with idle threads where the points do not divide the block;
+    """Blocks of 1 to 32 points, with idle threads where the points do not divide a warp;
     plans whose points do not fit keep their default."""
     from pacuda_b200 import batch as B
     import torch
@@ -64,7 +64,8 @@ def test_every_lanes_per_point_gives_the_same_bits(lanes):
             pass
     if not taken:
         pytest.skip(f"{lanes} lanes per point fit no plan")
-    assert any(p.lanes_per_point == 512 // (512 // lanes) for p in plans)
+    given = min(16 * (32 // n) for n in range(1, 33) if 16 * (32 // n) >= lanes)  # 16 warps
+    assert any(p.lanes_per_point == given for p in plans)
     b = B.Batch(plans, ext, out)
     b.run()
     torch.cuda.synchronize()
