@@ -43,7 +43,10 @@ def split_points(total, seed):
     rng = np.random.default_rng(seed)
     w = rng.dirichlet(np.ones(len(FAMILIES)))
     n = np.maximum(1024, np.floor(w * total).astype(int))
-    n[0] += total - n.sum()
+    rem = total - n.sum()
+    n[0 if n[0] + rem >= 1024 else int(np.argmax(n))] += rem
+    if total < 1024 * len(FAMILIES) or n.min() < 1024:
+        raise ValueError(f"{total} points do not give every family 1024")
     return [int(x) for x in n]
 
 
@@ -119,6 +122,38 @@ def fp64_peak(torch, lib):
         flops = 2.0 * 8 * iters * blocks.value * threads.value
         best = max(best, flops / (e0.elapsed_time(e1) * 1e-3))
     return best / 1e12
+
+
+def reduce_over_ranks(dist, ms, sums):
+    """The job's step time is the slowest rank's; each family's |M|^2 total adds up over the ranks
+    (the points are sharded: the only exchange is this reduction of two small tensors)."""
+    import torch
+
+    t = torch.tensor([ms], dtype=torch.float64, device=sums.device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total = sums.clone()
+    dist.all_reduce(total)
+    return float(t.item()), total
+
+
+def dram_bytes_per_point():
+    """DRAM bytes per point of the batch kernel, from the committed ncu summary (one capture of the
+    same family mix), or None."""
+    import re
+
+    try:
+        text = open(os.path.join(ROOT, "profiles", "launches_pp3j_bench.md")).read()
+    except OSError:
+        return None
+    m = re.search(r"^dram_bytes_per_point = ([0-9.]+)", text, re.M)
+    return float(m.group(1)) if m else None
+
+
+def hbm_peak():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]
+    except (OSError, ValueError, KeyError):
+        return 6650.0
 
 
 def cpu_baseline(fams, sample=2048):
@@ -277,27 +312,30 @@ def main():
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / args.steps
     clk = clocks.stop() if clocks else None
+    # the total |M|^2 of each family
+    sums = torch.stack([o.sum() for o in out])
     if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+        ms, sums = reduce_over_ranks(dist, ms, sums)
         dist.barrier()
     points = sum(p.shape[0] for _, _, p in fams) * world
     value = points / (ms * 1e-3)
-    # the total |M|^2 of each family (the path's one exchange: summed over the ranks)
-    sums = torch.stack([o.sum() for o in out])
-    if world > 1:
-        dist.all_reduce(sums)
     peak = fp64_peak(torch, B.lib())
-    achieved = flops / (ms * 1e-3) / 1e12 if world == 1 else flops / (ms * 1e-3) / 1e12
+    achieved = flops / (ms * 1e-3) / 1e12  # this rank's launch: its flops over its device time
+    per_point = dram_bytes_per_point() if not args.family else None
+    traffic = per_point * sum(p.shape[0] for _, _, p in fams) if per_point else None
     res = {"metric": metric, "value": value, "unit": "points/s", "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config,
            "gpu_launches": args.steps * batch.launches,
            "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                        "frac": achieved / peak, "traffic": None,
+                        "frac": achieved / peak, "traffic": traffic,
                         "peak_source": "f64 FMA throughput measured in this run (2 flops per DFMA); the "
                                        "reference's arithmetic has no FMA, so half of it is the ceiling",
+                        "frac_of_no_fma_ceiling": achieved / (peak / 2),
+                        "traffic_source": "dram read+write bytes per point from one ncu capture of the same mix "
+                                          "(profiles/launches_pp3j_bench.md), times this launch's points",
+                        "hbm": {"achieved_gbs": traffic / (ms * 1e-3) / 1e9 if traffic else None,
+                                "peak_gbs": hbm_peak(), "peak_source": "MEASURED_PEAKS.json hbm_gbs"},
                         "flops_per_point": {n: pl.flops for (n, _, _), pl in zip(fams, plans)}},
            "points_per_family": {n: p.shape[0] for n, _, p in fams},
            "lanes_per_point": {n: pl.lanes_per_point for (n, _, _), pl in zip(fams, plans)},
