@@ -57,6 +57,11 @@ uint32_t pacuda_b200_plan_lanes_per_point(const pacuda_b200_plan *plan);
 pacuda_b200_batch *pacuda_b200_batch_create(pacuda_b200_plan *const *plans, uint32_t nplans,
                                             const double *const *external, const uint32_t *count,
                                             double *const *output);
+/* Points the batch's plans at other arrays and point counts (as batch_create takes them), without
+ * allocating; a captured graph is dropped (capture again to replay). Waits for the previous run's
+ * copy of the launch descriptors, not for its kernel: the caller orders its use of the old arrays. */
+int pacuda_b200_batch_update(pacuda_b200_batch *batch, const double *const *external, const uint32_t *count,
+                             double *const *output);
 /* Times each plan's lanes-per-point choices on its own points and keeps the fastest. */
 int pacuda_b200_batch_tune(pacuda_b200_batch *batch, void *stream);
 /* One persistent launch over every plan's points, on `stream` (a cudaStream_t; NULL: default). */

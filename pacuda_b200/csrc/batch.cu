@@ -67,6 +67,7 @@ struct pacuda_b200_batch {
     size_t smem = 0, const_bytes = 0;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
+    cudaEvent_t copied = nullptr;  // recorded after each launch's descriptor copy
 };
 
 namespace {
@@ -163,6 +164,11 @@ TiledLaunch launch_args(const pacuda_b200_batch *b) {
 
 int launch(pacuda_b200_batch *b, cudaStream_t s) {
     if (failed(cudaMemcpyAsync(b->device, b->host, b->bytes, cudaMemcpyHostToDevice, s), "descriptors"))
+        return PACMAN_RECURRENCE_DEVICE_ERROR;
+    // (not while capturing: the graph's copy reads the block when it is replayed)
+    cudaStreamCaptureStatus capturing = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(s, &capturing);
+    if (capturing == cudaStreamCaptureStatusNone && b->copied && failed(cudaEventRecord(b->copied, s), "event"))
         return PACMAN_RECURRENCE_DEVICE_ERROR;
     if (!launch_tiled(b->plans[0]->kernel, launch_args(b), b->threads, b->smem, b->sms, s) ||
         failed(cudaGetLastError(), "launch"))
@@ -321,11 +327,34 @@ extern "C" pacuda_b200_batch *pacuda_b200_batch_create(pacuda_b200_plan *const *
     b->count.assign(count, count + nplans);
     b->output.assign(output, output + nplans);
     b->sms = device_sms();
-    if (!prepare(b)) {
+    if (failed(cudaEventCreateWithFlags(&b->copied, cudaEventDisableTiming), "event") || !prepare(b)) {
         pacuda_b200_batch_destroy(b);
         return nullptr;
     }
     return b;
+}
+
+extern "C" int pacuda_b200_batch_update(pacuda_b200_batch *b, const double *const *external, const uint32_t *count,
+                                        double *const *output) {
+    if (!b || !external || !count || !output) return PACMAN_RECURRENCE_INVALID;
+    for (size_t k = 0; k < b->plans.size(); k++)
+        if (!count[k] || !external[k] || !output[k]) {
+            fprintf(stderr, "%s: batch_update: plan %zu: a missing array or point count\n", kTag, k);
+            return PACMAN_RECURRENCE_INVALID;
+        }
+    // the previous launch's copy of the descriptors must have left the pinned block
+    if (failed(cudaEventSynchronize(b->copied), "batch_update")) return PACMAN_RECURRENCE_DEVICE_ERROR;
+    if (b->exec) {
+        cudaGraphExecDestroy(b->exec);
+        cudaGraphDestroy(b->graph);
+        b->exec = nullptr;
+        b->graph = nullptr;
+    }
+    size_t n = b->plans.size();
+    b->external.assign(external, external + n);
+    b->count.assign(count, count + n);
+    b->output.assign(output, output + n);
+    return prepare(b) ? PACMAN_RECURRENCE_OK : PACMAN_RECURRENCE_DEVICE_ERROR;
 }
 
 extern "C" int pacuda_b200_batch_run(pacuda_b200_batch *b, void *stream) {
@@ -420,6 +449,10 @@ extern "C" void pacuda_b200_batch_destroy(pacuda_b200_batch *b) {
     if (!b) return;
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->graph) cudaGraphDestroy(b->graph);
+    if (b->copied) {
+        cudaEventSynchronize(b->copied);
+        cudaEventDestroy(b->copied);
+    }
     cudaFreeHost(b->host);
     cudaFree(b->device);
     delete b;
