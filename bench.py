@@ -7,8 +7,10 @@ colour orderings summed, in f64 (bit for bit the reference runner's f64 arithmet
 
 * value: the batched device API, every family in one persistent launch (captured in a CUDA
   graph), momenta resident in HBM (168 MB of inputs: larger than L2, so no flush is needed);
-* e2e: the reference-facing C ABI (pacman_recurrence_v1_run + _reduce_resolved per tile of 2^16
-  points) from pinned host buffers, the copies in the timed region;
+* e2e: the call a generator makes, umami_matrix_element of the p p -> 3 jets UMAMI library
+  (pacuda_b200/umami), one call per step over all events from pinned host momenta to |M|^2 in
+  host memory, the copies in the timed region; e2e_abi: the runner's own C ABI
+  (pacman_recurrence_v1_run + _reduce_resolved per tile of 2^16 points) the same way;
 * roofline: the dominant kernel's algorithmic flops (fixed per-op counts) per launch over its
   CUDA-event time, against this GPU's f64 FMA throughput measured in the same run;
 * cpu_baseline: the CPU oracle (the runner's arithmetic restated in C++, OpenMP over all cores)
@@ -220,6 +222,82 @@ def e2e_abi(fams, steps, warmup, lib=None, kernel="f64"):
             "tile": TILE, "calls_per_step": 2 * len(jobs)}, [j[3] for j in jobs]
 
 
+def e2e_umami(fams, steps, warmup, outs=None):
+    """points/s through the UMAMI call a generator makes (umami_matrix_element, the reference's
+    production entry point): every step one call over all events, from pinned host momenta (copied
+    to the device inside the call) to |M|^2 in host memory (copied back inside the call)."""
+    import ctypes as C
+    import tempfile
+
+    from pacuda_b200 import pacuda_file
+    from pacuda_b200.runner import Runner
+    from pacuda_b200.umami import build as ub
+
+    lib = C.CDLL(ub.pp3j_library())
+    lib.umami_initialize.argtypes = [C.POINTER(C.c_void_p), C.c_char_p]
+    lib.umami_matrix_element.argtypes = [C.c_void_p, C.c_size_t, C.c_size_t, C.c_size_t, C.c_size_t,
+                                         C.POINTER(C.c_int), C.POINTER(C.c_void_p), C.c_size_t,
+                                         C.POINTER(C.c_int), C.POINTER(C.c_void_p)]
+    lib.umami_free.argtypes = [C.c_void_p]
+    art = os.path.join(tempfile.mkdtemp(prefix="pp3j_"), "artifact")
+    os.makedirs(art)
+    pacuda_file.write(pacuda_file.from_processes(ub.PP3J, kernel=1, reference_points=0), art + ".pacuda")
+    h = C.c_void_p()
+    if lib.umami_initialize(C.byref(h), art.encode()) != 0:
+        raise RuntimeError("umami_initialize failed")
+    r = Runner(None)
+    n = sum(p.shape[0] for _, _, p in fams)
+    legs = 5
+
+    def pinned(count, ctype):
+        ptr = r.lib.pacman_recurrence_v1_host_alloc(count * C.sizeof(ctype))
+        return ptr, np.ctypeslib.as_array((ctype * count).from_address(ptr))
+
+    mom_p, mom = pinned(legs * 4 * n, C.c_double)
+    fl_p, flavour = pinned(n, C.c_int)
+    me_p, me = pinned(n, C.c_double)
+    rows = mom.reshape(legs * 4, n)
+    start = 0
+    for name, _, p in fams:
+        m = p.shape[0]
+        for k in range(4):
+            for leg in range(legs):
+                rows[legs * k + leg, start:start + m] = p[:, leg, k]
+        flavour[start:start + m] = ub.PP3J.index(name)
+        start += m
+    keys_in = (C.c_int * 2)(0, 2)
+    ptr_in = (C.c_void_p * 2)(mom_p, fl_p)
+    keys_out = (C.c_int * 1)(0)
+    ptr_out = (C.c_void_p * 1)(me_p)
+
+    def step():
+        if lib.umami_matrix_element(h, n, n, 0, 2, keys_in, ptr_in, 1, keys_out, ptr_out) != 0:
+            raise RuntimeError("umami_matrix_element failed")
+
+    for _ in range(warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        step()
+    dt = (time.perf_counter() - t0) / steps
+    # the helicity sums agree with the device-resident run's outputs (a sanity check)
+    if outs is not None:
+        start = 0
+        for (name, t, p), o in zip(fams, outs):
+            m = p.shape[0]
+            num, den = t.meta["group_factor"]
+            want = (o.reshape(m, t.outputs)[:64] * float(num) / float(den)).sum(axis=1)
+            if not np.allclose(me[start:start + min(64, m)], want, rtol=1e-12, atol=0):
+                raise RuntimeError(f"{name}: UMAMI |M|^2 differs from the batched run")
+            start += m
+    lib.umami_free(h)
+    for ptr in (mom_p, fl_p, me_p):
+        r.lib.pacman_recurrence_v1_host_free(ptr)
+    return {"value": n / dt, "unit": "points/s", "h2d_bytes_per_step": n * legs * 4 * 8 + n * 24,
+            "d2h_bytes_per_step": n * 8, "api": "umami_matrix_element (helicity sum, one call per step)",
+            "calls_per_step": 1}
+
+
 def main():
     global POINTS, FAMILIES
     ap = argparse.ArgumentParser()
@@ -344,8 +422,11 @@ def main():
         res["clocks"] = clk
     if rank == 0 and world == 1:
         if not args.no_e2e:
-            e2e, _ = e2e_abi(fams, max(1, args.steps // 5), 1)
-            res["e2e"] = e2e
+            outs = [o.cpu().numpy() for o in out]
+            res["e2e"] = e2e_umami(fams, max(3, args.steps // 2), 2, outs)
+            abi_line, _ = e2e_abi(fams, max(1, args.steps // 5), 1)
+            abi_line["api"] = "pacman_recurrence_v1_run + _reduce_resolved per tile of 2^16 points"
+            res["e2e_abi"] = abi_line
         if not args.no_cpu:
             res["cpu_baseline"] = cpu_baseline(fams)
     if world > 1:

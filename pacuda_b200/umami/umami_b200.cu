@@ -8,15 +8,16 @@
 //   1. selects each event's contributions from its channel and flavour (the provider's tables),
 //      and groups them by (process, colour, leg permutation), events in order within a group;
 //   2. copies the events' momenta to the device once, as the caller lays them out (row
-//      n * k + leg for component k of a leg, one value per event);
+//      n * k + leg for component k of a leg, one value per event), and each item's inputs;
 //   3. gathers every group's external momenta on the device (the permutation and the process's
 //      crossing applied: external leg l = sign_l x input leg permutation[crossing_l]);
 //   4. evaluates every group in ONE persistent launch of the batched executor, each point's
 //      helicity values reduced in the kernel from its amplitudes (pacuda_b200_batch_*);
-//   5. copies the helicity values back and combines the events on the host exactly as the
-//      reference does: the process-group factor, the alpha_s scale, then a fixed helicity, the
-//      helicity sum, or the helicity drawn in proportion to its value (the arithmetic and order
-//      of the reference's reduce_sample, recurrence_runner.cu:1532-1572).
+//   5. finishes each item on the device (the process-group factor, the alpha_s scale, then the
+//      helicity sum, a fixed helicity's value, or the helicity drawn in proportion to its value,
+//      with the reference's arithmetic in its order: recurrence_runner.cu:1532-1572) and copies
+//      back one value per item (and the draw);
+//   6. combines each event's contributions on the host as the reference does.
 // The values equal the reference library's bit for bit: the same f64 arithmetic in the same
 // order, from the same resolved reduction.
 //
@@ -100,32 +101,117 @@ template <class T> struct PinnedArray {
     }
 };
 
-// one group's gather: external[(l * 4 + k) * points + q] = sign[l] * momenta[(legs * k + leg[l]) * events + event[q]]
-struct Gather {
+// One group of items (its class's plan over its events): the gather of its external momenta,
+// external[(l * 4 + k) * points + q] = sign[l] * momenta[(legs * k + leg[l]) * events + event[q]],
+// and where its helicity values go.
+struct Group {
     unsigned long long external;  // offset of the group's planes in the external buffer
-    unsigned long long first;     // offset of its events in the event list
+    unsigned long long first;     // its first item (items are grouped, events in order within)
+    unsigned long long values;    // offset of its values ([point][live]) in the value buffer
     uint32_t points, legs;
+    uint32_t live, helicities;    // outputs with planes, and all the process's helicities
+    uint32_t live_at;             // offset of the colour's live helicities in the helicity table
+    uint32_t factor;              // 1: times numerator / denominator (the process-group factor)
+    double numerator, denominator;
     uint32_t leg[kMaxLegs];
     double sign[kMaxLegs];
 };
 
-__global__ void gather_groups(const Gather *groups, uint32_t ngroups, const double *momenta, size_t events,
-                              const uint32_t *event, double *external) {
-    const Gather &g = groups[blockIdx.y];
-    (void)ngroups;
+// One item's inputs, in group order.
+struct ItemIn {
+    uint32_t event;    // relative to the call's first event
+    int32_t helicity;  // a fixed helicity's runtime index (or -1)
+    double scale;      // (alpha_s / alpha_s at conversion) ^ QCD power
+    double random;     // the helicity's random number (sampling)
+};
+
+enum Mode : int { MODE_SUM = 0, MODE_HELICITY = 1, MODE_SAMPLE = 2 };
+
+__device__ __forceinline__ uint32_t group_of(const Group *groups, uint32_t ngroups, unsigned long long item) {
+    uint32_t lo = 0, hi = ngroups;  // the last group whose first item is <= item
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) / 2;
+        if (groups[mid].first <= item) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+// the external momenta of every group; `bad` is set when a momentum is not finite
+__global__ void gather_groups(const Group *groups, const double *momenta, size_t events, const ItemIn *items,
+                              double *external, int *bad) {
+    const Group &g = groups[blockIdx.y];
     const size_t n = (size_t)g.points * g.legs * 4;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         size_t q = i % g.points, lk = i / g.points;
         uint32_t l = (uint32_t)(lk >> 2), k = (uint32_t)(lk & 3);
-        double v = momenta[((size_t)g.legs * k + g.leg[l]) * events + event[g.first + q]];
+        double v = momenta[((size_t)g.legs * k + g.leg[l]) * events + items[g.first + q].event];
+        if (!isfinite(v)) *bad = 1;
         external[g.external + i] = g.sign[l] * v;
+    }
+}
+
+// Each item's result from its helicity values, with the reference's arithmetic in its order: every
+// value times numerator / denominator, times the scale; then the sum over all the helicities (the
+// ones without planes as 0.0), the value of one helicity, or the sampling's total and draw
+// (recurrence_runner.cu:1532-1572).
+__global__ void finish_items(const Group *groups, uint32_t ngroups, const ItemIn *items, unsigned long long nitems,
+                             const double *values, const uint32_t *live_helicity, int mode, double *value_out,
+                             uint32_t *chosen_out) {
+    for (unsigned long long j = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; j < nitems;
+         j += (unsigned long long)gridDim.x * blockDim.x) {
+        const Group &g = groups[group_of(groups, ngroups, j)];
+        const ItemIn it = items[j];
+        const double *v = values + g.values + (j - g.first) * (g.live ? g.live : 1);
+        const uint32_t *lh = live_helicity + g.live_at;
+        auto value = [&](uint32_t o) {
+            double x = v[o];
+            if (g.factor) x = __ddiv_rn(__dmul_rn(x, g.numerator), g.denominator);
+            if (it.scale != 1.0) x = __dmul_rn(x, it.scale);
+            return x;
+        };
+        if (mode == MODE_SUM) {
+            double sum = 0.0;
+            uint32_t o = 0;
+            for (uint32_t h = 0; h < g.helicities; h++) {
+                double x = 0.0;
+                if (o < g.live && lh[o] == h) x = value(o++);
+                sum = __dadd_rn(sum, x);
+            }
+            value_out[j] = sum;
+        } else if (mode == MODE_HELICITY) {
+            double x = 0.0;
+            for (uint32_t o = 0; o < g.live; o++)
+                if (lh[o] == (uint32_t)it.helicity) x = value(o);
+            value_out[j] = x;
+        } else {
+            double total = 0.0;
+            for (uint32_t o = 0; o < g.live; o++) total = __dadd_rn(total, value(o));
+            double target = __dmul_rn(it.random, total), cumulative = 0.0;
+            uint32_t pick = 0;
+            for (uint32_t o = 0; o < g.live; o++) {
+                double x = value(o);
+                if (x <= 0.0) continue;
+                pick = lh[o];
+                cumulative = __dadd_rn(cumulative, x);
+                if (cumulative > target) break;
+            }
+            value_out[j] = total;
+            chosen_out[j] = pick;
+        }
     }
 }
 
 struct Colour {
     const PacudaColour *c = nullptr;
     pacuda_b200_plan *plan = nullptr;
-    uint32_t live = 0;  // outputs of the plan (the helicities with planes)
+    uint32_t live = 0;     // outputs of the plan (the helicities with planes)
+    uint32_t live_at = 0;  // its live helicities' offset in the instance's helicity table
+};
+
+// contributions that evaluate alike: one (process, colour id, leg permutation)
+struct Class {
+    const UmamiContribution *entry = nullptr;  // the first contribution of the class
+    const Colour *colour = nullptr;
 };
 
 struct Instance {
@@ -133,29 +219,24 @@ struct Instance {
     std::vector<int> process;       // per provider process: its file process, or -1
     std::vector<double> alpha_s;    // per provider process
     std::vector<std::vector<Colour>> colours;  // [file process][colour]
+    std::vector<Class> classes;
+    std::vector<std::vector<std::vector<uint32_t>>> class_of;  // [channel][flavour][contribution]
     cudaStream_t stream = nullptr;
-    // the call's device and host buffers
-    DeviceArray<double> momenta, external, values;
-    DeviceArray<uint32_t> events;
-    DeviceArray<Gather> gathers;
-    PinnedArray<double> host_values;
-    PinnedArray<uint32_t> host_events;
-    PinnedArray<Gather> host_gathers;
-    // the batch of the last call's groups (reused while the groups' plans repeat)
+    DeviceArray<uint32_t> live_helicity;  // every colour's live helicities
+    // the call's buffers
+    DeviceArray<double> momenta, external, values, value_out;
+    DeviceArray<uint32_t> chosen_out;
+    DeviceArray<ItemIn> items;
+    DeviceArray<Group> groups;
+    DeviceArray<int> bad;
+    PinnedArray<ItemIn> host_items;
+    PinnedArray<Group> host_groups;
+    PinnedArray<double> host_value;
+    PinnedArray<uint32_t> host_chosen;
+    PinnedArray<int> host_bad;
+    // the batch of the last call's groups (re-pointed while their plans repeat)
     pacuda_b200_batch *batch = nullptr;
     std::vector<pacuda_b200_plan *> batch_plans;
-};
-
-// One evaluation: an event's contribution.
-struct Item {
-    size_t event;
-    const UmamiContribution *contribution;
-    double scale;   // (alpha_s / alpha_s at conversion) ^ QCD power
-    double random;  // the helicity's random number
-    size_t values;  // its helicity values, offset into the call's value list (not sampling)
-    double total;   // sampling: the sum of the helicity values and the helicity drawn
-    uint32_t chosen;
-    size_t index;   // its position among the event-ordered items
 };
 
 bool const supported_inputs[UMAMI_INPUT_KEY_COUNT] = {
@@ -209,112 +290,127 @@ void free_instance(Instance *in) {
     pacuda_b200_batch_destroy(in->batch);
     for (auto &v : in->colours)
         for (Colour &c : v) pacuda_b200_plan_destroy(c.plan);
+    in->live_helicity.release();
     in->momenta.release();
     in->external.release();
     in->values.release();
-    in->events.release();
-    in->gathers.release();
-    in->host_values.release();
-    in->host_events.release();
-    in->host_gathers.release();
+    in->value_out.release();
+    in->chosen_out.release();
+    in->items.release();
+    in->groups.release();
+    in->bad.release();
+    in->host_items.release();
+    in->host_groups.release();
+    in->host_value.release();
+    in->host_chosen.release();
+    in->host_bad.release();
     if (in->stream) cudaStreamDestroy(in->stream);
     delete in;
 }
 
-// items alike when they share the process, the colour id and the leg permutation
-int compare_evaluation(const UmamiContribution *x, const UmamiContribution *y) {
-    if (x == y) return 0;
-    if (x->process_index != y->process_index) return x->process_index < y->process_index ? -1 : 1;
-    int c = strcmp(x->color_id, y->color_id);
-    if (c != 0) return c;
-    return memcmp(x->permutation, y->permutation, umami_provider.particle_count * sizeof(size_t));
+// alike when they share the process, the colour id and the leg permutation
+bool same_evaluation(const UmamiContribution *x, const UmamiContribution *y) {
+    return x->process_index == y->process_index && strcmp(x->color_id, y->color_id) == 0 &&
+           memcmp(x->permutation, y->permutation, umami_provider.particle_count * sizeof(size_t)) == 0;
 }
 
-// The helicity values of every group of `sorted` (groups: [first, end) ranges), in one batched
-// launch: values of group g's point q at group_values[g] + q * live.
-UmamiStatus evaluate_groups(Instance *in, const std::vector<Item> &sorted, const std::vector<size_t> &bounds,
-                            const double *momenta, size_t stride, size_t offset, size_t count,
-                            std::vector<size_t> &group_values) {
-    const size_t n = umami_provider.particle_count, groups = bounds.size() - 1;
-    // 2. the events' momenta, as the caller lays them out, rows offset .. offset + count
-    if (!in->momenta.reserve(4 * n * count)) return UMAMI_ERROR;
-    if (cuda_failed(cudaMemcpy2DAsync(in->momenta.p, count * sizeof(double), momenta + offset, stride * sizeof(double),
-                                      count * sizeof(double), 4 * n, cudaMemcpyHostToDevice, in->stream),
-                    "momenta"))
+// Every item's result (value_out, and chosen_out when sampling) on the host, from the items of
+// each class (`first`: the classes' first items, items grouped by class): the momenta in, one
+// gather, one batched launch over the classes with items, one finishing pass, the results out.
+UmamiStatus evaluate(Instance *in, const std::vector<uint32_t> &first, size_t nitems, const double *momenta,
+                     size_t stride, size_t offset, size_t count, int mode) {
+    const size_t n = umami_provider.particle_count;
+    if (!in->momenta.reserve(4 * n * count) || !in->items.reserve(nitems) || !in->value_out.reserve(nitems) ||
+        !in->chosen_out.reserve(nitems) || !in->host_value.reserve(nitems) || !in->host_chosen.reserve(nitems) ||
+        !in->bad.reserve(1) || !in->host_bad.reserve(1) || !in->groups.reserve(in->classes.size()) ||
+        !in->host_groups.reserve(in->classes.size()))
         return UMAMI_ERROR;
-    // 3. the groups' gathers and their points' events
-    if (!in->host_gathers.reserve(groups) || !in->host_events.reserve(sorted.size()) ||
-        !in->gathers.reserve(groups) || !in->events.reserve(sorted.size()))
-        return UMAMI_ERROR;
-    std::vector<pacuda_b200_plan *> plans(groups);
-    std::vector<uint32_t> points(groups);
-    size_t ext = 0, vals = 0;
-    group_values.assign(groups, 0);
-    std::vector<size_t> ext_at(groups);
-    for (size_t g = 0; g < groups; g++) {
-        const Item &first = sorted[bounds[g]];
-        const UmamiContribution *entry = first.contribution;
-        const PacudaProcess *p = process_of(in, entry->process_index);
-        const Colour *col = colour_of(in, entry);
-        Gather &G = in->host_gathers.p[g];
+    // the groups: the classes with items
+    std::vector<pacuda_b200_plan *> plans;
+    std::vector<uint32_t> points;
+    std::vector<size_t> ext_at, val_at;
+    size_t ext = 0, vals = 0, groups = 0;
+    for (size_t c = 0; c < in->classes.size(); c++) {
+        uint32_t m = first[c + 1] - first[c];
+        if (!m) continue;
+        const Class &cls = in->classes[c];
+        const PacudaProcess *p = process_of(in, cls.entry->process_index);
+        Group &G = in->host_groups.p[groups++];
         memset(&G, 0, sizeof G);
         G.external = ext;
-        G.first = bounds[g];
-        G.points = (uint32_t)(bounds[g + 1] - bounds[g]);
+        G.first = first[c];
+        G.values = vals;
+        G.points = m;
         G.legs = (uint32_t)n;
+        G.live = cls.colour->live;
+        G.helicities = p->helicities;
+        G.live_at = cls.colour->live_at;
+        G.factor = p->numerator != p->denominator;
+        G.numerator = (double)p->numerator;
+        G.denominator = (double)p->denominator;
         for (size_t l = 0; l < n; l++) {
             size_t source = p->crossing_leg.empty() ? l : p->crossing_leg[l];
-            G.leg[l] = (uint32_t)entry->permutation[source];
+            G.leg[l] = (uint32_t)cls.entry->permutation[source];
             G.sign[l] = p->crossing_leg.empty() ? 1.0 : p->crossing_sign[l];
         }
-        plans[g] = col->plan;
-        points[g] = G.points;
-        ext_at[g] = ext;
-        group_values[g] = vals;
-        ext += 4 * n * G.points;
-        vals += (size_t)std::max<uint32_t>(col->live, 1) * G.points;
+        plans.push_back(cls.colour->plan);
+        points.push_back(m);
+        ext_at.push_back(ext);
+        val_at.push_back(vals);
+        ext += 4 * n * m;
+        vals += (size_t)std::max<uint32_t>(G.live, 1) * m;
     }
-    for (size_t j = 0; j < sorted.size(); j++) in->host_events.p[j] = (uint32_t)(sorted[j].event - offset);
-    if (!in->external.reserve(ext) || !in->values.reserve(vals) || !in->host_values.reserve(vals)) return UMAMI_ERROR;
-    if (cuda_failed(cudaMemcpyAsync(in->gathers.p, in->host_gathers.p, groups * sizeof(Gather), cudaMemcpyHostToDevice,
-                                    in->stream),
-                    "gathers") ||
-        cuda_failed(cudaMemcpyAsync(in->events.p, in->host_events.p, sorted.size() * sizeof(uint32_t),
-                                    cudaMemcpyHostToDevice, in->stream),
-                    "events"))
+    if (!in->external.reserve(ext) || !in->values.reserve(vals)) return UMAMI_ERROR;
+    cudaStream_t s = in->stream;
+    in->host_bad.p[0] = 0;
+    if (cuda_failed(cudaMemcpy2DAsync(in->momenta.p, count * sizeof(double), momenta + offset, stride * sizeof(double),
+                                      count * sizeof(double), 4 * n, cudaMemcpyHostToDevice, s),
+                    "momenta") ||
+        cuda_failed(cudaMemcpyAsync(in->items.p, in->host_items.p, nitems * sizeof(ItemIn), cudaMemcpyHostToDevice, s),
+                    "items") ||
+        cuda_failed(cudaMemcpyAsync(in->groups.p, in->host_groups.p, groups * sizeof(Group), cudaMemcpyHostToDevice, s),
+                    "groups") ||
+        cuda_failed(cudaMemcpyAsync(in->bad.p, in->host_bad.p, sizeof(int), cudaMemcpyHostToDevice, s), "flag"))
         return UMAMI_ERROR;
     uint32_t most = *std::max_element(points.begin(), points.end());
-    dim3 grid((unsigned)std::min<size_t>((4 * n * most + 255) / 256, 4096), (unsigned)groups);
-    gather_groups<<<grid, 256, 0, in->stream>>>(in->gathers.p, (uint32_t)groups, in->momenta.p, count, in->events.p,
-                                                in->external.p);
+    dim3 grid((unsigned)std::min<size_t>((4 * n * most + 255) / 256, 2048), (unsigned)groups);
+    gather_groups<<<grid, 256, 0, s>>>(in->groups.p, in->momenta.p, count, in->items.p, in->external.p, in->bad.p);
     if (cuda_failed(cudaGetLastError(), "gather")) return UMAMI_ERROR;
-    // 4. one launch over every group (the batch of the previous call re-pointed when its plans repeat)
+    // one launch over every group (the previous call's batch re-pointed when its plans repeat)
     std::vector<const double *> ext_p(groups);
     std::vector<double *> out_p(groups);
     for (size_t g = 0; g < groups; g++) {
         ext_p[g] = in->external.p + ext_at[g];
-        out_p[g] = in->values.p + group_values[g];
+        out_p[g] = in->values.p + val_at[g];
     }
     if (in->batch && in->batch_plans == plans) {
         if (pacuda_b200_batch_update(in->batch, ext_p.data(), points.data(), out_p.data()) != PACMAN_RECURRENCE_OK)
             return UMAMI_ERROR;
     } else {
         if (in->batch) {
-            cudaStreamSynchronize(in->stream);
+            cudaStreamSynchronize(s);
             pacuda_b200_batch_destroy(in->batch);
         }
         in->batch = pacuda_b200_batch_create(plans.data(), (uint32_t)groups, ext_p.data(), points.data(), out_p.data());
         in->batch_plans = in->batch ? plans : std::vector<pacuda_b200_plan *>();
         if (!in->batch) return UMAMI_ERROR;
     }
-    if (pacuda_b200_batch_run(in->batch, in->stream) != PACMAN_RECURRENCE_OK) return UMAMI_ERROR;
-    // 5. the helicity values back
-    if (cuda_failed(cudaMemcpyAsync(in->host_values.p, in->values.p, vals * sizeof(double), cudaMemcpyDeviceToHost,
-                                    in->stream),
+    if (pacuda_b200_batch_run(in->batch, s) != PACMAN_RECURRENCE_OK) return UMAMI_ERROR;
+    unsigned blocks = (unsigned)std::min<size_t>((nitems + 255) / 256, 4096);
+    finish_items<<<blocks, 256, 0, s>>>(in->groups.p, (uint32_t)groups, in->items.p, nitems, in->values.p,
+                                        in->live_helicity.p, mode, in->value_out.p, in->chosen_out.p);
+    if (cuda_failed(cudaGetLastError(), "finish") ||
+        cuda_failed(cudaMemcpyAsync(in->host_value.p, in->value_out.p, nitems * sizeof(double), cudaMemcpyDeviceToHost,
+                                    s),
                     "values") ||
-        cuda_failed(cudaStreamSynchronize(in->stream), "evaluation"))
+        (mode == MODE_SAMPLE &&
+         cuda_failed(cudaMemcpyAsync(in->host_chosen.p, in->chosen_out.p, nitems * sizeof(uint32_t),
+                                     cudaMemcpyDeviceToHost, s),
+                     "draws")) ||
+        cuda_failed(cudaMemcpyAsync(in->host_bad.p, in->bad.p, sizeof(int), cudaMemcpyDeviceToHost, s), "flag") ||
+        cuda_failed(cudaStreamSynchronize(s), "evaluation"))
         return UMAMI_ERROR;
-    return UMAMI_SUCCESS;
+    return in->host_bad.p[0] ? UMAMI_ERROR : UMAMI_SUCCESS;  // a momentum that is not finite
 }
 
 }  // namespace
@@ -411,13 +507,16 @@ UMAMI_EXPORT UmamiStatus umami_initialize(UmamiHandle *handle, char const *param
         }
         if (p) in->alpha_s[i] = p->alpha_s;
     }
-    // every colour of the file's processes compiled once
+    // every colour of the file's processes compiled once; their live helicities in one table
     in->colours.resize(f.processes.size());
+    std::vector<uint32_t> helicity_table;
     for (size_t k = 0; k < f.processes.size(); k++)
         for (const PacudaColour &c : f.processes[k].colours) {
             Colour col;
             col.c = &c;
             col.live = (uint32_t)c.live_helicity.size();
+            col.live_at = (uint32_t)helicity_table.size();
+            helicity_table.insert(helicity_table.end(), c.live_helicity.begin(), c.live_helicity.end());
             // the plan as a runner call describes it (the words, widths, planes, constants, forms)
             pacman_recurrence_call call;
             memset(&call, 0, sizeof call);
@@ -454,8 +553,17 @@ UMAMI_EXPORT UmamiStatus umami_initialize(UmamiHandle *handle, char const *param
             }
             in->colours[k].push_back(col);
         }
-    // every contribution's process and colour in the file
-    for (size_t ch = 0; ch < umami_provider.channel_count; ch++)
+    if (!in->live_helicity.reserve(std::max<size_t>(helicity_table.size(), 1)) ||
+        cuda_failed(cudaMemcpy(in->live_helicity.p, helicity_table.data(), helicity_table.size() * sizeof(uint32_t),
+                               cudaMemcpyHostToDevice),
+                    "helicity table")) {
+        free_instance(in);
+        return UMAMI_ERROR;
+    }
+    // every contribution's process and colour in the file, and its class
+    in->class_of.resize(umami_provider.channel_count);
+    for (size_t ch = 0; ch < umami_provider.channel_count; ch++) {
+        in->class_of[ch].resize(umami_provider.channels[ch].flavour_count);
         for (size_t fl = 0; fl < umami_provider.channels[ch].flavour_count; fl++) {
             const UmamiFlavour &flavour = umami_provider.channels[ch].flavours[fl];
             for (size_t j = 0; j < flavour.contribution_count; j++) {
@@ -471,8 +579,13 @@ UMAMI_EXPORT UmamiStatus umami_initialize(UmamiHandle *handle, char const *param
                         free_instance(in);
                         return UMAMI_ERROR;
                     }
+                uint32_t c = 0;
+                while (c < in->classes.size() && !same_evaluation(in->classes[c].entry, entry)) c++;
+                if (c == in->classes.size()) in->classes.push_back(Class{entry, colour_of(in, entry)});
+                in->class_of[ch][fl].push_back(c);
             }
         }
+    }
     *handle = in;
     return UMAMI_SUCCESS;
 }
@@ -557,143 +670,95 @@ UMAMI_EXPORT UmamiStatus umami_matrix_element(UmamiHandle handle, size_t count, 
     const double *random_in = (const double *)in_[UMAMI_IN_RANDOM_HELICITY];
     const int *helicity_in = (const int *)in_[UMAMI_IN_HELICITY_INDEX];
     const double *alpha_in = (const double *)in_[UMAMI_IN_ALPHA_S];
-    const size_t n = umami_provider.particle_count;
-    auto selection_of = [&](size_t event) -> const UmamiFlavour * {
+    const int mode = helicity_in ? MODE_HELICITY : out_[UMAMI_OUT_HELICITY_INDEX] ? MODE_SAMPLE : MODE_SUM;
+
+    // 1. the events' selections (checked as the reference checks them) and each class's item count
+    std::vector<uint32_t> selection(count);  // per event: channel << 16 | flavour
+    std::vector<uint32_t> first(in->classes.size() + 1, 0);
+    size_t nitems = 0;
+    for (size_t e = 0; e < count; ++e) {
+        size_t event = offset + e;
         size_t channel = channel_in ? channel_in[event] : 0;
         int flavour = flavour_in ? flavour_in[event] : 0;
         if (channel >= umami_provider.channel_count || flavour < 0 ||
             (size_t)flavour >= umami_provider.channels[channel].flavour_count)
-            return nullptr;
-        return &umami_provider.channels[channel].flavours[flavour];
-    };
-
-    // 1. the items: every event's contributions, in event order
-    bool sample = !helicity_in && out_[UMAMI_OUT_HELICITY_INDEX];
-    std::vector<Item> items;
-    size_t value_count = 0;
-    for (size_t event = offset; event < offset + count; ++event) {
-        const UmamiFlavour *selection = selection_of(event);
-        if (!selection || selection->contribution_count == 0) return UMAMI_ERROR;
+            return UMAMI_ERROR;
+        const UmamiFlavour &sel = umami_provider.channels[channel].flavours[flavour];
+        if (sel.contribution_count == 0 || channel > 0xffff || flavour > 0xffff) return UMAMI_ERROR;
         double random = random_in ? random_in[event] : 0.5;
         if (!isfinite(random) || random < 0.0 || random >= 1.0) return UMAMI_ERROR;
         if (helicity_in) {
             int label = helicity_in[event];
             if (label < 0 || (size_t)label >= umami_provider.exported_helicity_count) return UMAMI_ERROR;
-        } else if (out_[UMAMI_OUT_HELICITY_INDEX] && selection->contribution_count != 1) {
+        } else if (out_[UMAMI_OUT_HELICITY_INDEX] && sel.contribution_count != 1) {
             return UMAMI_ERROR_UNSUPPORTED_OUTPUT;
         }
-        for (size_t l = 0; l < n; l++)
-            for (size_t k = 0; k < 4; k++)
-                if (!isfinite(momenta[event + stride * (n * k + l)])) return UMAMI_ERROR;
-        for (size_t j = 0; j < selection->contribution_count; ++j) {
-            const UmamiContribution *entry = &selection->contributions[j];
-            const PacudaProcess *p = process_of(in, entry->process_index);
-            double a = in->alpha_s[entry->process_index];
+        for (size_t j = 0; j < sel.contribution_count; ++j) {
+            const UmamiContribution *entry = &sel.contributions[j];
             if (alpha_in) {
-                a = alpha_in[event];
+                double a = alpha_in[event];
                 if (!isfinite(a) || a < 0.0) return UMAMI_ERROR;
-                if (p->alpha_s_name.empty()) return UMAMI_ERROR_UNSUPPORTED_INPUT;
+                if (process_of(in, entry->process_index)->alpha_s_name.empty()) return UMAMI_ERROR_UNSUPPORTED_INPUT;
             }
+            first[in->class_of[channel][flavour][j] + 1]++;
+        }
+        nitems += sel.contribution_count;
+        selection[e] = (uint32_t)channel << 16 | (uint32_t)flavour;
+    }
+    // 2. the items grouped by class, events in order within a class (a counting sort); `at` is
+    // each event-ordered item's place
+    for (size_t c = 0; c < in->classes.size(); c++) first[c + 1] += first[c];
+    if (!in->host_items.reserve(nitems)) return UMAMI_ERROR;
+    std::vector<uint32_t> next(first.begin(), first.end() - 1), at(nitems);
+    for (size_t e = 0, k = 0; e < count; ++e) {
+        size_t event = offset + e, channel = selection[e] >> 16, flavour = selection[e] & 0xffff;
+        const UmamiFlavour &sel = umami_provider.channels[channel].flavours[flavour];
+        for (size_t j = 0; j < sel.contribution_count; ++j, ++k) {
+            const UmamiContribution *entry = &sel.contributions[j];
+            const PacudaProcess *p = process_of(in, entry->process_index);
+            double a = alpha_in ? alpha_in[event] : in->alpha_s[entry->process_index];
             double scale = 1.0;
             if (!p->alpha_s_name.empty() && a != p->alpha_s) scale = pow(a / p->alpha_s, p->qcd_power);
-            Item it{event, entry, scale, random, value_count, 0.0, 0, items.size()};
-            items.push_back(it);
-            if (!sample) value_count += p->helicities;
+            uint32_t place = next[in->class_of[channel][flavour][j]]++;
+            at[k] = place;
+            ItemIn &it = in->host_items.p[place];
+            it.event = (uint32_t)e;
+            it.helicity = helicity_in ? entry->helicity_runtime[helicity_in[event]] : -1;
+            it.scale = scale;
+            it.random = random_in ? random_in[event] : 0.5;
         }
     }
-    // the groups: items by (process, colour, permutation), events in order within each
-    std::vector<Item> sorted(items);
-    std::stable_sort(sorted.begin(), sorted.end(), [](const Item &x, const Item &y) {
-        return compare_evaluation(x.contribution, y.contribution) < 0;
-    });
-    std::vector<size_t> bounds{0};
-    for (size_t j = 1; j < sorted.size(); j++)
-        if (compare_evaluation(sorted[j].contribution, sorted[j - 1].contribution) != 0) bounds.push_back(j);
-    bounds.push_back(sorted.size());
-    std::vector<size_t> group_values;
-    UmamiStatus status = evaluate_groups(in, sorted, bounds, momenta, stride, offset, count, group_values);
+    // 3. - 5. on the device
+    UmamiStatus status = evaluate(in, first, nitems, momenta, stride, offset, count, mode);
     if (status != UMAMI_SUCCESS) return status;
 
-    // each item's helicity values (or its draw), from its group's reduced values
-    std::vector<double> values(std::max<size_t>(value_count, 1), 0.0);
-    for (size_t g = 0; g + 1 < bounds.size(); g++) {
-        const UmamiContribution *entry = sorted[bounds[g]].contribution;
-        const PacudaProcess *p = process_of(in, entry->process_index);
-        const Colour *col = colour_of(in, entry);
-        const PacudaColour &c = *col->c;
-        const size_t live = col->live;
-        const bool factor = p->numerator != p->denominator;
-        for (size_t j = bounds[g]; j < bounds[g + 1]; j++) {
-            Item &item = sorted[j];
-            const double *v = in->host_values.p + group_values[g] + (j - bounds[g]) * std::max<size_t>(live, 1);
-            if (sample) {
-                // the helicity drawn in proportion to its value, as the reference's device sampling
-                auto value = [&](size_t o) {
-                    double acc = v[o];
-                    if (factor) acc = acc * (double)p->numerator / (double)p->denominator;
-                    if (item.scale != 1.0) acc = acc * item.scale;
-                    return acc;
-                };
-                double t = 0.0;
-                for (size_t o = 0; o < live; o++) t = t + value(o);
-                double target = item.random * t, cumulative = 0.0;
-                uint32_t pick = 0;
-                for (size_t o = 0; o < live; o++) {
-                    double x = value(o);
-                    if (x <= 0.0) continue;
-                    pick = c.live_helicity[o];
-                    cumulative = cumulative + x;
-                    if (cumulative > target) break;
-                }
-                item.total = live ? t : 0.0;
-                item.chosen = live ? pick : 0;
-                items[item.index].total = item.total;
-                items[item.index].chosen = item.chosen;
-                continue;
-            }
-            double *dst = values.data() + item.values;
-            for (size_t k = 0; k < live; k++) {
-                double x = v[k];
-                if (factor) x = x * (double)p->numerator / (double)p->denominator;
-                if (item.scale != 1.0) x *= item.scale;
-                dst[c.live_helicity[k]] = x;
-            }
-        }
-    }
-
-    // the events, combined as the reference does
-    size_t k = 0;
-    for (size_t event = offset; event < offset + count; ++event) {
-        const UmamiFlavour *selection = selection_of(event);
-        const UmamiContribution *first = &selection->contributions[0];
+    // 6. the events, combined as the reference does
+    const double *value = in->host_value.p;
+    for (size_t e = 0, k = 0; e < count; ++e) {
+        size_t event = offset + e;
+        const UmamiFlavour &sel = umami_provider.channels[selection[e] >> 16].flavours[selection[e] & 0xffff];
+        const UmamiContribution *head = &sel.contributions[0];
         int label = 0;
         double total = 0.0;
-        if (helicity_in) {
+        if (mode == MODE_HELICITY) {
             label = helicity_in[event];
-            for (size_t j = 0; j < selection->contribution_count; ++j) {
-                const UmamiContribution *entry = &selection->contributions[j];
+            for (size_t j = 0; j < sel.contribution_count; ++j) {
+                const UmamiContribution *entry = &sel.contributions[j];
                 if (entry->helicity_runtime[label] < 0) continue;
-                total += entry->factor * values[items[k + j].values + entry->helicity_runtime[label]];
+                total += entry->factor * value[at[k + j]];
             }
-        } else if (out_[UMAMI_OUT_HELICITY_INDEX]) {
-            total = items[k].total;
-            label = first->helicity_export[items[k].chosen];
-            total *= first->factor;
+        } else if (mode == MODE_SAMPLE) {
+            total = value[at[k]];
+            label = head->helicity_export[in->host_chosen.p[at[k]]];
+            total *= head->factor;
         } else {
-            for (size_t j = 0; j < selection->contribution_count; ++j) {
-                const UmamiContribution *entry = &selection->contributions[j];
-                size_t h = process_of(in, entry->process_index)->helicities;
-                const double *v = values.data() + items[k + j].values;
-                double value = 0.0;
-                for (size_t hel = 0; hel < h; ++hel) value += v[hel];
-                total += entry->factor * value;
-            }
+            for (size_t j = 0; j < sel.contribution_count; ++j) total += sel.contributions[j].factor * value[at[k + j]];
         }
-        k += selection->contribution_count;
+        k += sel.contribution_count;
         if (!isfinite(total)) return UMAMI_ERROR;
         if (out_[UMAMI_OUT_MATRIX_ELEMENT]) ((double *)out_[UMAMI_OUT_MATRIX_ELEMENT])[event] = total;
         if (out_[UMAMI_OUT_HELICITY_INDEX]) ((int *)out_[UMAMI_OUT_HELICITY_INDEX])[event] = label;
-        if (out_[UMAMI_OUT_COLOR_INDEX]) ((int *)out_[UMAMI_OUT_COLOR_INDEX])[event] = (int)first->color_index;
+        if (out_[UMAMI_OUT_COLOR_INDEX]) ((int *)out_[UMAMI_OUT_COLOR_INDEX])[event] = (int)head->color_index;
     }
     return UMAMI_SUCCESS;
 }
