@@ -54,6 +54,10 @@ namespace {
 
 const char *const kTag = "pacuda-b200 umami";
 constexpr int kMaxLegs = 16;
+// A call's events are evaluated in up to kChunks chunks of at least kChunkEvents: the host builds
+// a chunk's items while the device evaluates the previous chunk.
+constexpr int kChunks = 4;
+constexpr size_t kChunkEvents = 1 << 16;
 
 bool cuda_failed(cudaError_t e, const char *what) {
     if (e == cudaSuccess) return false;
@@ -221,7 +225,8 @@ struct Instance {
     std::vector<std::vector<Colour>> colours;  // [file process][colour]
     std::vector<Class> classes;
     std::vector<std::vector<std::vector<uint32_t>>> class_of;  // [channel][flavour][contribution]
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr, copies = nullptr;  // compute; and the copies in
+    cudaEvent_t arrived[kChunks] = {nullptr};         // a chunk's inputs are on the device
     DeviceArray<uint32_t> live_helicity;  // every colour's live helicities
     // the call's buffers
     DeviceArray<double> momenta, external, values, value_out;
@@ -234,9 +239,9 @@ struct Instance {
     PinnedArray<double> host_value;
     PinnedArray<uint32_t> host_chosen;
     PinnedArray<int> host_bad;
-    // the batch of the last call's groups (re-pointed while their plans repeat)
-    pacuda_b200_batch *batch = nullptr;
-    std::vector<pacuda_b200_plan *> batch_plans;
+    // per chunk: the batch of the last call's groups (re-pointed while their plans repeat)
+    pacuda_b200_batch *batch[kChunks] = {nullptr};
+    std::vector<pacuda_b200_plan *> batch_plans[kChunks];
 };
 
 bool const supported_inputs[UMAMI_INPUT_KEY_COUNT] = {
@@ -287,7 +292,11 @@ bool alpha_named(const PacudaProcess *p, const char *name) {
 void free_instance(Instance *in) {
     if (!in) return;
     if (in->stream) cudaStreamSynchronize(in->stream);
-    pacuda_b200_batch_destroy(in->batch);
+    if (in->copies) cudaStreamSynchronize(in->copies);
+    for (int c = 0; c < kChunks; c++) {
+        pacuda_b200_batch_destroy(in->batch[c]);
+        if (in->arrived[c]) cudaEventDestroy(in->arrived[c]);
+    }
     for (auto &v : in->colours)
         for (Colour &c : v) pacuda_b200_plan_destroy(c.plan);
     in->live_helicity.release();
@@ -305,6 +314,7 @@ void free_instance(Instance *in) {
     in->host_chosen.release();
     in->host_bad.release();
     if (in->stream) cudaStreamDestroy(in->stream);
+    if (in->copies) cudaStreamDestroy(in->copies);
     delete in;
 }
 
@@ -314,31 +324,35 @@ bool same_evaluation(const UmamiContribution *x, const UmamiContribution *y) {
            memcmp(x->permutation, y->permutation, umami_provider.particle_count * sizeof(size_t)) == 0;
 }
 
-// Every item's result (value_out, and chosen_out when sampling) on the host, from the items of
-// each class (`first`: the classes' first items, items grouped by class): the momenta in, one
-// gather, one batched launch over the classes with items, one finishing pass, the results out.
-UmamiStatus evaluate(Instance *in, const std::vector<uint32_t> &first, size_t nitems, const double *momenta,
-                     size_t stride, size_t offset, size_t count, int mode) {
-    const size_t n = umami_provider.particle_count;
-    if (!in->momenta.reserve(4 * n * count) || !in->items.reserve(nitems) || !in->value_out.reserve(nitems) ||
-        !in->chosen_out.reserve(nitems) || !in->host_value.reserve(nitems) || !in->host_chosen.reserve(nitems) ||
-        !in->bad.reserve(1) || !in->host_bad.reserve(1) || !in->groups.reserve(in->classes.size()) ||
-        !in->host_groups.reserve(in->classes.size()))
-        return UMAMI_ERROR;
-    // the groups: the classes with items
+// One chunk of a call: its events, its items (grouped by class) and where its data go.
+struct Chunk {
+    size_t e0 = 0, e1 = 0;           // its events, relative to the call's first
+    size_t item0 = 0, items = 0;     // its items among the call's
+    size_t external = 0, values = 0; // its places in the external-momentum and value buffers
+    std::vector<uint32_t> first;     // per class: its first item (relative to item0); classes + 1
+};
+
+// Queues one chunk: its momenta and items in on the copy stream, then on the compute stream
+// its gather, ONE batched launch over its classes with items, its finishing pass and its results
+// out. `group0`: its place in the group buffers (kChunks regions of one group per class).
+UmamiStatus launch_chunk(Instance *in, int slot, const Chunk &ch, const double *momenta, size_t stride,
+                         size_t offset, int mode) {
+    const size_t n = umami_provider.particle_count, events = ch.e1 - ch.e0, group0 = slot * in->classes.size();
     std::vector<pacuda_b200_plan *> plans;
     std::vector<uint32_t> points;
-    std::vector<size_t> ext_at, val_at;
-    size_t ext = 0, vals = 0, groups = 0;
+    std::vector<const double *> ext_p;
+    std::vector<double *> out_p;
+    size_t ext = ch.external, vals = ch.values, groups = 0;
+    double *dev_mom = in->momenta.p + 4 * n * ch.e0;
     for (size_t c = 0; c < in->classes.size(); c++) {
-        uint32_t m = first[c + 1] - first[c];
+        uint32_t m = ch.first[c + 1] - ch.first[c];
         if (!m) continue;
         const Class &cls = in->classes[c];
         const PacudaProcess *p = process_of(in, cls.entry->process_index);
-        Group &G = in->host_groups.p[groups++];
+        Group &G = in->host_groups.p[group0 + groups++];
         memset(&G, 0, sizeof G);
         G.external = ext;
-        G.first = first[c];
+        G.first = ch.first[c];
         G.values = vals;
         G.points = m;
         G.legs = (uint32_t)n;
@@ -355,62 +369,59 @@ UmamiStatus evaluate(Instance *in, const std::vector<uint32_t> &first, size_t ni
         }
         plans.push_back(cls.colour->plan);
         points.push_back(m);
-        ext_at.push_back(ext);
-        val_at.push_back(vals);
+        ext_p.push_back(in->external.p + ext);
+        out_p.push_back(in->values.p + vals);
         ext += 4 * n * m;
         vals += (size_t)std::max<uint32_t>(G.live, 1) * m;
     }
-    if (!in->external.reserve(ext) || !in->values.reserve(vals)) return UMAMI_ERROR;
-    cudaStream_t s = in->stream;
-    in->host_bad.p[0] = 0;
-    if (cuda_failed(cudaMemcpy2DAsync(in->momenta.p, count * sizeof(double), momenta + offset, stride * sizeof(double),
-                                      count * sizeof(double), 4 * n, cudaMemcpyHostToDevice, s),
+    ItemIn *items = in->items.p + ch.item0;
+    Group *dev_groups = in->groups.p + group0;
+    if (cuda_failed(cudaMemcpy2DAsync(dev_mom, events * sizeof(double), momenta + offset + ch.e0,
+                                      stride * sizeof(double), events * sizeof(double), 4 * n,
+                                      cudaMemcpyHostToDevice, in->copies),
                     "momenta") ||
-        cuda_failed(cudaMemcpyAsync(in->items.p, in->host_items.p, nitems * sizeof(ItemIn), cudaMemcpyHostToDevice, s),
+        cuda_failed(cudaMemcpyAsync(items, in->host_items.p + ch.item0, ch.items * sizeof(ItemIn),
+                                    cudaMemcpyHostToDevice, in->copies),
                     "items") ||
-        cuda_failed(cudaMemcpyAsync(in->groups.p, in->host_groups.p, groups * sizeof(Group), cudaMemcpyHostToDevice, s),
+        cuda_failed(cudaMemcpyAsync(dev_groups, in->host_groups.p + group0, groups * sizeof(Group),
+                                    cudaMemcpyHostToDevice, in->copies),
                     "groups") ||
-        cuda_failed(cudaMemcpyAsync(in->bad.p, in->host_bad.p, sizeof(int), cudaMemcpyHostToDevice, s), "flag"))
+        cuda_failed(cudaEventRecord(in->arrived[slot], in->copies), "event") ||
+        cuda_failed(cudaStreamWaitEvent(in->stream, in->arrived[slot], 0), "event"))
         return UMAMI_ERROR;
+    cudaStream_t s = in->stream;
     uint32_t most = *std::max_element(points.begin(), points.end());
     dim3 grid((unsigned)std::min<size_t>((4 * n * most + 255) / 256, 2048), (unsigned)groups);
-    gather_groups<<<grid, 256, 0, s>>>(in->groups.p, in->momenta.p, count, in->items.p, in->external.p, in->bad.p);
+    gather_groups<<<grid, 256, 0, s>>>(dev_groups, dev_mom, events, items, in->external.p, in->bad.p);
     if (cuda_failed(cudaGetLastError(), "gather")) return UMAMI_ERROR;
-    // one launch over every group (the previous call's batch re-pointed when its plans repeat)
-    std::vector<const double *> ext_p(groups);
-    std::vector<double *> out_p(groups);
-    for (size_t g = 0; g < groups; g++) {
-        ext_p[g] = in->external.p + ext_at[g];
-        out_p[g] = in->values.p + val_at[g];
-    }
-    if (in->batch && in->batch_plans == plans) {
-        if (pacuda_b200_batch_update(in->batch, ext_p.data(), points.data(), out_p.data()) != PACMAN_RECURRENCE_OK)
+    pacuda_b200_batch *&batch = in->batch[slot];
+    if (batch && in->batch_plans[slot] == plans) {
+        if (pacuda_b200_batch_update(batch, ext_p.data(), points.data(), out_p.data()) != PACMAN_RECURRENCE_OK)
             return UMAMI_ERROR;
     } else {
-        if (in->batch) {
+        if (batch) {
             cudaStreamSynchronize(s);
-            pacuda_b200_batch_destroy(in->batch);
+            pacuda_b200_batch_destroy(batch);
         }
-        in->batch = pacuda_b200_batch_create(plans.data(), (uint32_t)groups, ext_p.data(), points.data(), out_p.data());
-        in->batch_plans = in->batch ? plans : std::vector<pacuda_b200_plan *>();
-        if (!in->batch) return UMAMI_ERROR;
+        batch = pacuda_b200_batch_create(plans.data(), (uint32_t)groups, ext_p.data(), points.data(), out_p.data());
+        in->batch_plans[slot] = batch ? plans : std::vector<pacuda_b200_plan *>();
+        if (!batch) return UMAMI_ERROR;
     }
-    if (pacuda_b200_batch_run(in->batch, s) != PACMAN_RECURRENCE_OK) return UMAMI_ERROR;
-    unsigned blocks = (unsigned)std::min<size_t>((nitems + 255) / 256, 4096);
-    finish_items<<<blocks, 256, 0, s>>>(in->groups.p, (uint32_t)groups, in->items.p, nitems, in->values.p,
-                                        in->live_helicity.p, mode, in->value_out.p, in->chosen_out.p);
+    if (pacuda_b200_batch_run(batch, s) != PACMAN_RECURRENCE_OK) return UMAMI_ERROR;
+    unsigned blocks = (unsigned)std::min<size_t>((ch.items + 255) / 256, 4096);
+    finish_items<<<blocks, 256, 0, s>>>(dev_groups, (uint32_t)groups, items, ch.items, in->values.p,
+                                        in->live_helicity.p, mode, in->value_out.p + ch.item0,
+                                        in->chosen_out.p + ch.item0);
     if (cuda_failed(cudaGetLastError(), "finish") ||
-        cuda_failed(cudaMemcpyAsync(in->host_value.p, in->value_out.p, nitems * sizeof(double), cudaMemcpyDeviceToHost,
-                                    s),
+        cuda_failed(cudaMemcpyAsync(in->host_value.p + ch.item0, in->value_out.p + ch.item0, ch.items * sizeof(double),
+                                    cudaMemcpyDeviceToHost, s),
                     "values") ||
         (mode == MODE_SAMPLE &&
-         cuda_failed(cudaMemcpyAsync(in->host_chosen.p, in->chosen_out.p, nitems * sizeof(uint32_t),
-                                     cudaMemcpyDeviceToHost, s),
-                     "draws")) ||
-        cuda_failed(cudaMemcpyAsync(in->host_bad.p, in->bad.p, sizeof(int), cudaMemcpyDeviceToHost, s), "flag") ||
-        cuda_failed(cudaStreamSynchronize(s), "evaluation"))
+         cuda_failed(cudaMemcpyAsync(in->host_chosen.p + ch.item0, in->chosen_out.p + ch.item0,
+                                     ch.items * sizeof(uint32_t), cudaMemcpyDeviceToHost, s),
+                     "draws")))
         return UMAMI_ERROR;
-    return in->host_bad.p[0] ? UMAMI_ERROR : UMAMI_SUCCESS;  // a momentum that is not finite
+    return UMAMI_SUCCESS;
 }
 
 }  // namespace
@@ -485,8 +496,11 @@ UMAMI_EXPORT UmamiStatus umami_initialize(UmamiHandle *handle, char const *param
         free_instance(in);
         return UMAMI_ERROR;
     }
-    if (f.kernel > PACMAN_RECURRENCE_KERNEL_MIXED64 ||
-        cuda_failed(cudaStreamCreateWithFlags(&in->stream, cudaStreamNonBlocking), "stream")) {
+    bool streams = !cuda_failed(cudaStreamCreateWithFlags(&in->stream, cudaStreamNonBlocking), "stream") &&
+                   !cuda_failed(cudaStreamCreateWithFlags(&in->copies, cudaStreamNonBlocking), "stream");
+    for (int c = 0; streams && c < kChunks; c++)
+        streams = !cuda_failed(cudaEventCreateWithFlags(&in->arrived[c], cudaEventDisableTiming), "event");
+    if (f.kernel > PACMAN_RECURRENCE_KERNEL_MIXED64 || !streams) {
         fprintf(stderr, "%s: kernel kind %u\n", kTag, f.kernel);
         free_instance(in);
         return UMAMI_ERROR;
@@ -672,65 +686,110 @@ UMAMI_EXPORT UmamiStatus umami_matrix_element(UmamiHandle handle, size_t count, 
     const double *alpha_in = (const double *)in_[UMAMI_IN_ALPHA_S];
     const int mode = helicity_in ? MODE_HELICITY : out_[UMAMI_OUT_HELICITY_INDEX] ? MODE_SAMPLE : MODE_SUM;
 
-    // 1. the events' selections (checked as the reference checks them) and each class's item count
+    // 1. every event's selection, checked as the reference checks them before anything is
+    // evaluated; the chunks and each chunk's item count per class
+    const size_t nchunks = std::min<size_t>(kChunks, std::max<size_t>(1, count / kChunkEvents));
+    std::vector<Chunk> chunks(nchunks);
+    const size_t nclasses = in->classes.size();
     std::vector<uint32_t> selection(count);  // per event: channel << 16 | flavour
-    std::vector<uint32_t> first(in->classes.size() + 1, 0);
     size_t nitems = 0;
-    for (size_t e = 0; e < count; ++e) {
-        size_t event = offset + e;
-        size_t channel = channel_in ? channel_in[event] : 0;
-        int flavour = flavour_in ? flavour_in[event] : 0;
-        if (channel >= umami_provider.channel_count || flavour < 0 ||
-            (size_t)flavour >= umami_provider.channels[channel].flavour_count)
-            return UMAMI_ERROR;
-        const UmamiFlavour &sel = umami_provider.channels[channel].flavours[flavour];
-        if (sel.contribution_count == 0 || channel > 0xffff || flavour > 0xffff) return UMAMI_ERROR;
-        double random = random_in ? random_in[event] : 0.5;
-        if (!isfinite(random) || random < 0.0 || random >= 1.0) return UMAMI_ERROR;
-        if (helicity_in) {
-            int label = helicity_in[event];
-            if (label < 0 || (size_t)label >= umami_provider.exported_helicity_count) return UMAMI_ERROR;
-        } else if (out_[UMAMI_OUT_HELICITY_INDEX] && sel.contribution_count != 1) {
-            return UMAMI_ERROR_UNSUPPORTED_OUTPUT;
-        }
-        for (size_t j = 0; j < sel.contribution_count; ++j) {
-            const UmamiContribution *entry = &sel.contributions[j];
-            if (alpha_in) {
-                double a = alpha_in[event];
-                if (!isfinite(a) || a < 0.0) return UMAMI_ERROR;
-                if (process_of(in, entry->process_index)->alpha_s_name.empty()) return UMAMI_ERROR_UNSUPPORTED_INPUT;
+    for (size_t c = 0; c < nchunks; c++) {
+        Chunk &ch = chunks[c];
+        ch.e0 = count * c / nchunks;
+        ch.e1 = count * (c + 1) / nchunks;
+        ch.item0 = nitems;
+        ch.first.assign(nclasses + 1, 0);
+        for (size_t e = ch.e0; e < ch.e1; ++e) {
+            size_t event = offset + e;
+            size_t channel = channel_in ? channel_in[event] : 0;
+            int flavour = flavour_in ? flavour_in[event] : 0;
+            if (channel >= umami_provider.channel_count || flavour < 0 ||
+                (size_t)flavour >= umami_provider.channels[channel].flavour_count)
+                return UMAMI_ERROR;
+            const UmamiFlavour &sel = umami_provider.channels[channel].flavours[flavour];
+            if (sel.contribution_count == 0 || channel > 0xffff || flavour > 0xffff) return UMAMI_ERROR;
+            double random = random_in ? random_in[event] : 0.5;
+            if (!isfinite(random) || random < 0.0 || random >= 1.0) return UMAMI_ERROR;
+            if (helicity_in) {
+                int label = helicity_in[event];
+                if (label < 0 || (size_t)label >= umami_provider.exported_helicity_count) return UMAMI_ERROR;
+            } else if (out_[UMAMI_OUT_HELICITY_INDEX] && sel.contribution_count != 1) {
+                return UMAMI_ERROR_UNSUPPORTED_OUTPUT;
             }
-            first[in->class_of[channel][flavour][j] + 1]++;
+            for (size_t j = 0; j < sel.contribution_count; ++j) {
+                const UmamiContribution *entry = &sel.contributions[j];
+                if (alpha_in) {
+                    double a = alpha_in[event];
+                    if (!isfinite(a) || a < 0.0) return UMAMI_ERROR;
+                    if (process_of(in, entry->process_index)->alpha_s_name.empty())
+                        return UMAMI_ERROR_UNSUPPORTED_INPUT;
+                }
+                ch.first[in->class_of[channel][flavour][j] + 1]++;
+            }
+            nitems += sel.contribution_count;
+            selection[e] = (uint32_t)channel << 16 | (uint32_t)flavour;
         }
-        nitems += sel.contribution_count;
-        selection[e] = (uint32_t)channel << 16 | (uint32_t)flavour;
+        ch.items = nitems - ch.item0;
+        for (size_t k = 0; k < nclasses; k++) ch.first[k + 1] += ch.first[k];
     }
-    // 2. the items grouped by class, events in order within a class (a counting sort); `at` is
-    // each event-ordered item's place
-    for (size_t c = 0; c < in->classes.size(); c++) first[c + 1] += first[c];
-    if (!in->host_items.reserve(nitems)) return UMAMI_ERROR;
-    std::vector<uint32_t> next(first.begin(), first.end() - 1), at(nitems);
-    for (size_t e = 0, k = 0; e < count; ++e) {
-        size_t event = offset + e, channel = selection[e] >> 16, flavour = selection[e] & 0xffff;
-        const UmamiFlavour &sel = umami_provider.channels[channel].flavours[flavour];
-        for (size_t j = 0; j < sel.contribution_count; ++j, ++k) {
-            const UmamiContribution *entry = &sel.contributions[j];
-            const PacudaProcess *p = process_of(in, entry->process_index);
-            double a = alpha_in ? alpha_in[event] : in->alpha_s[entry->process_index];
-            double scale = 1.0;
-            if (!p->alpha_s_name.empty() && a != p->alpha_s) scale = pow(a / p->alpha_s, p->qcd_power);
-            uint32_t place = next[in->class_of[channel][flavour][j]]++;
-            at[k] = place;
-            ItemIn &it = in->host_items.p[place];
-            it.event = (uint32_t)e;
-            it.helicity = helicity_in ? entry->helicity_runtime[helicity_in[event]] : -1;
-            it.scale = scale;
-            it.random = random_in ? random_in[event] : 0.5;
+    // 2. every buffer of the call at its size before anything is queued
+    const size_t n = umami_provider.particle_count;
+    size_t ext = 0, vals = 0;
+    for (Chunk &ch : chunks) {
+        ch.external = ext;
+        ch.values = vals;
+        for (size_t k = 0; k < nclasses; k++) {
+            size_t m = ch.first[k + 1] - ch.first[k];
+            ext += 4 * n * m;
+            vals += (size_t)std::max<uint32_t>(in->classes[k].colour->live, 1) * m;
         }
     }
-    // 3. - 5. on the device
-    UmamiStatus status = evaluate(in, first, nitems, momenta, stride, offset, count, mode);
-    if (status != UMAMI_SUCCESS) return status;
+    if (!in->momenta.reserve(4 * n * count) || !in->items.reserve(nitems) || !in->value_out.reserve(nitems) ||
+        !in->chosen_out.reserve(nitems) || !in->host_items.reserve(nitems) || !in->host_value.reserve(nitems) ||
+        !in->host_chosen.reserve(nitems) || !in->bad.reserve(1) || !in->host_bad.reserve(1) ||
+        !in->groups.reserve(kChunks * nclasses) || !in->host_groups.reserve(kChunks * nclasses) ||
+        !in->external.reserve(ext) || !in->values.reserve(vals))
+        return UMAMI_ERROR;
+    in->host_bad.p[0] = 0;
+    if (cuda_failed(cudaMemcpyAsync(in->bad.p, in->host_bad.p, sizeof(int), cudaMemcpyHostToDevice, in->copies),
+                    "flag"))
+        return UMAMI_ERROR;
+    // 3. per chunk: its items grouped by class, events in order within a class (a counting sort;
+    // `at` is each event-ordered item's place), then its work queued while the host goes on
+    std::vector<uint32_t> at(nitems);
+    UmamiStatus status = UMAMI_SUCCESS;
+    for (size_t c = 0; c < nchunks && status == UMAMI_SUCCESS; c++) {
+        const Chunk &ch = chunks[c];
+        std::vector<uint32_t> next(ch.first.begin(), ch.first.end() - 1);
+        for (size_t e = ch.e0, k = ch.item0; e < ch.e1; ++e) {
+            size_t event = offset + e, channel = selection[e] >> 16, flavour = selection[e] & 0xffff;
+            const UmamiFlavour &sel = umami_provider.channels[channel].flavours[flavour];
+            for (size_t j = 0; j < sel.contribution_count; ++j, ++k) {
+                const UmamiContribution *entry = &sel.contributions[j];
+                const PacudaProcess *p = process_of(in, entry->process_index);
+                double a = alpha_in ? alpha_in[event] : in->alpha_s[entry->process_index];
+                double scale = 1.0;
+                if (!p->alpha_s_name.empty() && a != p->alpha_s) scale = pow(a / p->alpha_s, p->qcd_power);
+                uint32_t place = next[in->class_of[channel][flavour][j]]++;
+                at[k] = (uint32_t)ch.item0 + place;
+                ItemIn &it = in->host_items.p[ch.item0 + place];
+                it.event = (uint32_t)(e - ch.e0);
+                it.helicity = helicity_in ? entry->helicity_runtime[helicity_in[event]] : -1;
+                it.scale = scale;
+                it.random = random_in ? random_in[event] : 0.5;
+            }
+        }
+        status = launch_chunk(in, (int)c, ch, momenta, stride, offset, mode);
+    }
+    // 4. the results (and whether every momentum was finite) back
+    if (status == UMAMI_SUCCESS &&
+        cuda_failed(cudaMemcpyAsync(in->host_bad.p, in->bad.p, sizeof(int), cudaMemcpyDeviceToHost, in->stream),
+                    "flag"))
+        status = UMAMI_ERROR;
+    bool synced = !cuda_failed(cudaStreamSynchronize(in->stream), "evaluation") &&
+                  !cuda_failed(cudaStreamSynchronize(in->copies), "copies");
+    if (status != UMAMI_SUCCESS || !synced) return UMAMI_ERROR;
+    if (in->host_bad.p[0]) return UMAMI_ERROR;  // a momentum that is not finite
 
     // 6. the events, combined as the reference does
     const double *value = in->host_value.p;

@@ -134,3 +134,25 @@ def test_parameters(umami):
         assert same_bits(me[OFFSET:OFFSET + COUNT], want)
     finally:
         assert lib.umami_set_parameter(h, b"aS", 0.118, 0.0) == 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", ["sum", "sample"])
+def test_a_call_of_several_chunks(umami, mode):
+    """A call of more than 2^17 events is evaluated in chunks whose host and device work overlap."""
+    from oracle import oracle as O
+
+    count, stride, offset = 3 * 65536 + 123, 3 * 65536 + 200, 11
+    m, p, channel, flavour = U.events(count, stride, offset, seed=23, single=mode == "sample")
+    random = np.random.default_rng(9).random(stride)
+    me, hel = np.full(stride, -1.0), np.full(stride, -1, np.int32)
+    ins = [(0, m), (2, flavour), (8, channel)]
+    outs = [(0, me)]
+    if mode == "sample":
+        ins.append((4, random))
+        outs.append((3, hel))
+    assert call(umami, ins, outs, count=count, stride=stride, offset=offset) == 0
+    want_me, _, want_hel = U.expected(p, channel, flavour, offset, mode, O, random=random)
+    assert same_bits(me[offset:offset + count], want_me)
+    if mode == "sample":
+        assert np.array_equal(hel[offset:offset + count], want_hel)

@@ -67,75 +67,85 @@ def events(count, stride, offset, seed=11, single=False):
     return m, p, channel, flavour
 
 
+_TEMPLATES = {}
+
+
+def template(name):
+    if name not in _TEMPLATES:
+        _TEMPLATES[name] = processes.template(name)
+    return _TEMPLATES[name]
+
+
 def contribution_values(p, entry, oracle):
     """Per event (point-major p), the contribution's helicity values (f64, resolved from zero) of
     its process at its permuted (and crossed) momenta, from the oracle."""
-    proc = SPEC["processes"][entry["process"]]
-    name = proc["key"]
+    name = SPEC["processes"][entry["process"]]["key"]
     crossing = CROSSING if name == "qg>qgg" else [(l, 1.0) for l in range(LEGS)]
     q = np.empty_like(p)
     for l, (source, sign) in enumerate(crossing):
         q[:, l, :] = sign * p[:, entry["permutation"][source], :]
-    _, out = oracle.evaluate(processes.template(name), q, kernel=1)
+    _, out = oracle.evaluate(template(name), q, kernel=1)
     return out  # [event][helicity]
 
 
 def expected(p, channel, flavour, offset, mode, oracle, alpha=None, random=None, helicity=None):
-    """|M|^2, colour index and helicity label per event as the reference library computes them."""
+    """|M|^2, colour index and helicity label per event as the reference library computes them.
+    Vectorised over events; every sum and draw runs over the helicities in order, so each value
+    is the one the scalar arithmetic gives."""
     count = p.shape[0]
-    cache = {}
+    ch = np.asarray(channel[offset:offset + count])
+    fl = np.asarray(flavour[offset:offset + count])
     me, col, hel = np.zeros(count), np.zeros(count, np.int32), np.zeros(count, np.int32)
-    for e in range(count):
-        sel = SPEC["channels"][channel[offset + e]][flavour[offset + e]]
-        first = sel[0]
-        total, label = 0.0, 0
-        vals = []
-        for entry in sel:
-            key = (entry["process"], tuple(entry["permutation"]))
-            if key not in cache:
-                cache[key] = contribution_values(p, entry, oracle)
-            t = processes.template(SPEC["processes"][entry["process"]]["key"])
-            num, den = t.meta["group_factor"]
-            a0, power = t.meta["alpha_s"], t.meta["qcd_power"]
-            a = a0 if alpha is None else alpha[offset + e]
-            scale = 1.0 if a == a0 else math.pow(a / a0, power)
-            v = []
-            for x in cache[key][e]:
-                if t.offsets[len(v) + 1] > t.offsets[len(v)]:
-                    if num != den:
-                        x = x * float(num) / float(den)
-                    if scale != 1.0:
-                        x = x * scale
-                else:
-                    x = 0.0
-                v.append(x)
-            vals.append(v)
-        if mode == "helicity":
-            label = int(helicity[offset + e])
-            for entry, v in zip(sel, vals):
-                total += entry["factor"] * v[label]
-        elif mode == "sample":
-            v = vals[0]
-            t = processes.template(SPEC["processes"][first["process"]]["key"])
-            live = [h for h in range(t.outputs) if t.offsets[h + 1] > t.offsets[h]]
-            s = 0.0
-            for h in live:
-                s = s + v[h]
-            target, cumulative, pick = random[offset + e] * s, 0.0, 0
-            for h in live:
-                if v[h] <= 0.0:
-                    continue
-                pick = h
-                cumulative = cumulative + v[h]
-                if cumulative > target:
-                    break
-            total = s * first["factor"]
-            label = pick
-        else:
-            for entry, v in zip(sel, vals):
-                value = 0.0
-                for x in v:
-                    value += x
-                total += entry["factor"] * value
-        me[e], col[e], hel[e] = total, first.get("color_index", 0), label
+    cache = {}
+    for c, channel_spec in enumerate(SPEC["channels"]):
+        for f, sel in enumerate(channel_spec):
+            ev = np.nonzero((ch == c) & (fl == f))[0]
+            if ev.size == 0:
+                continue
+            vals = []
+            for entry in sel:
+                key = (entry["process"], tuple(entry["permutation"]))
+                if key not in cache:
+                    cache[key] = contribution_values(p, entry, oracle)
+                t = template(SPEC["processes"][entry["process"]]["key"])
+                num, den = t.meta["group_factor"]
+                a0, power = t.meta["alpha_s"], t.meta["qcd_power"]
+                a = np.full(ev.size, a0) if alpha is None else np.asarray(alpha[offset + ev], np.float64)
+                scale = np.array([1.0 if x == a0 else math.pow(x / a0, power) for x in a])
+                v = cache[key][ev].copy()
+                live = np.array([t.offsets[h + 1] > t.offsets[h] for h in range(t.outputs)])
+                if num != den:
+                    v = v * float(num) / float(den)
+                v = np.where(scale[:, None] != 1.0, v * scale[:, None], v)
+                v[:, ~live] = 0.0
+                vals.append((entry, v, live))
+            first = sel[0]
+            total = np.zeros(ev.size)
+            label = np.zeros(ev.size, np.int32)
+            if mode == "helicity":
+                label = np.asarray(helicity[offset + ev], np.int32)
+                for entry, v, _ in vals:
+                    total = total + entry["factor"] * v[np.arange(ev.size), label]
+            elif mode == "sample":
+                _, v, live = vals[0]
+                hs = np.nonzero(live)[0]
+                s = np.zeros(ev.size)
+                for h in hs:
+                    s = s + v[:, h]
+                target = np.asarray(random[offset + ev]) * s
+                cumulative, pick, active = np.zeros(ev.size), np.zeros(ev.size, np.int32), np.ones(ev.size, bool)
+                for h in hs:
+                    take = active & (v[:, h] > 0.0)
+                    pick = np.where(take, h, pick)
+                    cumulative = np.where(take, cumulative + v[:, h], cumulative)
+                    active = active & ~(take & (cumulative > target))
+                total = s * first["factor"]
+                label = pick
+            else:
+                for entry, v, _ in vals:
+                    value = np.zeros(ev.size)
+                    for h in range(v.shape[1]):
+                        value = value + v[:, h]
+                    total = total + entry["factor"] * value
+            me[ev], col[ev], hel[ev] = total, first.get("color_index", 0), label
     return me, col, hel
