@@ -227,6 +227,7 @@ struct Instance {
     std::vector<std::vector<std::vector<uint32_t>>> class_of;  // [channel][flavour][contribution]
     cudaStream_t stream = nullptr, copies = nullptr;  // compute; and the copies in
     cudaEvent_t arrived[kChunks] = {nullptr};         // a chunk's inputs are on the device
+    cudaEvent_t done[kChunks] = {nullptr};            // a chunk's results are on the host
     DeviceArray<uint32_t> live_helicity;  // every colour's live helicities
     // the call's buffers
     DeviceArray<double> momenta, external, values, value_out;
@@ -296,6 +297,7 @@ void free_instance(Instance *in) {
     for (int c = 0; c < kChunks; c++) {
         pacuda_b200_batch_destroy(in->batch[c]);
         if (in->arrived[c]) cudaEventDestroy(in->arrived[c]);
+        if (in->done[c]) cudaEventDestroy(in->done[c]);
     }
     for (auto &v : in->colours)
         for (Colour &c : v) pacuda_b200_plan_destroy(c.plan);
@@ -499,7 +501,8 @@ UMAMI_EXPORT UmamiStatus umami_initialize(UmamiHandle *handle, char const *param
     bool streams = !cuda_failed(cudaStreamCreateWithFlags(&in->stream, cudaStreamNonBlocking), "stream") &&
                    !cuda_failed(cudaStreamCreateWithFlags(&in->copies, cudaStreamNonBlocking), "stream");
     for (int c = 0; streams && c < kChunks; c++)
-        streams = !cuda_failed(cudaEventCreateWithFlags(&in->arrived[c], cudaEventDisableTiming), "event");
+        streams = !cuda_failed(cudaEventCreateWithFlags(&in->arrived[c], cudaEventDisableTiming), "event") &&
+                  !cuda_failed(cudaEventCreateWithFlags(&in->done[c], cudaEventDisableTiming), "event");
     if (f.kernel > PACMAN_RECURRENCE_KERNEL_MIXED64 || !streams) {
         fprintf(stderr, "%s: kernel kind %u\n", kTag, f.kernel);
         free_instance(in);
@@ -686,80 +689,85 @@ UMAMI_EXPORT UmamiStatus umami_matrix_element(UmamiHandle handle, size_t count, 
     const double *alpha_in = (const double *)in_[UMAMI_IN_ALPHA_S];
     const int mode = helicity_in ? MODE_HELICITY : out_[UMAMI_OUT_HELICITY_INDEX] ? MODE_SAMPLE : MODE_SUM;
 
-    // 1. every event's selection, checked as the reference checks them before anything is
-    // evaluated; the chunks and each chunk's item count per class
+    // The call in chunks of events. Per chunk the host checks its events (as the reference checks
+    // them), groups its items by class and queues its device work, then goes on with the next
+    // chunk while the device runs; a chunk's events are combined as soon as its results are back.
+    // Nothing reaches the caller's outputs until every chunk has been checked and every momentum
+    // found finite, as in the reference (which checks all inputs before it evaluates).
+    const size_t n = umami_provider.particle_count, nclasses = in->classes.size();
     const size_t nchunks = std::min<size_t>(kChunks, std::max<size_t>(1, count / kChunkEvents));
+    // every buffer at its largest for this call, before anything is queued
+    size_t most_items = 0, most_values = 1;
+    for (size_t c = 0; c < umami_provider.channel_count; c++)
+        for (size_t f = 0; f < umami_provider.channels[c].flavour_count; f++)
+            most_items = std::max(most_items, umami_provider.channels[c].flavours[f].contribution_count);
+    for (const Class &cls : in->classes) most_values = std::max<size_t>(most_values, cls.colour->live);
+    const size_t cap = count * most_items;
+    if (!in->momenta.reserve(4 * n * count) || !in->items.reserve(cap) || !in->value_out.reserve(cap) ||
+        !in->chosen_out.reserve(cap) || !in->host_items.reserve(cap) || !in->host_value.reserve(cap) ||
+        !in->host_chosen.reserve(cap) || !in->bad.reserve(1) || !in->host_bad.reserve(1) ||
+        !in->groups.reserve(kChunks * nclasses) || !in->host_groups.reserve(kChunks * nclasses) ||
+        !in->external.reserve(4 * n * cap) || !in->values.reserve(most_values * cap))
+        return UMAMI_ERROR;
+    auto drain = [&]() {  // queued copies read the caller's memory: they end before the call returns
+        bool ok = !cuda_failed(cudaStreamSynchronize(in->stream), "evaluation");
+        return !cuda_failed(cudaStreamSynchronize(in->copies), "copies") && ok;
+    };
+    in->host_bad.p[0] = 0;
+    if (cuda_failed(cudaMemcpyAsync(in->bad.p, in->host_bad.p, sizeof(int), cudaMemcpyHostToDevice, in->copies),
+                    "flag"))
+        return drain(), UMAMI_ERROR;
     std::vector<Chunk> chunks(nchunks);
-    const size_t nclasses = in->classes.size();
     std::vector<uint32_t> selection(count);  // per event: channel << 16 | flavour
-    size_t nitems = 0;
+    std::vector<uint32_t> at(cap);           // per event-ordered item: its place among the items
+    size_t items_so_far = 0, ext = 0, vals = 0;
     for (size_t c = 0; c < nchunks; c++) {
         Chunk &ch = chunks[c];
         ch.e0 = count * c / nchunks;
         ch.e1 = count * (c + 1) / nchunks;
-        ch.item0 = nitems;
+        ch.item0 = items_so_far;
         ch.first.assign(nclasses + 1, 0);
+        // its events' selections and its item count per class
         for (size_t e = ch.e0; e < ch.e1; ++e) {
             size_t event = offset + e;
             size_t channel = channel_in ? channel_in[event] : 0;
             int flavour = flavour_in ? flavour_in[event] : 0;
             if (channel >= umami_provider.channel_count || flavour < 0 ||
                 (size_t)flavour >= umami_provider.channels[channel].flavour_count)
-                return UMAMI_ERROR;
+                return drain(), UMAMI_ERROR;
             const UmamiFlavour &sel = umami_provider.channels[channel].flavours[flavour];
-            if (sel.contribution_count == 0 || channel > 0xffff || flavour > 0xffff) return UMAMI_ERROR;
+            if (sel.contribution_count == 0 || channel > 0xffff || flavour > 0xffff) return drain(), UMAMI_ERROR;
             double random = random_in ? random_in[event] : 0.5;
-            if (!isfinite(random) || random < 0.0 || random >= 1.0) return UMAMI_ERROR;
+            if (!isfinite(random) || random < 0.0 || random >= 1.0) return drain(), UMAMI_ERROR;
             if (helicity_in) {
                 int label = helicity_in[event];
-                if (label < 0 || (size_t)label >= umami_provider.exported_helicity_count) return UMAMI_ERROR;
+                if (label < 0 || (size_t)label >= umami_provider.exported_helicity_count) return drain(), UMAMI_ERROR;
             } else if (out_[UMAMI_OUT_HELICITY_INDEX] && sel.contribution_count != 1) {
-                return UMAMI_ERROR_UNSUPPORTED_OUTPUT;
+                return drain(), UMAMI_ERROR_UNSUPPORTED_OUTPUT;
             }
             for (size_t j = 0; j < sel.contribution_count; ++j) {
                 const UmamiContribution *entry = &sel.contributions[j];
                 if (alpha_in) {
                     double a = alpha_in[event];
-                    if (!isfinite(a) || a < 0.0) return UMAMI_ERROR;
+                    if (!isfinite(a) || a < 0.0) return drain(), UMAMI_ERROR;
                     if (process_of(in, entry->process_index)->alpha_s_name.empty())
-                        return UMAMI_ERROR_UNSUPPORTED_INPUT;
+                        return drain(), UMAMI_ERROR_UNSUPPORTED_INPUT;
                 }
                 ch.first[in->class_of[channel][flavour][j] + 1]++;
             }
-            nitems += sel.contribution_count;
+            items_so_far += sel.contribution_count;
             selection[e] = (uint32_t)channel << 16 | (uint32_t)flavour;
         }
-        ch.items = nitems - ch.item0;
-        for (size_t k = 0; k < nclasses; k++) ch.first[k + 1] += ch.first[k];
-    }
-    // 2. every buffer of the call at its size before anything is queued
-    const size_t n = umami_provider.particle_count;
-    size_t ext = 0, vals = 0;
-    for (Chunk &ch : chunks) {
+        ch.items = items_so_far - ch.item0;
         ch.external = ext;
         ch.values = vals;
         for (size_t k = 0; k < nclasses; k++) {
-            size_t m = ch.first[k + 1] - ch.first[k];
+            size_t m = ch.first[k + 1];
             ext += 4 * n * m;
             vals += (size_t)std::max<uint32_t>(in->classes[k].colour->live, 1) * m;
+            ch.first[k + 1] += ch.first[k];
         }
-    }
-    if (!in->momenta.reserve(4 * n * count) || !in->items.reserve(nitems) || !in->value_out.reserve(nitems) ||
-        !in->chosen_out.reserve(nitems) || !in->host_items.reserve(nitems) || !in->host_value.reserve(nitems) ||
-        !in->host_chosen.reserve(nitems) || !in->bad.reserve(1) || !in->host_bad.reserve(1) ||
-        !in->groups.reserve(kChunks * nclasses) || !in->host_groups.reserve(kChunks * nclasses) ||
-        !in->external.reserve(ext) || !in->values.reserve(vals))
-        return UMAMI_ERROR;
-    in->host_bad.p[0] = 0;
-    if (cuda_failed(cudaMemcpyAsync(in->bad.p, in->host_bad.p, sizeof(int), cudaMemcpyHostToDevice, in->copies),
-                    "flag"))
-        return UMAMI_ERROR;
-    // 3. per chunk: its items grouped by class, events in order within a class (a counting sort;
-    // `at` is each event-ordered item's place), then its work queued while the host goes on
-    std::vector<uint32_t> at(nitems);
-    UmamiStatus status = UMAMI_SUCCESS;
-    for (size_t c = 0; c < nchunks && status == UMAMI_SUCCESS; c++) {
-        const Chunk &ch = chunks[c];
+        // its items grouped by class, events in order within a class (a counting sort)
         std::vector<uint32_t> next(ch.first.begin(), ch.first.end() - 1);
         for (size_t e = ch.e0, k = ch.item0; e < ch.e1; ++e) {
             size_t event = offset + e, channel = selection[e] >> 16, flavour = selection[e] & 0xffff;
@@ -779,45 +787,63 @@ UMAMI_EXPORT UmamiStatus umami_matrix_element(UmamiHandle handle, size_t count, 
                 it.random = random_in ? random_in[event] : 0.5;
             }
         }
-        status = launch_chunk(in, (int)c, ch, momenta, stride, offset, mode);
+        if (launch_chunk(in, (int)c, ch, momenta, stride, offset, mode) != UMAMI_SUCCESS ||
+            cuda_failed(cudaEventRecord(in->done[c], in->stream), "event"))
+            return drain(), UMAMI_ERROR;
     }
-    // 4. the results (and whether every momentum was finite) back
-    if (status == UMAMI_SUCCESS &&
-        cuda_failed(cudaMemcpyAsync(in->host_bad.p, in->bad.p, sizeof(int), cudaMemcpyDeviceToHost, in->stream),
+    if (cuda_failed(cudaMemcpyAsync(in->host_bad.p, in->bad.p, sizeof(int), cudaMemcpyDeviceToHost, in->stream),
                     "flag"))
-        status = UMAMI_ERROR;
-    bool synced = !cuda_failed(cudaStreamSynchronize(in->stream), "evaluation") &&
-                  !cuda_failed(cudaStreamSynchronize(in->copies), "copies");
-    if (status != UMAMI_SUCCESS || !synced) return UMAMI_ERROR;
-    if (in->host_bad.p[0]) return UMAMI_ERROR;  // a momentum that is not finite
+        return drain(), UMAMI_ERROR;
 
-    // 6. the events, combined as the reference does
-    const double *value = in->host_value.p;
-    for (size_t e = 0, k = 0; e < count; ++e) {
+    // the events combined as the reference does, chunk by chunk as the results come back; the
+    // first event whose |M|^2 is not finite ends the call (the events before it are written)
+    std::vector<double> total_of(count);
+    std::vector<int> label_of(count);
+    size_t good = count;
+    for (size_t c = 0; c < nchunks && good == count; c++) {
+        if (cuda_failed(cudaEventSynchronize(in->done[c]), "evaluation")) return drain(), UMAMI_ERROR;
+        const Chunk &ch = chunks[c];
+        const double *value = in->host_value.p;
+        for (size_t e = ch.e0, k = ch.item0; e < ch.e1; ++e) {
+            size_t event = offset + e;
+            const UmamiFlavour &sel = umami_provider.channels[selection[e] >> 16].flavours[selection[e] & 0xffff];
+            const UmamiContribution *head = &sel.contributions[0];
+            int label = 0;
+            double total = 0.0;
+            if (mode == MODE_HELICITY) {
+                label = helicity_in[event];
+                for (size_t j = 0; j < sel.contribution_count; ++j) {
+                    const UmamiContribution *entry = &sel.contributions[j];
+                    if (entry->helicity_runtime[label] < 0) continue;
+                    total += entry->factor * value[at[k + j]];
+                }
+            } else if (mode == MODE_SAMPLE) {
+                total = value[at[k]];
+                label = head->helicity_export[in->host_chosen.p[at[k]]];
+                total *= head->factor;
+            } else {
+                for (size_t j = 0; j < sel.contribution_count; ++j)
+                    total += sel.contributions[j].factor * value[at[k + j]];
+            }
+            k += sel.contribution_count;
+            if (!isfinite(total)) {
+                good = e;
+                break;
+            }
+            total_of[e] = total;
+            label_of[e] = label;
+        }
+    }
+    if (!drain()) return UMAMI_ERROR;
+    if (in->host_bad.p[0]) return UMAMI_ERROR;  // a momentum that is not finite
+    for (size_t e = 0; e < good; ++e) {
         size_t event = offset + e;
         const UmamiFlavour &sel = umami_provider.channels[selection[e] >> 16].flavours[selection[e] & 0xffff];
-        const UmamiContribution *head = &sel.contributions[0];
-        int label = 0;
-        double total = 0.0;
-        if (mode == MODE_HELICITY) {
-            label = helicity_in[event];
-            for (size_t j = 0; j < sel.contribution_count; ++j) {
-                const UmamiContribution *entry = &sel.contributions[j];
-                if (entry->helicity_runtime[label] < 0) continue;
-                total += entry->factor * value[at[k + j]];
-            }
-        } else if (mode == MODE_SAMPLE) {
-            total = value[at[k]];
-            label = head->helicity_export[in->host_chosen.p[at[k]]];
-            total *= head->factor;
-        } else {
-            for (size_t j = 0; j < sel.contribution_count; ++j) total += sel.contributions[j].factor * value[at[k + j]];
-        }
-        k += sel.contribution_count;
-        if (!isfinite(total)) return UMAMI_ERROR;
-        if (out_[UMAMI_OUT_MATRIX_ELEMENT]) ((double *)out_[UMAMI_OUT_MATRIX_ELEMENT])[event] = total;
-        if (out_[UMAMI_OUT_HELICITY_INDEX]) ((int *)out_[UMAMI_OUT_HELICITY_INDEX])[event] = label;
-        if (out_[UMAMI_OUT_COLOR_INDEX]) ((int *)out_[UMAMI_OUT_COLOR_INDEX])[event] = (int)head->color_index;
+        if (out_[UMAMI_OUT_MATRIX_ELEMENT]) ((double *)out_[UMAMI_OUT_MATRIX_ELEMENT])[event] = total_of[e];
+        if (out_[UMAMI_OUT_HELICITY_INDEX]) ((int *)out_[UMAMI_OUT_HELICITY_INDEX])[event] = label_of[e];
+        if (out_[UMAMI_OUT_COLOR_INDEX])
+            ((int *)out_[UMAMI_OUT_COLOR_INDEX])[event] = (int)sel.contributions[0].color_index;
     }
+    if (good != count) return UMAMI_ERROR;
     return UMAMI_SUCCESS;
 }
