@@ -267,6 +267,7 @@ extern "C" pacuda_b200_plan *pacuda_b200_plan_create(const pacman_recurrence_cal
               to_device(&p->red_weights, weights, offsets[outputs]) && upload_schedule(p->tiled, tiled_threads(p->kernel), 0) &&
               !failed(cudaDeviceSynchronize(), "plan upload");
     if (!ok) {
+        if (!p->tiled.host.why.empty()) fprintf(stderr, "%s: plan_create: %s\n", kTag, p->tiled.host.why.c_str());
         pacuda_b200_plan_destroy(p);
         return nullptr;
     }

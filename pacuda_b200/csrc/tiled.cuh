@@ -22,8 +22,8 @@
 namespace pacuda {
 
 struct TiledPlan {
-    // the schedule
-    const Ins *ins;
+    // the schedule (instructions in the 16-byte form: pack_ins)
+    const uint4 *ins;
     const uint32_t *task_first;   // per task, its instructions (tasks + 1 entries)
     const uint32_t *order;        // per level position, its task's (first, end) instructions; lane = position % G
     const uint32_t *level_first;  // levels + 1 entries into order
@@ -65,6 +65,22 @@ struct TiledLaunch {
     size_t ld;
     uint32_t const_bytes;                  // shared memory kept for a plan's constants
 };
+
+// The on-chip executor's 16-byte instruction: kind | op << 4 | flags << 8 | form 0 << 16 |
+// form 1 << 24, then (a, b), (c, s), (x, y) as 16-bit pairs. Every field of a plan whose points fit
+// shared memory fits (slots and constant indices below 65536, forms below 256); the host checks.
+__device__ __forceinline__ Ins unpack_ins(uint4 w) {
+    Ins o;
+    o.head = w.x & 0xffff;
+    o.f = ((w.x >> 16) & 0xff) | (w.x >> 24) << 16;
+    o.a = w.y & 0xffff;
+    o.b = w.y >> 16;
+    o.c = w.z & 0xffff;
+    o.s = w.z >> 16;
+    o.x = w.w & 0xffff;
+    o.y = w.w >> 16;
+    return o;
+}
 
 // a complex value as shared memory holds it: (re, im) side by side, one 8- or 16-byte access
 template <class R> struct alignas(2 * sizeof(R)) Pair {
@@ -219,7 +235,7 @@ __global__ void __launch_bounds__(512, 1) run_tiled(TiledLaunch L) {
             }
         }
         __syncthreads();  // the constants, forms and live-in values are in
-        const Ins *ins = p.ins;
+        const uint4 *ins = p.ins;
         const uint2 *order = reinterpret_cast<const uint2 *>(p.order);
         for (uint32_t lv = 0; lv < levels; lv++) {
             const uint32_t j0 = __ldg(p.level_first + lv), j1 = active ? __ldg(p.level_first + lv + 1) : 0;
@@ -228,7 +244,7 @@ __global__ void __launch_bounds__(512, 1) run_tiled(TiledLaunch L) {
                     uint2 r = __ldg(order + j);
                     // sources: f64 wavefunctions from the f64 forms and constants, narrowed
                     for (uint32_t n = r.x; n < r.y; n++) {
-                        Ins o = load_ins(ins, n);
+                        Ins o = unpack_ins(__ldg(ins + n));
                         double mom[4];
                         for (int c = 0; c < 4; c++) mom[c] = forms64[(o.f * 4 + c) * np + pw];
                         double fr = __ldg(p.f64 + o.x), fi = __ldg(p.f64 + p.factors + o.x), mass = __ldg(p.s64 + o.s);
@@ -255,7 +271,13 @@ __global__ void __launch_bounds__(512, 1) run_tiled(TiledLaunch L) {
                     Cx<R> acc[6];
 #pragma unroll
                     for (int c = 0; c < 6; c++) acc[c] = cx(konst<R>(0.0), konst<R>(0.0));
-                    for (uint32_t n = cur.x; n < cur.y; n++) exec_row<K>(v, load_ins(ins, n), acc);
+                    // each next instruction is fetched while its predecessor runs
+                    uint4 next = __ldg(ins + cur.x);
+                    for (uint32_t n = cur.x; n < cur.y; n++) {
+                        const uint4 now = next;
+                        if (n + 1 < cur.y) next = __ldg(ins + n + 1);
+                        exec_row<K>(v, unpack_ins(now), acc);
+                    }
                 }
             }
             __syncthreads();

@@ -42,8 +42,28 @@ void TiledDevice::release() {
     ok = false;
 }
 
+bool pack_ins(const Ins &i, uint4 &w) {
+    // (a closure's f records its global amplitude plane for the host; the executor reads its slot)
+    uint32_t f = ins_kind(i) == K_CLOSURE ? 0 : i.f, f0 = f & 0xffff, f1 = f >> 16;
+    if (ins_flags(i) > 255 || f0 > 255 || f1 > 255 || i.a > 0xffff || i.b > 0xffff || i.c > 0xffff || i.s > 0xffff ||
+        i.x > 0xffff || i.y > 0xffff)
+        return false;
+    w.x = (i.head & 0xffff) | f0 << 16 | f1 << 24;
+    w.y = i.a | i.b << 16;
+    w.z = i.c | i.s << 16;
+    w.w = i.x | i.y << 16;
+    return true;
+}
+
 bool upload_schedule(TiledDevice &t, int threads, cudaStream_t s) {
-    t.ok = threads > 0 && put(&t.ins, t.host.ins, s) && put(&t.task_first, t.host.task_first, s) &&
+    std::vector<uint4> packed(t.host.ins.size());
+    for (size_t n = 0; n < packed.size(); n++)
+        if (!pack_ins(t.host.ins[n], packed[n])) {
+            t.host.why = "an instruction's field does not fit the on-chip executor's 16-byte form";
+            t.ok = false;
+            return false;
+        }
+    t.ok = threads > 0 && put(&t.ins, packed, s) && put(&t.task_first, t.host.task_first, s) &&
            put(&t.loads, t.host.loads, s) && put(&t.amp_planes, t.host.amp_planes, s);
     t.levels = (uint32_t)t.host.level_first.size() - 1;
     t.threads = threads;

@@ -18,7 +18,7 @@ inline uint32_t tiled_lanes(uint32_t points, int threads) { return (uint32_t)(th
 
 struct TiledDevice {
     Schedule host;
-    Ins *ins = nullptr;
+    uint4 *ins = nullptr;  // the schedule's instructions, packed (pack_ins)
     uint32_t *task_first = nullptr, *loads = nullptr, *amp_planes = nullptr;
     // per points-per-block count P: the lane order for threads / P lanes and its level
     // boundaries, concatenated (offsets in 32-bit words, index P - 1)
@@ -33,8 +33,12 @@ struct TiledDevice {
 // bytes of shared memory a block needs for one plan's constants (scales and factors, re and im)
 size_t tiled_const_bytes(uint32_t scales, uint32_t factors);
 
+// an instruction in the on-chip executor's 16-byte form (tiled.cuh unpack_ins); false when a field
+// does not fit it
+bool pack_ins(const Ins &i, uint4 &w);
+
 // the schedule's arrays on the device, with the lane orders of every points-per-block count for
-// blocks of `threads`
+// blocks of `threads`; false (with the reason in t.host.why) when an instruction does not pack
 bool upload_schedule(TiledDevice &t, int threads, cudaStream_t stream);
 
 // bytes of shared memory one point needs (kernel: PACMAN_RECURRENCE_KERNEL_*), 16-aligned
