@@ -237,6 +237,8 @@ extern "C" pacuda_b200_plan *pacuda_b200_plan_create(const pacman_recurrence_cal
         delete p;
         return nullptr;
     }
+    // the plan only reduces its amplitudes: where it can, keep each amplitude's term instead
+    use_terms(p->tiled.host, offsets, planes, outputs, c->amplitude_planes);
     p->forms = forms;
     p->scales = c->scale_count;
     p->factors = c->factor_count;

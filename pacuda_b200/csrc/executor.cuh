@@ -62,6 +62,8 @@ template <class K> struct PointView {
     }
     // the global arena is the storage: nothing to write back
     __device__ __forceinline__ void writeback(uint32_t, const Cx<R> *, int) const {}
+    // (its schedules keep amplitudes: no closure stores a reduction term)
+    template <class A> __device__ __forceinline__ void put_term(uint32_t, A, A) const {}
 };
 
 template <class K, int OP, class V>
@@ -128,7 +130,13 @@ __device__ __forceinline__ void exec_closure(const V &v, const Ins &o, const Cx<
     typedef typename K::Amp Amp;
     Cx<R> f = v.factor(o.x);
     Amp dr, di;
-    v.amp(o.c, dr, di);
+    const bool term = ins_flags(o) & 64;  // F_TERM: the amplitude's only closure, from zero
+    if (term) {
+        dr = konst<Amp>(0.0);
+        di = konst<Amp>(0.0);
+    } else {
+        v.amp(o.c, dr, di);
+    }
     if (ins_flags(o) & 16) {
         // parent 0 is the task's sums (at most 6 components): indices known at compile time keep
         // the sums in registers
@@ -147,7 +155,8 @@ __device__ __forceinline__ void exec_closure(const V &v, const Ins &o, const Cx<
             di = di + amp_of(t.im, (Amp *)nullptr);
         }
     }
-    v.put_amp(o.c, dr, di);
+    if (!term) v.put_amp(o.c, dr, di);
+    else if (o.c != 0xffff) v.put_term(o.c, dr, di);
 }
 
 // identity (op 10) and clear (op 1) over `o.b` components

@@ -347,6 +347,15 @@ bool build_schedule(const Program &p, uint32_t P, uint32_t A, Schedule &out) {
         active.emplace(glast[g], std::make_pair(slot, gsize[g]));
     }
     out.cur_slots = top;
+    {
+        int levels_n = 0;
+        for (uint32_t g = 0; g < G; g++) levels_n = std::max(levels_n, glast[g] + 1);
+        std::vector<uint32_t> live((size_t)std::max(levels_n, 1), 0);
+        for (uint32_t g = 0; g < G; g++)
+            if (!in_register[g] && glast[g] >= 0)
+                for (int l = gfirst[g]; l <= glast[g]; l++) live[l] += gsize[g];
+        out.peak_live = *std::max_element(live.begin(), live.end());
+    }
     auto slot_of = [&](uint32_t plane) {
         uint32_t g = group_of[plane];
         return in_register[g] ? 0u : gslot[g] + (plane - gbase[g]);
@@ -433,6 +442,27 @@ void lane_order(const Schedule &s, uint32_t lanes, std::vector<uint32_t> &order,
             for (uint32_t l = 0; l < L; l++) order.push_back(r < lane[l].size() ? lane[l][r] : ~0u);
         level_first.push_back((uint32_t)order.size());
     }
+}
+
+bool use_terms(Schedule &s, const uint32_t *offsets, const uint32_t *planes, uint32_t outputs, uint32_t amplitude_planes) {
+    const uint32_t T = offsets[outputs];
+    if (T >= 0xffff) return false;
+    std::vector<uint32_t> term_of(amplitude_planes, 0xffff), rows(amplitude_planes, 0);
+    for (uint32_t k = 0; k < T; k++) {
+        if (planes[k] >= amplitude_planes || term_of[planes[k]] != 0xffff) return false;  // one term per amplitude
+        term_of[planes[k]] = k;
+    }
+    for (const Ins &i : s.ins)
+        if (ins_kind(i) == K_CLOSURE && ++rows[i.f] > 1) return false;  // (a closure's f is its amplitude plane)
+    for (Ins &i : s.ins)
+        if (ins_kind(i) == K_CLOSURE) {
+            i.head |= F_TERM << 8;
+            i.c = term_of[i.f];
+        }
+    s.terms = T;
+    s.amp_slots = 0;
+    s.amp_planes.clear();
+    return true;
 }
 
 }  // namespace pacuda

@@ -29,6 +29,7 @@ struct TiledPlan {
     const uint32_t *level_first;  // levels + 1 entries into order
     uint32_t levels;
     uint32_t cur_slots, amp_slots, forms;
+    uint32_t terms;               // reduction terms kept instead of amplitudes (batch mode), or 0
     uint32_t points;              // P points per block
     uint32_t lanes;               // G lanes per point: warps * floor(32 / P)
     uint32_t point_bytes;         // shared memory of one point
@@ -87,6 +88,9 @@ template <class R> struct alignas(2 * sizeof(R)) Pair {
     R re, im;
 };
 
+__device__ __forceinline__ double to_f64_value(double x) { return x; }
+__device__ __forceinline__ double to_f64_value(D x) { return __dadd_rn((double)x.hi, (double)x.lo); }
+
 // the C ABI's mode: where an item's points write their planes back (thread 0 sets it per item;
 // in shared memory so that no lane holds these in registers through its tasks)
 struct AbiItem {
@@ -104,6 +108,8 @@ template <class K, bool ABI> struct SlotView {
     typedef typename K::Const Const;
     Pair<R> *cur_;        // [slot][points of the region]
     Pair<Amp> *amp_;      // [amplitude slot][points of the region]
+    double *term_;        // [reduction term][points] (a schedule that keeps terms)
+    const double *tw;     // the reduction's weights
     const Den *mom;
     const Const *sre, *sim, *fre, *fim;  // the plan's constants, in shared memory
     uint32_t np, pw;      // the block's points (interleaved) and this thread's
@@ -126,6 +132,11 @@ template <class K, bool ABI> struct SlotView {
         re = v.re;
         im = v.im;
     }
+    // a reduction term: weight x fma(re, re, im x im), the resolved reduction's arithmetic
+    __device__ __forceinline__ void put_term(uint32_t t, Amp re, Amp im) const {
+        double r = to_f64_value(re), i = to_f64_value(im);
+        term_[at(t)] = __dmul_rn(__ldg(tw + t), __fma_rn(r, r, __dmul_rn(i, i)));
+    }
     __device__ __forceinline__ void put_amp(uint32_t a, Amp re, Amp im) const {
         Pair<Amp> x;
         x.re = re;
@@ -147,8 +158,6 @@ template <class K, bool ABI> struct SlotView {
     }
 };
 
-__device__ __forceinline__ double to_f64_value(double x) { return x; }
-__device__ __forceinline__ double to_f64_value(D x) { return __dadd_rn((double)x.hi, (double)x.lo); }
 
 // ABI: the C ABI's mode (arena in and out) or a batch's (outputs only)
 template <class K, bool ABI>
@@ -187,7 +196,9 @@ __global__ void __launch_bounds__(512, 1) run_tiled(TiledLaunch L) {
         SlotView<K, ABI> v;
         v.cur_ = (Pair<R> *)(smem + L.const_bytes);
         v.amp_ = (Pair<Amp> *)(v.cur_ + (size_t)p.cur_slots * np);
-        double *forms64 = (double *)(v.amp_ + (size_t)p.amp_slots * np);
+        v.term_ = (double *)(v.amp_ + (size_t)p.amp_slots * np);
+        v.tw = p.red_weights;
+        double *forms64 = v.term_ + (size_t)p.terms * np;
         v.mom = (const Den *)forms64;
         v.sre = consts;
         v.sim = v.sre + p.scales;
@@ -232,6 +243,8 @@ __global__ void __launch_bounds__(512, 1) run_tiled(TiledLaunch L) {
                 }
             } else {
                 for (uint32_t a = tl; a < p.amp_slots; a += lanes) v.put_amp(a, konst<Amp>(0.0), konst<Amp>(0.0));
+                // a term whose amplitude no closure makes: the term of a zero amplitude
+                for (uint32_t t = tl; t < p.terms; t += lanes) v.put_term(t, konst<Amp>(0.0), konst<Amp>(0.0));
             }
         }
         __syncthreads();  // the constants, forms and live-in values are in
@@ -306,7 +319,13 @@ __global__ void __launch_bounds__(512, 1) run_tiled(TiledLaunch L) {
             // the resolved reduction from zero: out[point][o] = 0 + w fma(re, re, im im) + ...
             const size_t point = (size_t)(item - L.item_first[k]) * np + pw;
             double *out = L.output[k] + point * p.outputs;
-            for (uint32_t o = tl; o < p.outputs; o += lanes) {
+            for (uint32_t o = tl; p.terms && o < p.outputs; o += lanes) {
+                double acc = 0.0;
+                for (uint32_t j = __ldg(p.red_offsets + o), e = __ldg(p.red_offsets + o + 1); j < e; j++)
+                    acc = __dadd_rn(acc, v.term_[v.at(j)]);
+                out[o] = acc;
+            }
+            for (uint32_t o = tl; !p.terms && o < p.outputs; o += lanes) {
                 double acc = 0.0;
                 for (uint32_t j = __ldg(p.red_offsets + o), e = __ldg(p.red_offsets + o + 1); j < e; j++) {
                     uint32_t s = __ldg(p.red_slots + j);

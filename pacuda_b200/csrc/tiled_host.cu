@@ -90,7 +90,7 @@ size_t tiled_const_bytes(uint32_t scales, uint32_t factors) { return ((2 * (size
 
 size_t tiled_point_bytes(const Schedule &s, uint32_t forms, int kernel) {
     size_t value = kernel == PACMAN_RECURRENCE_KERNEL_MIXED || kernel == PACMAN_RECURRENCE_KERNEL_MIXED64 ? 4 : 8;
-    size_t per_point = 2 * value * s.cur_slots + 2 * 8 * s.amp_slots + 8 * 4 * (size_t)forms;
+    size_t per_point = 2 * value * s.cur_slots + 2 * 8 * s.amp_slots + 8 * (size_t)s.terms + 8 * 4 * (size_t)forms;
     return (per_point + 15) / 16 * 16;
 }
 
@@ -148,6 +148,7 @@ void describe(const TiledDevice &t, uint32_t forms, uint32_t points, size_t poin
     p.levels = t.levels;
     p.cur_slots = t.host.cur_slots;
     p.amp_slots = t.host.amp_slots;
+    p.terms = t.host.terms;
     p.forms = forms;
     p.points = points;
     p.lanes = tiled_lanes(points, t.threads);

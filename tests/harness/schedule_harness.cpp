@@ -11,7 +11,8 @@ using namespace pacuda;
 
 extern "C" {
 
-// stats[0..7] = rows, tasks, levels, cur_slots, amp_slots, max_task_len, live-in groups, max tasks per level
+// stats[0..8] = rows, tasks, levels, cur_slots, amp_slots, max_task_len, live-in groups, max tasks per
+// level, peak live current slots
 int schedule_stats(const uint64_t *words, uint32_t count, const uint8_t *width, uint32_t planes, uint32_t amps,
                    uint32_t forms, uint32_t scales, uint32_t factors, uint32_t *stats) {
     Program p;
@@ -30,6 +31,7 @@ int schedule_stats(const uint64_t *words, uint32_t count, const uint8_t *width, 
     uint32_t mx = 0;
     for (size_t l = 0; l + 1 < s.level_first.size(); l++) mx = std::max(mx, s.level_first[l + 1] - s.level_first[l]);
     stats[7] = mx;
+    stats[8] = s.peak_live;
     return 0;
 }
 

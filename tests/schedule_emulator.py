@@ -44,10 +44,10 @@ def _args(words, width, planes, amps, forms, scales, factors):
 
 def stats(words, width, planes, amps, forms, scales, factors):
     keep, a = _args(words, width, planes, amps, forms, scales, factors)
-    st = np.zeros(8, dtype=np.uint32)
+    st = np.zeros(9, dtype=np.uint32)
     assert lib().schedule_stats(*a, st.ctypes.data) == 0
     return dict(zip(["instructions", "tasks", "levels", "cur_slots", "amp_slots", "max_task_len", "live_in_groups",
-                     "max_tasks_per_level"], st.tolist()))
+                     "max_tasks_per_level", "peak_live"], st.tolist()))
 
 
 def export(words, width, planes, amps, forms, scales, factors):
