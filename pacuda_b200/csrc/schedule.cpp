@@ -172,6 +172,47 @@ bool build_schedule(const Program &p, uint32_t P, uint32_t A, Schedule &out) {
         tasks.push_back(t);
     }
 
+    // ---- propagators fused into the run of their current ----
+    // A propagator acts in place on the current a destination run wrote. When no task between
+    // the run and the propagator (in program order) reads or writes that current, the propagator
+    // can follow the run at once: the run's task applies it, and it needs no level of its own.
+    {
+        std::vector<std::vector<Range>> touched(tasks.size());
+        for (size_t ti = 0; ti < tasks.size(); ti++) {
+            std::vector<Range> r, w;
+            for (const Ins &i : tasks[ti].ins) access(i, r, w);
+            touched[ti] = r;
+            touched[ti].insert(touched[ti].end(), w.begin(), w.end());
+        }
+        auto overlaps = [](const std::vector<Range> &v, uint32_t first, uint32_t count) {
+            for (const Range &x : v)
+                if (x.first < first + count && first < x.first + x.count) return true;
+            return false;
+        };
+        std::vector<uint8_t> gone(tasks.size(), 0);
+        for (size_t ti = 0; ti < tasks.size(); ti++) {
+            if (tasks[ti].ins.size() != 1 || ins_kind(tasks[ti].ins[0]) != K_PROP) continue;
+            const Ins &prop = tasks[ti].ins[0];
+            const uint32_t m = ins_op(prop) == 9 ? 4 : 2;
+            for (size_t tj = ti; tj-- > 0;) {
+                if (gone[tj] || !overlaps(touched[tj], prop.a, m)) continue;
+                Task &run = tasks[tj];
+                const Ins &last = run.ins.back();
+                int c0, c1, cd;
+                contribution_shape(ins_op(last), &c0, &c1, &cd);
+                if (ins_kind(last) == K_CONTRIB && (ins_flags(last) & F_LAST) && last.c == prop.a && (uint32_t)cd == m) {
+                    run.ins.push_back(prop);
+                    gone[ti] = 1;
+                }
+                break;  // the nearest task that touches the current decides
+            }
+        }
+        std::vector<Task> kept;
+        for (size_t ti = 0; ti < tasks.size(); ti++)
+            if (!gone[ti]) kept.push_back(std::move(tasks[ti]));
+        tasks.swap(kept);
+    }
+
     // ---- closures fused into the task of their closing current ----
     // A closing current read by nothing but closures, whose amplitudes receive no other closure,
     // is computed, closed and forgotten by one task: the closures read its sums in registers and
