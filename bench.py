@@ -138,6 +138,41 @@ def reduce_over_ranks(dist, ms, sums):
     return float(t.item()), total
 
 
+def precision_line(torch, B, fams, ext, ref_out, steps, warmup, kind="mixed"):
+    """The same points in another kernel kind (mixed: f32 currents, df64 denominators and
+    amplitudes): its points/s on the device, and each point's relative error in its helicity sum
+    against the f64 run."""
+    plans, outs = [], []
+    for (name, t, p), e in zip(fams, ext):
+        plans.append(B.Plan(t, kind))
+        outs.append(torch.empty(p.shape[0] * t.outputs, dtype=torch.float64, device="cuda"))
+    batch = B.Batch(plans, ext, outs)
+    batch.tune()
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):
+        batch.capture(stream)
+    for _ in range(warmup):
+        batch.run(stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        batch.run(stream)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    rel = []
+    for (name, t, p), o, r in zip(fams, outs, ref_out):
+        x = o.view(p.shape[0], t.outputs).sum(dim=1)
+        y = r.view(p.shape[0], t.outputs).sum(dim=1)
+        rel.append(((x - y).abs() / y.abs().clamp_min(1e-300)).cpu().numpy())
+    rel = np.concatenate(rel)
+    n = rel.size
+    return {"kind": kind, "value": n / (ms * 1e-3), "unit": "points/s", "ms_per_step": ms,
+            "rel_error_vs_f64": {"median": float(np.median(rel)), "q999": float(np.quantile(rel, 0.999)),
+                                 "max": float(rel.max()), "frac_le_1e-10": float((rel <= 1e-10).mean())},
+            "lanes_per_point": {nm: pl.lanes_per_point for (nm, _, _), pl in zip(fams, plans)}}
+
+
 def dram_bytes_per_point():
     """DRAM bytes per point of the batch kernel, from the committed ncu summary (one capture of the
     same family mix), or None."""
@@ -311,6 +346,7 @@ def main():
     ap.add_argument("--points", type=int, default=POINTS, help="points per GPU")
     ap.add_argument("--no-tune", action="store_true", help="keep the default points per warp")
     ap.add_argument("--lanes-per-point", type=int, default=0)
+    ap.add_argument("--no-precision", action="store_true", help="skip the mixed-precision line")
     args = ap.parse_args()
     POINTS = args.points
     if args.family:
@@ -429,6 +465,9 @@ def main():
             res["e2e_abi"] = abi_line
         if not args.no_cpu:
             res["cpu_baseline"] = cpu_baseline(fams)
+        if not args.no_precision:
+            res["precision"] = [precision_line(torch, B, fams, ext, out, args.steps, args.warmup, k)
+                                for k in ("mixed", "mixed64", "df64")]
     if world > 1:
         import torch.distributed as dist
 
