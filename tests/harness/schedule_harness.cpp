@@ -76,3 +76,32 @@ int schedule_export(const uint64_t *words, uint32_t count, const uint8_t *width,
     return 0;
 }
 }
+
+extern "C" {
+// the schedule in reduction-term mode (use_terms with the reduction offsets[outputs + 1], planes):
+// sizes = ins, tasks + 1, levels + 1, applied (0/1), terms, cur_slots; arrays as schedule_export
+int schedule_export_terms(const uint64_t *words, uint32_t count, const uint8_t *width, uint32_t planes, uint32_t amps,
+                          uint32_t forms, uint32_t scales, uint32_t factors, const uint32_t *offsets,
+                          const uint32_t *red_planes, uint32_t outputs, uint32_t *sizes, uint32_t *ins,
+                          uint32_t *task_first, uint32_t *level_first) {
+    Program p;
+    Limits lim{planes, amps, forms, scales, factors};
+    BuildError e = build_program(words, count, width, true, lim, p);
+    if (e.status) return e.status;
+    Schedule s;
+    if (!build_schedule(p, planes, amps, s)) return -1;
+    bool applied = use_terms(s, offsets, red_planes, outputs, amps);
+    sizes[0] = (uint32_t)s.ins.size();
+    sizes[1] = (uint32_t)s.task_first.size();
+    sizes[2] = (uint32_t)s.level_first.size();
+    sizes[3] = applied;
+    sizes[4] = s.terms;
+    sizes[5] = s.cur_slots;
+    if (ins) {
+        memcpy(ins, s.ins.data(), s.ins.size() * sizeof(Ins));
+        memcpy(task_first, s.task_first.data(), s.task_first.size() * 4);
+        memcpy(level_first, s.level_first.data(), s.level_first.size() * 4);
+    }
+    return 0;
+}
+}

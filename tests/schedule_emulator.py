@@ -20,7 +20,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 HARNESS = os.path.join(HERE, "harness")
 LIB = os.path.join(HARNESS, "libschedule_harness.so")
 K_CONTRIB, K_PROP, K_IDENTITY, K_CLEAR, K_CLOSURE, K_SOURCE = 1, 2, 3, 4, 5, 6
-F_INIT, F_FIRST, F_LAST, F_WB, F_ACC0, F_NOSTORE = 1, 2, 4, 8, 16, 32
+F_INIT, F_FIRST, F_LAST, F_WB, F_ACC0, F_NOSTORE, F_TERM = 1, 2, 4, 8, 16, 32, 64
+ZERO = hash(("zero amplitude",))
 _lib = None
 
 
@@ -33,6 +34,7 @@ def lib():
         _lib.program_export.argtypes = sig + [C.c_void_p, C.c_void_p]
         _lib.schedule_export.argtypes = sig + [C.c_void_p] * 7
         _lib.schedule_stats.argtypes = sig + [C.c_void_p]
+        _lib.schedule_export_terms.argtypes = sig + [C.c_void_p, C.c_void_p, C.c_uint32] + [C.c_void_p] * 4
     return _lib
 
 
@@ -89,8 +91,8 @@ def _head(i):
 class _Store:
     """Values by address: planes of the arena, or slots."""
 
-    def __init__(self, get, put, amp_get, amp_put):
-        self.get, self.put, self.amp_get, self.amp_put = get, put, amp_get, amp_put
+    def __init__(self, get, put, amp_get, amp_put, term_put=None):
+        self.get, self.put, self.amp_get, self.amp_put, self.term_put = get, put, amp_get, amp_put, term_put
 
 
 def _row(store, i, acc, wb=None):
@@ -135,11 +137,15 @@ def _row(store, i, acc, wb=None):
             if wb and flags & F_WB:
                 wb(y + k, [0])
     elif kind == K_CLOSURE:
-        v = store.amp_get(c)
+        v = ZERO if flags & F_TERM else store.amp_get(c)
         for k in range(s):
             left = acc[k] if flags & F_ACC0 else store.get(a + k)
             v = hash(("closure", x, y + k, left, store.get(b + k), v))
-        store.amp_put(c, v)
+        if flags & F_TERM:
+            if c != 0xffff:
+                store.term_put(c, v)
+        else:
+            store.amp_put(c, v)
     elif kind == K_SOURCE:
         out = [hash(("source", y, f, x, s, k)) for k in range(_src_comps(y))]
         for k, v in enumerate(out):
@@ -194,3 +200,63 @@ def scheduled(ins, task_first, level_first, loads, amp_planes, cur_slots, planes
     for slot, p in enumerate(amp_planes):
         amp[int(p)] = aslots[slot]
     return arena, amp
+
+
+def export_terms(words, width, planes, amps, forms, scales, factors, offsets, red_planes):
+    """The schedule in reduction-term mode: (applied, ins, task_first, level_first, terms, cur_slots)."""
+    keep, a = _args(words, width, planes, amps, forms, scales, factors)
+    off = np.ascontiguousarray(offsets, dtype=np.uint32)
+    rp = np.ascontiguousarray(red_planes, dtype=np.uint32)
+    outputs = len(off) - 1
+    sizes = np.zeros(8, dtype=np.uint32)
+    assert lib().schedule_export_terms(*a, off.ctypes.data, rp.ctypes.data, outputs, sizes.ctypes.data,
+                                       None, None, None) == 0
+    ins = np.zeros(8 * int(sizes[0]) + 8, dtype=np.uint32)
+    tf = np.zeros(int(sizes[1]) + 1, dtype=np.uint32)
+    lf = np.zeros(int(sizes[2]) + 1, dtype=np.uint32)
+    assert lib().schedule_export_terms(*a, off.ctypes.data, rp.ctypes.data, outputs, sizes.ctypes.data,
+                                       ins.ctypes.data, tf.ctypes.data, lf.ctypes.data) == 0
+    return (bool(sizes[3]), ins[: 8 * int(sizes[0])].reshape(-1, 8), tf[: int(sizes[1])], lf[: int(sizes[2])],
+            int(sizes[4]), int(sizes[5]))
+
+
+def reference_terms(prog, planes, amps, red_planes):
+    """The reduction's terms when every amplitude starts at zero: term k from amplitude red_planes[k]."""
+    arena = [hash(("init", p)) for p in range(planes)]
+    amp = [ZERO] * amps
+    st = _Store(arena.__getitem__, arena.__setitem__, amp.__getitem__, amp.__setitem__)
+    acc = [0] * 6
+    for i in prog:
+        _row(st, i, acc)
+    return [hash(("term", amp[int(q)])) for q in red_planes]
+
+
+def scheduled_terms(ins, task_first, level_first, cur_slots, terms, planes, reverse=True):
+    """The terms as the term-mode schedule makes them (no live-in loads: batch plans have none)."""
+    slots = [None] * max(1, cur_slots)
+    out = [hash(("term", ZERO))] * terms
+
+    def get(sl):
+        v = slots[sl]
+        assert v is not None, f"slot {sl} read before any write"
+        return v
+
+    def put(sl, v):
+        slots[sl] = v
+
+    def term_put(t, v):
+        out[t] = hash(("term", v))
+
+    def no_amp(*_):
+        raise AssertionError("a term-mode schedule touched an amplitude slot")
+
+    st = _Store(get, put, no_amp, no_amp, term_put)
+    for lv in range(len(level_first) - 1):
+        tasks = list(range(int(level_first[lv]), int(level_first[lv + 1])))
+        if reverse:
+            tasks.reverse()
+        for t in tasks:
+            acc = [0] * 6
+            for n in range(int(task_first[t]), int(task_first[t + 1])):
+                _row(st, ins[n], acc)
+    return out

@@ -31,3 +31,29 @@ def test_physics_plans(name):
     t = processes.template(name)
     check(t.words, t.width, t.current_planes, t.amplitude_planes, t.momentum_planes // 4, len(t.scale_re),
           len(t.factor_re))
+
+
+@pytest.mark.parametrize("name", ["gg>ggg", "qg>qgg", "gg>qq~g"])
+def test_term_mode_gives_every_reduction_term_its_value(name):
+    """Batch plans keep reduction terms instead of amplitudes (use_terms): every term is made from
+    the same amplitude value as the reference's row order gives, for the physics plans (where it
+    applies) and for a plan where an amplitude has two closure rows (where it must not)."""
+    t = processes.template(name)
+    args = (t.words, t.width, t.current_planes, t.amplitude_planes, t.momentum_planes // 4, len(t.scale_re),
+            len(t.factor_re))
+    applied, ins, tf, lf, terms, slots = E.export_terms(*args, t.offsets, t.planes)
+    assert applied and terms == len(t.planes)
+    prog = E.export(*args)[0]
+    want = E.reference_terms(prog, t.current_planes, t.amplitude_planes, t.planes)
+    for reverse in (False, True):
+        assert E.scheduled_terms(ins, tf, lf, slots, terms, t.current_planes, reverse=reverse) == want
+
+
+def test_term_mode_refuses_shared_terms():
+    t = processes.template("qg>qgg")
+    args = (t.words, t.width, t.current_planes, t.amplitude_planes, t.momentum_planes // 4, len(t.scale_re),
+            len(t.factor_re))
+    planes = np.concatenate([t.planes, t.planes[:1]])  # an amplitude in two terms
+    offsets = np.concatenate([t.offsets, [t.offsets[-1] + 1]])
+    applied = E.export_terms(*args, offsets, planes)[0]
+    assert not applied
