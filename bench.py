@@ -126,16 +126,24 @@ def fp64_peak(torch, lib):
     return best / 1e12
 
 
-def reduce_over_ranks(dist, ms, sums):
-    """The job's step time is the slowest rank's; each family's |M|^2 total adds up over the ranks
-    (the points are sharded: the only exchange is this reduction of two small tensors)."""
+def reduce_over_ranks(dist, ms, sums, squares=None, peak=None):
+    """The job's step time is the slowest rank's; each family's |M|^2 total and sum of squares
+    add up over the ranks, its largest |M|^2 is the largest of any rank (the points are sharded:
+    the only exchange is this reduction of small tensors)."""
     import torch
 
     t = torch.tensor([ms], dtype=torch.float64, device=sums.device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     total = sums.clone()
     dist.all_reduce(total)
-    return float(t.item()), total
+    out = [float(t.item()), total]
+    if squares is not None:
+        sq = squares.clone()
+        dist.all_reduce(sq)
+        mx = peak.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        out += [sq, mx]
+    return tuple(out)
 
 
 def precision_line(torch, B, fams, ext, ref_out, steps, warmup, kind="mixed"):
@@ -426,10 +434,14 @@ def main():
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / args.steps
     clk = clocks.stop() if clocks else None
-    # the total |M|^2 of each family
-    sums = torch.stack([o.sum() for o in out])
+    # per family: the total |M|^2, its sum of squares and its largest value (per point, summed
+    # over the helicities)
+    m2 = [o.view(p.shape[0], t.outputs).sum(dim=1) for o, (_, t, p) in zip(out, fams)]
+    sums = torch.stack([x.sum() for x in m2])
+    squares = torch.stack([(x * x).sum() for x in m2])
+    peak_m2 = torch.stack([x.max() for x in m2])
     if world > 1:
-        ms, sums = reduce_over_ranks(dist, ms, sums)
+        ms, sums, squares, peak_m2 = reduce_over_ranks(dist, ms, sums, squares, peak_m2)
         dist.barrier()
     points = sum(p.shape[0] for _, _, p in fams) * world
     value = points / (ms * 1e-3)
@@ -453,7 +465,9 @@ def main():
                         "flops_per_point": {n: pl.flops for (n, _, _), pl in zip(fams, plans)}},
            "points_per_family": {n: p.shape[0] for n, _, p in fams},
            "lanes_per_point": {n: pl.lanes_per_point for (n, _, _), pl in zip(fams, plans)},
-           "sum_m2_per_family": [float(x) for x in sums.cpu()]}
+           "sum_m2_per_family": [float(x) for x in sums.cpu()],
+           "sum_m2_squared_per_family": [float(x) for x in squares.cpu()],
+           "max_m2_per_family": [float(x) for x in peak_m2.cpu()]}
     if clk:
         res["clocks"] = clk
     if rank == 0 and world == 1:

@@ -277,3 +277,52 @@ def from_processes(names, kernel=1, batch=0, reference_points=8, seed=7):
         p.colours.append(Colour("lc", t, mom.reshape(-1), np.zeros(reference_points * t.outputs), reference_points))
         f.processes.append(p)
     return f
+
+
+def summary(f: PacudaFile, arrays: bool = False) -> dict:
+    """A JSON-ready description of a file (for debugging, as the reference's pac2json): per
+    process its parameters and crossing, per colour its plan's sizes, its decoded rows' op counts
+    and its reduction; with `arrays`, the tables themselves."""
+    from . import plan as P
+
+    def table(a):
+        return [x.item() if hasattr(x, "item") else x for x in np.asarray(a).reshape(-1)]
+
+    out = {"kernel": f.kernel, "batch": f.batch, "symjit_sha256": list(f.symjit_sha256), "processes": []}
+    for p in f.processes:
+        pd = {"key": p.key, "legs": p.legs, "helicities": p.helicities, "alpha_s": [p.alpha_s_name, p.alpha_s],
+              "qcd_power": p.qcd_power, "parameters": [list(x) for x in p.parameters], "factor": list(p.factor),
+              "crossing": [list(x) for x in p.crossing] if p.crossing else None, "colours": []}
+        for c in p.colours:
+            t = c.template
+            ops = {}
+            for row in P.decode(t.words, t.width):
+                ops[int(row[0])] = ops.get(int(row[0]), 0) + 1
+            offsets = np.asarray(t.offsets)
+            cd = {"id": c.id, "tile": int(t.tile), "words": len(t.words), "width": [int(x) for x in t.width],
+                  "current_planes": int(t.current_planes), "amplitude_planes": int(t.amplitude_planes),
+                  "momentum_planes": int(t.momentum_planes), "scales": len(t.scale_re), "factors": len(t.factor_re),
+                  "external_count": int(t.external_count), "terms": len(t.term_slots),
+                  "ops": {str(k): v for k, v in sorted(ops.items())},
+                  "outputs": len(offsets) - 1,
+                  "live_outputs": int(np.count_nonzero(offsets[1:] > offsets[:-1])),
+                  "reduction_terms": int(offsets[-1]), "reference_points": int(c.reference_points)}
+            if arrays:
+                cd.update({"words_hex": [f"{int(w):016x}" for w in t.words], "scale_re": table(t.scale_re),
+                           "scale_im": table(t.scale_im), "factor_re": table(t.factor_re),
+                           "factor_im": table(t.factor_im), "zero": table(t.zero_amplitude),
+                           "download": table(t.download_amplitude), "form_terms": table(t.form_terms),
+                           "term_slots": table(t.term_slots), "term_coefficients": table(t.term_coefficients),
+                           "offsets": table(t.offsets), "planes": table(t.planes), "weights": table(t.weights)})
+            pd["colours"].append(cd)
+        out["processes"].append(pd)
+    return out
+
+
+if __name__ == "__main__":
+    import json
+    import sys
+
+    if len(sys.argv) < 2:
+        sys.exit("usage: python -m pacuda_b200.pacuda_file FILE.pacuda [--arrays]")
+    print(json.dumps(summary(read(sys.argv[1]), arrays="--arrays" in sys.argv[2:]), indent=1))

@@ -25,12 +25,14 @@ def _rank(rank, world, port, path):
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
     try:
         sums = torch.tensor([1.0 + rank, 10.0 * rank], dtype=torch.float64)
-        ms, total = bench.reduce_over_ranks(dist, 3.0 + 2.0 * rank, sums)
+        squares = torch.tensor([2.0, 3.0 + rank], dtype=torch.float64)
+        peak = torch.tensor([5.0 - rank, 1.0 + rank], dtype=torch.float64)
+        ms, total, sq, mx = bench.reduce_over_ranks(dist, 3.0 + 2.0 * rank, sums, squares, peak)
         bench.POINTS = 4096
         fams = bench.workload(rank)
         first = np.concatenate([p[:4].reshape(-1) for _, _, p in fams])
-        np.savez(f"{path}_{rank}.npz", ms=ms, total=total.numpy(), counts=[p.shape[0] for _, _, p in fams],
-                 first=first)
+        np.savez(f"{path}_{rank}.npz", ms=ms, total=total.numpy(), sq=sq.numpy(), mx=mx.numpy(),
+                 counts=[p.shape[0] for _, _, p in fams], first=first)
     finally:
         dist.destroy_process_group()
 
@@ -43,6 +45,7 @@ def test_two_gloo_ranks_shard_points_and_reduce_once(tmp_path):
     for x in r:
         assert float(x["ms"]) == 5.0                       # the slowest rank's time
         assert np.array_equal(x["total"], [3.0, 10.0])     # summed over the ranks
+        assert np.array_equal(x["sq"], [4.0, 7.0]) and np.array_equal(x["mx"], [5.0, 2.0])
     assert np.array_equal(r[0]["counts"], r[1]["counts"])  # the same family split per rank
     assert sum(r[0]["counts"]) == 4096
     assert not np.array_equal(r[0]["first"], r[1]["first"])  # each rank its own points

@@ -1,4 +1,5 @@
 """The .pacuda v2 file (convert/src/format.rs:1-29): write, read back, and the byte layout."""
+import os
 import struct
 
 import numpy as np
@@ -45,3 +46,23 @@ def test_rejects_truncated_and_trailing_bytes():
         except ValueError:
             continue
         raise AssertionError("accepted a malformed file")
+
+
+def test_summary_dump(tmp_path):
+    """The debugging dump (python -m pacuda_b200.pacuda_file FILE): sizes, op counts, reduction."""
+    import json
+    import subprocess
+    import sys
+
+    from pacuda_b200 import pacuda_file as PF
+
+    f = PF.from_processes(["gg>ggg"], reference_points=0)
+    path = str(tmp_path / "a.pacuda")
+    PF.write(f, path)
+    out = subprocess.run([sys.executable, "-m", "pacuda_b200.pacuda_file", path, "--arrays"], capture_output=True,
+                         text=True, check=True, cwd=os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    d = json.loads(out.stdout)
+    c = d["processes"][0]["colours"][0]
+    t = f.processes[0].colours[0].template
+    assert c["words"] == len(t.words) and len(c["words_hex"]) == len(t.words)
+    assert sum(c["ops"].values()) == len(t.words) and c["outputs"] == 32 and c["live_outputs"] > 0
