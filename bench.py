@@ -178,7 +178,8 @@ def precision_line(torch, B, fams, ext, ref_out, steps, warmup, kind="mixed"):
     return {"kind": kind, "value": n / (ms * 1e-3), "unit": "points/s", "ms_per_step": ms,
             "rel_error_vs_f64": {"median": float(np.median(rel)), "q999": float(np.quantile(rel, 0.999)),
                                  "max": float(rel.max()), "frac_le_1e-10": float((rel <= 1e-10).mean())},
-            "lanes_per_point": {nm: pl.lanes_per_point for (nm, _, _), pl in zip(fams, plans)}}
+            "lanes_per_point": {nm: batch.lanes_per_point(k) for k, (nm, _, _) in enumerate(fams)},
+            "blocks_per_sm": batch.blocks_per_sm}
 
 
 def dram_bytes_per_point():
@@ -355,6 +356,7 @@ def main():
     ap.add_argument("--no-tune", action="store_true", help="keep the default points per warp")
     ap.add_argument("--lanes-per-point", type=int, default=0)
     ap.add_argument("--no-precision", action="store_true", help="skip the mixed-precision line")
+    ap.add_argument("--blocks-per-sm", type=int, default=0, help="1, 2 or 4 (with --no-tune or --lanes-per-point)")
     args = ap.parse_args()
     POINTS = args.points
     if args.family:
@@ -415,6 +417,8 @@ def main():
     batch = B.Batch(plans, ext, out)
     if not args.no_tune and not args.lanes_per_point:
         batch.tune()
+    if args.blocks_per_sm:
+        batch.blocks_per_sm = args.blocks_per_sm
     stream = torch.cuda.Stream()
     with torch.cuda.stream(stream):
         batch.capture(stream)
@@ -464,7 +468,8 @@ def main():
                                 "peak_gbs": hbm_peak(), "peak_source": "MEASURED_PEAKS.json hbm_gbs"},
                         "flops_per_point": {n: pl.flops for (n, _, _), pl in zip(fams, plans)}},
            "points_per_family": {n: p.shape[0] for n, _, p in fams},
-           "lanes_per_point": {n: pl.lanes_per_point for (n, _, _), pl in zip(fams, plans)},
+           "lanes_per_point": {n: batch.lanes_per_point(k) for k, (n, _, _) in enumerate(fams)},
+           "blocks_per_sm": batch.blocks_per_sm,
            "sum_m2_per_family": [float(x) for x in sums.cpu()],
            "sum_m2_squared_per_family": [float(x) for x in squares.cpu()],
            "max_m2_per_family": [float(x) for x in peak_m2.cpu()]}

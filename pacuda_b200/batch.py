@@ -31,6 +31,11 @@ def lib(path=None):
             getattr(L, name).argtypes = [C.c_void_p, C.c_void_p]
         L.pacuda_b200_batch_launches.argtypes = [C.c_void_p]
         L.pacuda_b200_batch_launches.restype = C.c_uint32
+        L.pacuda_b200_batch_set_blocks_per_sm.argtypes = [C.c_void_p, C.c_uint32]
+        L.pacuda_b200_batch_blocks_per_sm.argtypes = [C.c_void_p]
+        L.pacuda_b200_batch_blocks_per_sm.restype = C.c_uint32
+        L.pacuda_b200_batch_lanes_per_point.argtypes = [C.c_void_p, C.c_uint32]
+        L.pacuda_b200_batch_lanes_per_point.restype = C.c_uint32
         L.pacuda_b200_batch_destroy.argtypes = [C.c_void_p]
     return _lib
 
@@ -111,6 +116,19 @@ class Batch:
     @property
     def launches(self):
         return lib().pacuda_b200_batch_launches(self.handle)
+
+    def lanes_per_point(self, k):
+        """The lanes per point plan k runs with in this batch's launch."""
+        return lib().pacuda_b200_batch_lanes_per_point(self.handle, k)
+
+    @property
+    def blocks_per_sm(self):
+        return lib().pacuda_b200_batch_blocks_per_sm(self.handle)
+
+    @blocks_per_sm.setter
+    def blocks_per_sm(self, n):
+        if lib().pacuda_b200_batch_set_blocks_per_sm(self.handle, n) != 0:
+            raise RunnerError(f"{n} blocks per SM do not fit")
 
     def __del__(self):
         if getattr(self, "handle", None) and _lib is not None:

@@ -60,10 +60,12 @@ struct pacuda_b200_batch {
     std::vector<const double *> external;
     std::vector<uint32_t> count;
     std::vector<double *> output;
+    std::vector<uint32_t> points;  // per plan: its points per block in this batch's launch
     // descriptor block: TiledPlan[n] | item_first[n + 1] | external[n] | output[n] | count[n] | counter
     unsigned char *host = nullptr, *device = nullptr;
     size_t bytes = 0;
     int threads = 0, sms = 0;
+    int blocks = 1;  // per SM (tiled_host.h kMaxBlocks)
     size_t smem = 0, const_bytes = 0;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -72,9 +74,9 @@ struct pacuda_b200_batch {
 
 namespace {
 
-void fill_plan(const pacuda_b200_plan *p, TiledPlan &d) {
+void fill_plan(const pacuda_b200_plan *p, TiledPlan &d, uint32_t points, int blocks = 1) {
     memset(&d, 0, sizeof d);
-    describe(p->tiled, p->forms, p->points, p->point_bytes, d);
+    describe(p->tiled, p->forms, points, p->point_bytes, d, blocks);
     d.s64 = p->consts;
     d.f64 = p->consts + 2 * p->scales;
     d.kconst = p->consts + 2 * (p->scales + p->factors);
@@ -115,26 +117,35 @@ bool prepare(pacuda_b200_batch *b) {
             return false;
     }
     memset(b->host, 0, b->bytes);
+    b->points.assign(n, 0);
     TiledPlan *plans = (TiledPlan *)(b->host + o.plans);
     unsigned long long *items = (unsigned long long *)(b->host + o.items);
-    b->threads = tiled_threads(b->plans[0]->kernel);
+    const int kernel = b->plans[0]->kernel;
+    b->threads = tiled_threads(kernel, b->blocks);
     b->const_bytes = 0;
     for (size_t k = 0; k < n; k++)
         b->const_bytes = std::max(b->const_bytes, tiled_const_bytes(b->plans[k]->scales, b->plans[k]->factors));
-    size_t max_smem = tiled_max_smem(b->plans[0]->kernel) - b->const_bytes;
+    size_t room = tiled_max_smem(kernel, b->blocks);
+    if (room <= b->const_bytes) {
+        fprintf(stderr, "%s: the plans' constants do not fit a block's shared memory\n", kTag);
+        return false;
+    }
+    size_t max_smem = room - b->const_bytes;
     b->smem = 0;
     items[0] = 0;
     for (size_t k = 0; k < n; k++) {
         pacuda_b200_plan *p = b->plans[k];
         uint32_t most = tiled_max_points(p->point_bytes, b->threads, max_smem);
-        if (!most || p->tiled.threads != b->threads) {
+        if (!most || p->tiled.threads != tiled_threads(kernel)) {
             fprintf(stderr, "%s: a plan's point does not fit a block's shared memory\n", kTag);
             return false;
         }
-        if (!tiled_points_fit(p->points, p->point_bytes, b->threads, max_smem))
-            p->points = tiled_default_points(p->point_bytes, b->threads, max_smem);
-        fill_plan(p, plans[k]);
-        uint32_t per = p->points;
+        // the plan's choice where it fits this launch, else the default for it
+        uint32_t per = tiled_points_fit(p->points, p->point_bytes, b->threads, max_smem)
+                           ? p->points
+                           : tiled_default_points(p->point_bytes, b->threads, max_smem);
+        b->points[k] = per;
+        fill_plan(p, plans[k], per, b->blocks);
         b->smem = std::max<size_t>(b->smem, (size_t)per * p->point_bytes);
         items[k + 1] = items[k] + (b->count[k] + per - 1) / per;
     }
@@ -170,7 +181,7 @@ int launch(pacuda_b200_batch *b, cudaStream_t s) {
     cudaStreamIsCapturing(s, &capturing);
     if (capturing == cudaStreamCaptureStatusNone && b->copied && failed(cudaEventRecord(b->copied, s), "event"))
         return PACMAN_RECURRENCE_DEVICE_ERROR;
-    if (!launch_tiled(b->plans[0]->kernel, launch_args(b), b->threads, b->smem, b->sms, s) ||
+    if (!launch_tiled(b->plans[0]->kernel, launch_args(b), b->threads, b->smem, b->sms * b->blocks, s) ||
         failed(cudaGetLastError(), "launch"))
         return PACMAN_RECURRENCE_DEVICE_ERROR;
     return PACMAN_RECURRENCE_OK;
@@ -403,26 +414,19 @@ extern "C" int pacuda_b200_batch_tune(pacuda_b200_batch *b, void *stream) {
     cudaEvent_t t0, t1;
     cudaEventCreate(&t0);
     cudaEventCreate(&t1);
-    for (size_t k = 0; k < b->plans.size(); k++) {
-        pacuda_b200_plan *p = b->plans[k];
-        if (p->fixed) continue;
-        uint32_t sample = std::min<uint32_t>(b->count[k], 1u << 16);
-        pacuda_b200_plan *one[1] = {p};
+    // one plan alone at `points` per block and `blocks` per SM: the best of three launches, in ms
+    // (or a negative time when it does not fit)
+    auto time_plan = [&](size_t k, uint32_t points, int blocks) -> float {
+        pacuda_b200_plan *p = b->plans[k], *one[1] = {p};
         const double *ext[1] = {b->external[k]};
         double *out[1] = {b->output[k]};
-        float best = 1e30f;
-        uint32_t best_points = p->points;
-        int threads = tiled_threads(p->kernel);
-        // from the most points per block that fit down to half of them (fewer points leave more
-        // of the block's lanes idle at the levels' barriers)
-        uint32_t most = tiled_max_points(p->point_bytes, threads, point_smem(p));
-        for (uint32_t points = most; points >= 1 && 2 * points >= most; points--) {
-            p->points = points;
-            uint32_t n = b->count[k];
-            pacuda_b200_batch *tb = pacuda_b200_batch_create(one, 1, ext, &n, out);
-            if (!tb) continue;
-            float ms = 0;
-            bool ok = launch(tb, s) == PACMAN_RECURRENCE_OK;
+        uint32_t n = b->count[k], keep = p->points;
+        p->points = points;
+        pacuda_b200_batch *tb = pacuda_b200_batch_create(one, 1, ext, &n, out);
+        float ms = -1.0f;
+        if (tb) {
+            tb->blocks = blocks;
+            bool ok = prepare(tb) && tb->points[0] == points && launch(tb, s) == PACMAN_RECURRENCE_OK;
             for (int rep = 0; ok && rep < 3; rep++) {
                 cudaEventRecord(t0, s);
                 ok = launch(tb, s) == PACMAN_RECURRENCE_OK;
@@ -432,21 +436,86 @@ extern "C" int pacuda_b200_batch_tune(pacuda_b200_batch *b, void *stream) {
                 cudaEventElapsedTime(&m, t0, t1);
                 ms = rep == 0 ? m : std::min(ms, m);
             }
+            if (!ok) ms = -1.0f;
             pacuda_b200_batch_destroy(tb);
-            if (ok && ms < best) {
-                best = ms;
-                best_points = points;
-            }
         }
-        p->points = best_points;
-        (void)sample;
+        p->points = keep;
+        return ms;
+    };
+    // per blocks-per-SM choice: each plan's fastest points per block (from the most that fit down
+    // to half of them: fewer leave more of a block's lanes idle at the levels' barriers); the
+    // choice whose plans' times add up least is kept
+    std::vector<uint32_t> choice[kMaxBlocks + 1];
+    float total[kMaxBlocks];
+    const int kernel = b->plans[0]->kernel;
+    for (int blocks = 1; blocks <= kMaxBlocks; blocks++) {
+        total[blocks - 1] = -1.0f;
+        if (blocks == 3) continue;  // (16 warps do not split in three)
+        int threads = tiled_threads(kernel, blocks);
+        size_t room = tiled_max_smem(kernel, blocks);
+        total[blocks - 1] = 0.0f;
+        for (size_t k = 0; k < b->plans.size() && total[blocks - 1] >= 0.0f; k++) {
+            pacuda_b200_plan *p = b->plans[k];
+            size_t cb = tiled_const_bytes(p->scales, p->factors);
+            uint32_t most = room > cb ? tiled_max_points(p->point_bytes, threads, room - cb) : 0;
+            float best = -1.0f;
+            uint32_t best_points = 0;
+            for (uint32_t points = most; points >= 1 && 2 * points >= most; points--) {
+                if (p->fixed && points != p->points) continue;
+                float ms = time_plan(k, points, blocks);
+                if (ms >= 0.0f && (best < 0.0f || ms < best)) {
+                    best = ms;
+                    best_points = points;
+                }
+            }
+            choice[blocks - 1].push_back(best_points);
+            total[blocks - 1] = best < 0.0f ? -1.0f : total[blocks - 1] + best;
+        }
+    }
+    int pick = 1;
+    for (int blocks = 2; blocks <= kMaxBlocks; blocks++)
+        if (total[blocks - 1] >= 0.0f && (total[pick - 1] < 0.0f || total[blocks - 1] < total[pick - 1])) pick = blocks;
+    if (total[pick - 1] >= 0.0f) {
+        for (size_t k = 0; k < b->plans.size(); k++) b->plans[k]->points = choice[pick - 1][k];
+        b->blocks = pick;
     }
     cudaEventDestroy(t0);
     cudaEventDestroy(t1);
+    if (b->exec) {
+        cudaGraphExecDestroy(b->exec);
+        cudaGraphDestroy(b->graph);
+        b->exec = nullptr;
+        b->graph = nullptr;
+    }
     return prepare(b) ? PACMAN_RECURRENCE_OK : PACMAN_RECURRENCE_DEVICE_ERROR;
 }
 
 extern "C" uint32_t pacuda_b200_batch_launches(const pacuda_b200_batch *b) { return b ? 1 : 0; }
+
+extern "C" int pacuda_b200_batch_set_blocks_per_sm(pacuda_b200_batch *b, uint32_t blocks) {
+    if (!b || blocks > (uint32_t)kMaxBlocks || blocks == 3) return PACMAN_RECURRENCE_INVALID;
+    if (failed(cudaEventSynchronize(b->copied), "batch")) return PACMAN_RECURRENCE_DEVICE_ERROR;
+    if (b->exec) {
+        cudaGraphExecDestroy(b->exec);
+        cudaGraphDestroy(b->graph);
+        b->exec = nullptr;
+        b->graph = nullptr;
+    }
+    int before = b->blocks;
+    b->blocks = blocks ? (int)blocks : 1;
+    if (!prepare(b)) {
+        b->blocks = before;
+        prepare(b);
+        return PACMAN_RECURRENCE_INVALID;
+    }
+    return PACMAN_RECURRENCE_OK;
+}
+
+extern "C" uint32_t pacuda_b200_batch_blocks_per_sm(const pacuda_b200_batch *b) { return b ? (uint32_t)b->blocks : 0; }
+
+extern "C" uint32_t pacuda_b200_batch_lanes_per_point(const pacuda_b200_batch *b, uint32_t plan) {
+    return b && plan < b->points.size() && b->points[plan] ? tiled_lanes(b->points[plan], b->threads) : 0;
+}
 
 extern "C" void pacuda_b200_batch_destroy(pacuda_b200_batch *b) {
     if (!b) return;
@@ -566,8 +635,7 @@ extern "C" int pacuda_b200_run_static(pacuda_b200_plan *const *plans, uint32_t n
         uint32_t per = tiled_points_fit(p->points, p->point_bytes, threads, max_smem)
                            ? p->points
                            : tiled_default_points(p->point_bytes, threads, max_smem);
-        fill_plan(p, block.plans[k]);
-        describe(p->tiled, p->forms, per, p->point_bytes, block.plans[k]);
+        fill_plan(p, block.plans[k], per);
         smem = std::max<size_t>(smem, (size_t)per * p->point_bytes);
         block.items[k + 1] = block.items[k] + (count[k] + per - 1) / per;
         block.external[k] = external[k];

@@ -68,18 +68,19 @@ bool upload_schedule(TiledDevice &t, int threads, cudaStream_t s) {
     t.levels = (uint32_t)t.host.level_first.size() - 1;
     t.threads = threads;
     std::vector<uint32_t> ranges, firsts;
-    for (uint32_t np = 1; t.ok && np <= kMaxPoints; np++) {
-        std::vector<uint32_t> order, lf;
-        lane_order(t.host, tiled_lanes(np, threads), order, lf);
-        // each position holds its task's instruction range (first, end); (0, 0) for none
-        t.order_at[np - 1] = ranges.size();
-        t.level_at[np - 1] = firsts.size();
-        for (uint32_t task : order) {
-            ranges.push_back(task == ~0u ? 0 : t.host.task_first[task]);
-            ranges.push_back(task == ~0u ? 0 : t.host.task_first[task + 1]);
+    for (int b = 1; t.ok && b <= kMaxBlocks; b++)
+        for (uint32_t np = 1; np <= kMaxPoints; np++) {
+            std::vector<uint32_t> order, lf;
+            lane_order(t.host, tiled_lanes(np, std::max(32, threads / b)), order, lf);
+            // each position holds its task's instruction range (first, end); (0, 0) for none
+            t.order_at[b - 1][np - 1] = ranges.size();
+            t.level_at[b - 1][np - 1] = firsts.size();
+            for (uint32_t task : order) {
+                ranges.push_back(task == ~0u ? 0 : t.host.task_first[task]);
+                ranges.push_back(task == ~0u ? 0 : t.host.task_first[task + 1]);
+            }
+            firsts.insert(firsts.end(), lf.begin(), lf.end());
         }
-        firsts.insert(firsts.end(), lf.begin(), lf.end());
-    }
     t.ok = t.ok && put(&t.orders, ranges, s) && put(&t.level_firsts, firsts, s);
     // the host vectors must outlive the asynchronous copies
     cudaStreamSynchronize(s);
@@ -94,7 +95,7 @@ size_t tiled_point_bytes(const Schedule &s, uint32_t forms, int kernel) {
     return (per_point + 15) / 16 * 16;
 }
 
-int tiled_threads(int kernel) {
+int tiled_threads(int kernel, int blocks) {
     cudaFuncAttributes attr, abi;
     if (cudaFuncGetAttributes(&attr, kernel_for(kernel, false)) != cudaSuccess ||
         cudaFuncGetAttributes(&abi, kernel_for(kernel, true)) != cudaSuccess)
@@ -107,19 +108,24 @@ int tiled_threads(int kernel) {
     int per_warp = ((attr.numRegs * 32 + 255) / 256) * 256;
     int warps = per_warp ? regs / per_warp : 16;
     warps = std::min(warps, attr.maxThreadsPerBlock / 32);
-    return 32 * std::max(1, std::min(warps, 16));
+    warps = std::max(1, std::min(warps, 16));
+    return 32 * std::max(1, warps / std::max(1, blocks));
 }
 
-size_t tiled_max_smem(int kernel) {
+size_t tiled_max_smem(int kernel, int blocks) {
     cudaFuncAttributes attr, abi;
     if (cudaFuncGetAttributes(&attr, kernel_for(kernel, false)) != cudaSuccess ||
         cudaFuncGetAttributes(&abi, kernel_for(kernel, true)) != cudaSuccess)
         return 0;
     attr.sharedSizeBytes = std::max(attr.sharedSizeBytes, abi.sharedSizeBytes);
-    int dev = 0, smem = 0;
+    int dev = 0, smem = 0, per_sm = 0, reserved = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    return (size_t)smem - attr.sharedSizeBytes;
+    cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
+    // with several blocks per SM each gets its share of the SM's shared memory
+    size_t limit = blocks > 1 ? std::min<size_t>(smem, (size_t)(per_sm - blocks * reserved) / blocks) : (size_t)smem;
+    return limit > attr.sharedSizeBytes ? limit - attr.sharedSizeBytes : 0;
 }
 
 bool tiled_points_fit(uint32_t points, size_t point_bytes, int threads, size_t max_smem) {
@@ -140,29 +146,29 @@ uint32_t tiled_default_points(size_t point_bytes, int threads, size_t max_smem) 
     return best;
 }
 
-void describe(const TiledDevice &t, uint32_t forms, uint32_t points, size_t point_bytes, TiledPlan &p) {
+void describe(const TiledDevice &t, uint32_t forms, uint32_t points, size_t point_bytes, TiledPlan &p, int blocks) {
     p.ins = t.ins;
     p.task_first = t.task_first;
-    p.order = t.orders + t.order_at[points - 1];
-    p.level_first = t.level_firsts + t.level_at[points - 1];
+    p.order = t.orders + t.order_at[blocks - 1][points - 1];
+    p.level_first = t.level_firsts + t.level_at[blocks - 1][points - 1];
     p.levels = t.levels;
     p.cur_slots = t.host.cur_slots;
     p.amp_slots = t.host.amp_slots;
     p.terms = t.host.terms;
     p.forms = forms;
     p.points = points;
-    p.lanes = tiled_lanes(points, t.threads);
+    p.lanes = tiled_lanes(points, std::max(32, t.threads / blocks));
     p.point_bytes = (uint32_t)point_bytes;
     p.loads = t.loads;
     p.nloads = (uint32_t)t.host.loads.size() / 3;
     p.amp_planes = t.amp_planes;
 }
 
-bool launch_tiled(int kernel, const TiledLaunch &args, int threads, size_t smem, int sms, cudaStream_t stream) {
+bool launch_tiled(int kernel, const TiledLaunch &args, int threads, size_t smem, int grid, cudaStream_t stream) {
     const void *fn = kernel_for(kernel, args.abi);
     if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return false;
     void *params[] = {(void *)&args};
-    return cudaLaunchKernel(fn, dim3(sms), dim3(threads), params, smem, stream) == cudaSuccess;
+    return cudaLaunchKernel(fn, dim3(grid), dim3(threads), params, smem, stream) == cudaSuccess;
 }
 
 }  // namespace pacuda

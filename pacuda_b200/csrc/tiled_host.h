@@ -14,6 +14,9 @@ struct TiledLaunch;
 // points per block: 1 .. kMaxPoints; a point then has warps * floor(32 / P) lanes (a lane of all
 // P points is P adjacent threads of one warp)
 constexpr uint32_t kMaxPoints = 32;
+// blocks per SM: 1 (one block of all the warps the registers allow), 2 or 4 (independent blocks
+// that share them and reach their barriers at different times)
+constexpr int kMaxBlocks = 4;
 inline uint32_t tiled_lanes(uint32_t points, int threads) { return (uint32_t)(threads / 32) * (32 / points); }
 
 struct TiledDevice {
@@ -23,8 +26,8 @@ struct TiledDevice {
     // per points-per-block count P: the lane order for threads / P lanes and its level
     // boundaries, concatenated (offsets in 32-bit words, index P - 1)
     uint32_t *orders = nullptr, *level_firsts = nullptr;
-    size_t order_at[kMaxPoints] = {0}, level_at[kMaxPoints] = {0};
-    int threads = 0;  // the block the orders were made for
+    size_t order_at[kMaxBlocks][kMaxPoints] = {{0}}, level_at[kMaxBlocks][kMaxPoints] = {{0}};
+    int threads = 0;  // the threads of one block per SM (blocks of b per SM have threads / b)
     uint32_t levels = 0;
     bool ok = false;
     void release();
@@ -44,9 +47,10 @@ bool upload_schedule(TiledDevice &t, int threads, cudaStream_t stream);
 // bytes of shared memory one point needs (kernel: PACMAN_RECURRENCE_KERNEL_*), 16-aligned
 size_t tiled_point_bytes(const Schedule &s, uint32_t forms, int kernel);
 
-// the block's threads (as the kernel's registers allow, at most 512) and its largest shared memory
-int tiled_threads(int kernel);
-size_t tiled_max_smem(int kernel);
+// a block's threads with `blocks` blocks per SM (as the kernel's registers allow, at most 512 per
+// SM) and its largest dynamic shared memory
+int tiled_threads(int kernel, int blocks = 1);
+size_t tiled_max_smem(int kernel, int blocks = 1);
 
 // whether a block of `threads` runs `points` points within `max_smem` bytes
 bool tiled_points_fit(uint32_t points, size_t point_bytes, int threads, size_t max_smem);
@@ -56,10 +60,11 @@ uint32_t tiled_max_points(size_t point_bytes, int threads, size_t max_smem);
 // warp without a lane (P * floor(32 / P) largest), the larger on ties; 0 when none fits
 uint32_t tiled_default_points(size_t point_bytes, int threads, size_t max_smem);
 
-// fills the schedule fields of a plan descriptor for `points` points per block
-void describe(const TiledDevice &t, uint32_t forms, uint32_t points, size_t point_bytes, TiledPlan &p);
+// fills the schedule fields of a plan descriptor for `points` points per block, `blocks` per SM
+void describe(const TiledDevice &t, uint32_t forms, uint32_t points, size_t point_bytes, TiledPlan &p, int blocks = 1);
 
-// launches the persistent kernel (one block per SM) with `smem` bytes of shared memory
-bool launch_tiled(int kernel, const TiledLaunch &args, int threads, size_t smem, int sms, cudaStream_t stream);
+// launches the persistent kernel (`grid` blocks: the SMs times the blocks per SM) with `smem` bytes
+// of shared memory
+bool launch_tiled(int kernel, const TiledLaunch &args, int threads, size_t smem, int grid, cudaStream_t stream);
 
 }  // namespace pacuda

@@ -87,3 +87,20 @@ def test_tuned_and_captured_runs_give_the_same_bits():
     torch.cuda.synchronize()
     check(out, want)
     assert b.launches == 1
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", ["f64", "mixed"])
+@pytest.mark.parametrize("blocks", [2, 4])
+def test_several_blocks_per_sm_give_the_same_bits(kind, blocks):
+    """Independent blocks per SM (each with its share of the SM's shared memory and warps)."""
+    from pacuda_b200 import batch as B
+    import torch
+
+    plans, ext, out, want = setup(kind, [70, 33, 129, 5])
+    b = B.Batch(plans, ext, out)
+    b.blocks_per_sm = blocks
+    assert b.blocks_per_sm == blocks
+    b.run()
+    torch.cuda.synchronize()
+    check(out, want)
