@@ -140,16 +140,21 @@ __device__ __forceinline__ uint32_t group_of(const Group *groups, uint32_t ngrou
     return lo;
 }
 
-// the external momenta of every group; `bad` is set when a momentum is not finite
+// `bad` is set when any of the n values is not finite
+__global__ void check_finite(const double *values, size_t n, int *bad) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        if (!isfinite(values[i])) *bad = 1;
+}
+
+// the external momenta of every group
 __global__ void gather_groups(const Group *groups, const double *momenta, size_t events, const ItemIn *items,
-                              double *external, int *bad) {
+                              double *external) {
     const Group &g = groups[blockIdx.y];
     const size_t n = (size_t)g.points * g.legs * 4;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         size_t q = i % g.points, lk = i / g.points;
         uint32_t l = (uint32_t)(lk >> 2), k = (uint32_t)(lk & 3);
         double v = momenta[((size_t)g.legs * k + g.leg[l]) * events + items[g.first + q].event];
-        if (!isfinite(v)) *bad = 1;
         external[g.external + i] = g.sign[l] * v;
     }
 }
@@ -382,6 +387,9 @@ UmamiStatus launch_chunk(Instance *in, int slot, const Chunk &ch, const double *
                                       stride * sizeof(double), events * sizeof(double), 4 * n,
                                       cudaMemcpyHostToDevice, in->copies),
                     "momenta") ||
+        (check_finite<<<(unsigned)std::min<size_t>((4 * n * events + 255) / 256, 1024), 256, 0, in->copies>>>(
+             dev_mom, 4 * n * events, in->bad.p),
+         cuda_failed(cudaGetLastError(), "check")) ||
         cuda_failed(cudaMemcpyAsync(items, in->host_items.p + ch.item0, ch.items * sizeof(ItemIn),
                                     cudaMemcpyHostToDevice, in->copies),
                     "items") ||
@@ -394,7 +402,7 @@ UmamiStatus launch_chunk(Instance *in, int slot, const Chunk &ch, const double *
     cudaStream_t s = in->stream;
     uint32_t most = *std::max_element(points.begin(), points.end());
     dim3 grid((unsigned)std::min<size_t>((4 * n * most + 255) / 256, 2048), (unsigned)groups);
-    gather_groups<<<grid, 256, 0, s>>>(dev_groups, dev_mom, events, items, in->external.p, in->bad.p);
+    gather_groups<<<grid, 256, 0, s>>>(dev_groups, dev_mom, events, items, in->external.p);
     if (cuda_failed(cudaGetLastError(), "gather")) return UMAMI_ERROR;
     pacuda_b200_batch *&batch = in->batch[slot];
     if (batch && in->batch_plans[slot] == plans) {
@@ -726,8 +734,11 @@ UMAMI_EXPORT UmamiStatus umami_matrix_element(UmamiHandle handle, size_t count, 
     size_t items_so_far = 0, ext = 0, vals = 0;
     for (size_t c = 0; c < nchunks; c++) {
         Chunk &ch = chunks[c];
-        ch.e0 = count * c / nchunks;
-        ch.e1 = count * (c + 1) / nchunks;
+        // four chunks of 1/8, 3/8, 3/8 and 1/8 of the events: the device starts after a short
+        // first chunk, and the host's last combining after a short last one
+        static const size_t eighths[kChunks + 1] = {0, 1, 4, 7, 8};
+        ch.e0 = nchunks == kChunks ? count * eighths[c] / 8 : count * c / nchunks;
+        ch.e1 = nchunks == kChunks ? count * eighths[c + 1] / 8 : count * (c + 1) / nchunks;
         ch.item0 = items_so_far;
         ch.first.assign(nclasses + 1, 0);
         // its events' selections and its item count per class
@@ -794,16 +805,20 @@ UMAMI_EXPORT UmamiStatus umami_matrix_element(UmamiHandle handle, size_t count, 
             cuda_failed(cudaEventRecord(in->done[c], in->stream), "event"))
             return drain(), UMAMI_ERROR;
     }
-    if (cuda_failed(cudaMemcpyAsync(in->host_bad.p, in->bad.p, sizeof(int), cudaMemcpyDeviceToHost, in->stream),
-                    "flag"))
+    // every momentum's check is on the copy stream, well ahead of the evaluation: the call's
+    // verdict on them comes before any output is written (as the reference checks them all first)
+    if (cuda_failed(cudaMemcpyAsync(in->host_bad.p, in->bad.p, sizeof(int), cudaMemcpyDeviceToHost, in->copies),
+                    "flag") ||
+        cuda_failed(cudaStreamSynchronize(in->copies), "copies"))
         return drain(), UMAMI_ERROR;
+    if (in->host_bad.p[0]) return drain(), UMAMI_ERROR;  // a momentum that is not finite
 
-    // the events combined as the reference does, chunk by chunk as the results come back; the
-    // first event whose |M|^2 is not finite ends the call (the events before it are written)
-    std::vector<double> total_of(count);
-    std::vector<int> label_of(count);
-    size_t good = count;
-    for (size_t c = 0; c < nchunks && good == count; c++) {
+    // the events combined as the reference does, chunk by chunk as the results come back, into
+    // the outputs; the first event whose |M|^2 is not finite ends the call (the events before it
+    // are written)
+    double *me_out = (double *)out_[UMAMI_OUT_MATRIX_ELEMENT];
+    int *hel_out = (int *)out_[UMAMI_OUT_HELICITY_INDEX], *col_out = (int *)out_[UMAMI_OUT_COLOR_INDEX];
+    for (size_t c = 0; c < nchunks; c++) {
         if (cuda_failed(cudaEventSynchronize(in->done[c]), "evaluation")) return drain(), UMAMI_ERROR;
         const Chunk &ch = chunks[c];
         const double *value = in->host_value.p;
@@ -829,24 +844,12 @@ UMAMI_EXPORT UmamiStatus umami_matrix_element(UmamiHandle handle, size_t count, 
                     total += sel.contributions[j].factor * value[at[k + j]];
             }
             k += sel.contribution_count;
-            if (!isfinite(total)) {
-                good = e;
-                break;
-            }
-            total_of[e] = total;
-            label_of[e] = label;
+            if (!isfinite(total)) return drain(), UMAMI_ERROR;
+            if (me_out) me_out[event] = total;
+            if (hel_out) hel_out[event] = label;
+            if (col_out) col_out[event] = (int)head->color_index;
         }
     }
     if (!drain()) return UMAMI_ERROR;
-    if (in->host_bad.p[0]) return UMAMI_ERROR;  // a momentum that is not finite
-    for (size_t e = 0; e < good; ++e) {
-        size_t event = offset + e;
-        const UmamiFlavour &sel = umami_provider.channels[selection[e] >> 16].flavours[selection[e] & 0xffff];
-        if (out_[UMAMI_OUT_MATRIX_ELEMENT]) ((double *)out_[UMAMI_OUT_MATRIX_ELEMENT])[event] = total_of[e];
-        if (out_[UMAMI_OUT_HELICITY_INDEX]) ((int *)out_[UMAMI_OUT_HELICITY_INDEX])[event] = label_of[e];
-        if (out_[UMAMI_OUT_COLOR_INDEX])
-            ((int *)out_[UMAMI_OUT_COLOR_INDEX])[event] = (int)sel.contributions[0].color_index;
-    }
-    if (good != count) return UMAMI_ERROR;
     return UMAMI_SUCCESS;
 }
