@@ -136,12 +136,14 @@ def outgoing_kind(leg):
     return leg.kind
 
 
-def build(legs, alpha_s=ALPHA_S, gauge_leg=None):
+def build(legs, alpha_s=ALPHA_S, gauge_leg=None, part=(0, 1)):
     """The plan (a `plan.Template`) of a process with these legs: all gluons, or one quark line
     (one outgoing-picture quark and one antiquark) and gluons.
 
     `gauge_leg`: a gluon leg whose wavefunction is left to the caller (no source row): the
-    gauge-invariance test uploads its momentum there."""
+    gauge-invariance test uploads its momentum there.
+    `part`: (k, parts): only the colour orderings k, k + parts, ... (a process whose plan does not
+    fit 64-bit words is split into parts, each its own plan; their outputs add up)."""
     n = len(legs)
     kinds = [outgoing_kind(leg) for leg in legs]
     gluons = [l for l in range(n) if kinds[l] == "g"]
@@ -191,6 +193,7 @@ def build(legs, alpha_s=ALPHA_S, gauge_leg=None):
         rest = gluons[1:]
         orderings = [tuple(p) for p in itertools.permutations(rest) if p[0] < p[-1]] if len(rest) > 1 else [tuple(rest)]
 
+    orderings = orderings[part[0]::part[1]]
     # the gluon words: contiguous sub-words of every ordering; the full word of a gluon-only
     # ordering is the closing current (no propagator, no tensor)
     full = set(orderings) if not quark_line else set()
@@ -390,3 +393,15 @@ PP4J = ["gg>gggg", "qg>qggg", "qq~>gggg", "gg>qq~gg"]
 
 def template(name, **kw):
     return build(PROCESSES[name], **kw)
+
+
+def parts(name):
+    """The fewest parts (1, 2, 3, 4, 6, ...) whose plans all fit 64-bit words: [template, ...].
+    A part evaluates a subset of the colour orderings; the process's outputs are their sum."""
+    for n in (1, 2, 3, 4, 5, 6, 8, 10, 12):
+        try:
+            return [template(name, part=(k, n)) for k in range(n)]
+        except ValueError as e:
+            if "bits" not in str(e):
+                raise
+    raise ValueError(f"{name}: no split into 12 or fewer parts fits 64-bit words")

@@ -104,3 +104,27 @@ def test_several_blocks_per_sm_give_the_same_bits(kind, blocks):
     b.run()
     torch.cuda.synchronize()
     check(out, want)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", ["f64", "mixed"])
+def test_six_gluon_parts_match_oracle_bitwise(kind):
+    """gg>gggg as its parts (subsets of the colour orderings), in one batch: each part's outputs
+    equal the oracle's bit for bit (one point per block, 512 lanes, 5 levels)."""
+    from pacuda_b200 import batch as B
+    import torch
+
+    parts = processes.parts("gg>gggg")
+    plans, ext, out, want = [], [], [], []
+    for k, t in enumerate(parts):
+        n = 40 + 13 * k
+        p = phase_space.sample(6, n, 31 + k, ecm=13000.0)
+        _, w = O.evaluate(t, p, kernel=abi.KERNELS[kind])
+        plans.append(B.Plan(t, kind))
+        ext.append(torch.tensor(phase_space.source_major(p), dtype=torch.float64, device="cuda"))
+        out.append(torch.full((n * t.outputs,), float("nan"), dtype=torch.float64, device="cuda"))
+        want.append(w)
+    b = B.Batch(plans, ext, out)
+    b.run()
+    torch.cuda.synchronize()
+    check(out, want)

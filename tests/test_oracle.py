@@ -225,3 +225,55 @@ def test_abi_struct_layout_is_the_references():
     assert C.sizeof(abi.ReduceResolved) == 64
     assert C.sizeof(abi.ReduceSample) == 96
     assert C.sizeof(abi.Options) == 24
+
+
+def test_six_gluon_parts_match_mhv_formulas_and_vanish():
+    """gg>gggg, split into parts of its 60 colour orderings (one plan would not fit 64-bit words):
+    every MHV and anti-MHV amplitude matches Parke-Taylor, every amplitude with at most one
+    negative or one positive helicity vanishes (NMHV ones are covered by the gauge test below)."""
+    legs = processes.PROCESSES["gg>gggg"]
+    n = len(legs)
+    parts = processes.parts("gg>gggg")
+    assert len(parts) > 1 and sum(len(t.meta["orderings"]) for t in parts) == 60
+    p = phase_space.sample(n, 2, 5)
+    sign = np.array([-1.0 if l.incoming else 1.0 for l in legs])
+    k = p * sign[None, :, None]
+    checked, worst, zero, typical = 0, 0.0, 0.0, 0.0
+    for t in parts:
+        amps, _ = O.evaluate(t, p)
+        typical = max(typical, np.abs(amps).max() ** 2 / G2 ** (n - 2))
+        for o, hel, a in t.meta["amplitudes"]:
+            neg = [l for l in range(n) if hel[l] == -1]
+            pos = [l for l in range(n) if hel[l] == 1]
+            cyc = [0] + list(o)
+            for pt in range(p.shape[0]):
+                a2 = abs(amps[a, pt]) ** 2 / G2 ** (n - 2)
+                if len(neg) <= 1 or len(pos) <= 1:
+                    zero = max(zero, a2)
+                elif len(neg) == 2 or len(pos) == 2:
+                    sel = neg if len(neg) == 2 else pos
+                    den = np.prod([_s(k, cyc[m], cyc[(m + 1) % n], pt) for m in range(n)])
+                    worst = max(worst, abs(a2 / (_s(k, sel[0], sel[1], pt) ** 4 / den) - 1))
+                    checked += 1
+    assert checked > 0 and worst < 1e-11, worst
+    assert zero < 1e-20 * typical
+
+
+def test_six_gluon_part_is_gauge_invariant():
+    """A gluon polarisation replaced by its momentum zeroes every amplitude of a gg>gggg part,
+    NMHV ones included."""
+    legs = processes.PROCESSES["gg>gggg"]
+    n = len(legs)
+    nparts = len(processes.parts("gg>gggg"))
+    p = phase_space.sample(n, 2, 7)
+    sign = np.array([-1.0 if l.incoming else 1.0 for l in legs])
+    ref, _ = O.evaluate(processes.template("gg>gggg", part=(1, nparts)), p)
+    for g in (0, 3):
+        t = processes.build(legs, gauge_leg=g, part=(1, nparts))
+        args = t.call(phase_space.source_major(p), 2)
+        for h in range(2):
+            base = 4 * (2 * g + h)
+            for c in range(4):
+                args.cre[(base + c) * 2:(base + c + 1) * 2] = sign[g] * p[:, g, c]
+        assert O.run(args, kernel=1) == 0
+        assert np.abs(args.are + 1j * args.aim).max() < 1e-10 * np.abs(ref).max()

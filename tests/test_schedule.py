@@ -57,3 +57,10 @@ def test_term_mode_refuses_shared_terms():
     offsets = np.concatenate([t.offsets, [t.offsets[-1] + 1]])
     applied = E.export_terms(*args, offsets, planes)[0]
     assert not applied
+
+
+def test_six_gluon_part_plan():
+    """A gg>gggg part (16-17 thousand rows, 5 levels, about 10 000 slots per point)."""
+    t = processes.parts("gg>gggg")[0]
+    check(t.words, t.width, t.current_planes, t.amplitude_planes, t.momentum_planes // 4, len(t.scale_re),
+          len(t.factor_re))
