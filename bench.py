@@ -182,6 +182,47 @@ def precision_line(torch, B, fams, ext, ref_out, steps, warmup, kind="mixed"):
             "blocks_per_sm": batch.blocks_per_sm}
 
 
+def six_gluon_line(torch, B, points=1 << 20, steps=3, warmup=2):
+    """The precision configuration: g g -> 4 g, leading colour (60 orderings x 64 helicities, as
+    the plan parts that fit 64-bit words), `points` seeded RAMBO points at 13 TeV with the loosened
+    cuts pT > 5 GeV and Delta R > 0.1; points/s in f64 and in mixed precision, and the histogram of
+    each point's relative error in |M|^2 (mixed against f64)."""
+    from pacuda_b200 import phase_space, processes
+
+    parts = processes.parts("gg>gggg")
+    p = phase_space.sample(6, points, SEED + 6, ecm=ECM, pt_min=5.0, dr_min=0.1)
+    ext = torch.tensor(phase_space.source_major(p), dtype=torch.float64, device="cuda")
+    res, totals = {"workload": f"gg>gggg LC: 60 orderings x 64 helicities as {len(parts)} plans, {points} points, "
+                               "13 TeV, pT>5 GeV, |eta|<5, dR>0.1"}, {}
+    for kind in ("f64", "mixed"):
+        plans = [B.Plan(t, kind) for t in parts]
+        outs = [torch.empty(points * t.outputs, dtype=torch.float64, device="cuda") for t in parts]
+        batch = B.Batch(plans, [ext] * len(parts), outs)
+        for _ in range(warmup):
+            batch.run()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            batch.run()
+        e1.record()
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        flops = sum(pl.flops for pl in plans) * points
+        res[kind] = {"value": points / (ms * 1e-3), "unit": "points/s", "ms_per_step": ms,
+                     "tflops": flops / (ms * 1e-3) / 1e12,
+                     "lanes_per_point": [batch.lanes_per_point(k) for k in range(len(plans))]}
+        totals[kind] = sum(o.view(points, t.outputs).sum(dim=1) for o, t in zip(outs, parts))
+        del batch, outs
+    rel = ((totals["mixed"] - totals["f64"]).abs() / totals["f64"].abs().clamp_min(1e-300)).cpu().numpy()
+    edges = [0.0] + [10.0 ** e for e in range(-16, 1)] + [np.inf]
+    hist, _ = np.histogram(rel, bins=edges)
+    res["mixed"]["rel_error_vs_f64"] = {
+        "median": float(np.median(rel)), "q999": float(np.quantile(rel, 0.999)), "max": float(rel.max()),
+        "frac_le_1e-10": float((rel <= 1e-10).mean()),
+        "histogram": {"edges_log10": list(range(-16, 1)), "counts": [int(c) for c in hist]}}
+    return res
+
+
 def dram_bytes_per_point():
     """DRAM bytes per point of the batch kernel, from the committed ncu summary (one capture of the
     same family mix), or None."""
@@ -355,7 +396,7 @@ def main():
     ap.add_argument("--points", type=int, default=POINTS, help="points per GPU")
     ap.add_argument("--no-tune", action="store_true", help="keep the default points per warp")
     ap.add_argument("--lanes-per-point", type=int, default=0)
-    ap.add_argument("--no-precision", action="store_true", help="skip the mixed-precision line")
+    ap.add_argument("--no-precision", action="store_true", help="skip the mixed-precision lines")
     ap.add_argument("--blocks-per-sm", type=int, default=0, help="1, 2 or 4 (with --no-tune or --lanes-per-point)")
     args = ap.parse_args()
     POINTS = args.points
@@ -487,6 +528,7 @@ def main():
         if not args.no_precision:
             res["precision"] = [precision_line(torch, B, fams, ext, out, args.steps, args.warmup, k)
                                 for k in ("mixed", "mixed64", "df64")]
+            res["precision_gg4g"] = six_gluon_line(torch, B)
     if world > 1:
         import torch.distributed as dist
 
