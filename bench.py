@@ -223,6 +223,56 @@ def six_gluon_line(torch, B, points=1 << 20, steps=3, warmup=2):
     return res
 
 
+def pp4j_line(torch, B, points=1 << 22, steps=3, warmup=2):
+    """p p -> 4 jets, every massless family the intrinsic ops express (gg>gggg as its plan parts,
+    qg>qggg, qq~>gggg, gg>qq~gg), `points` seeded RAMBO points at 13 TeV with pT > 20 GeV and
+    Delta R > 0.4 split over the families by seeded random weights, all in one persistent launch:
+    points/s in f64 and in mixed precision, with the mixed kernel's relative error in |M|^2."""
+    from pacuda_b200 import phase_space, processes
+
+    names = processes.PP4J
+    rng = np.random.default_rng(SEED + 4)
+    w = rng.dirichlet(np.ones(len(names)))
+    counts = np.maximum(1024, np.floor(w * points).astype(int))
+    counts[int(np.argmax(counts))] += points - counts.sum()
+    fams = []
+    for k, (name, n) in enumerate(zip(names, counts)):
+        p = phase_space.sample(6, int(n), SEED + 40 + k, ecm=ECM)
+        e = torch.tensor(phase_space.source_major(p), dtype=torch.float64, device="cuda")
+        for t in processes.parts(name):
+            fams.append((name, t, int(n), e))
+    res, totals = {"workload": f"pp>4j LC f64: {', '.join(names)}; {points} points, 13 TeV, pT>20 GeV, |eta|<5, "
+                               f"dR>0.4; {len(fams)} plans in one launch",
+                   "points_per_family": {nm: int(c) for nm, c in zip(names, counts)}}, {}
+    for kind in ("f64", "mixed"):
+        plans = [B.Plan(t, kind) for _, t, _, _ in fams]
+        outs = [torch.empty(n * t.outputs, dtype=torch.float64, device="cuda") for _, t, n, _ in fams]
+        batch = B.Batch(plans, [e for *_, e in fams], outs)
+        batch.blocks_per_sm = 1
+        for _ in range(warmup):
+            batch.run()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            batch.run()
+        e1.record()
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        flops = sum(pl.flops * n for pl, (_, _, n, _) in zip(plans, fams))
+        res[kind] = {"value": points / (ms * 1e-3), "unit": "points/s", "ms_per_step": ms,
+                     "tflops": flops / (ms * 1e-3) / 1e12}
+        per_family = {}
+        for (name, t, n, _), o in zip(fams, outs):
+            x = o.view(n, t.outputs).sum(dim=1)
+            per_family[name] = per_family[name] + x if name in per_family else x
+        totals[kind] = torch.cat([per_family[nm] for nm in names])
+        del batch, outs
+    rel = ((totals["mixed"] - totals["f64"]).abs() / totals["f64"].abs().clamp_min(1e-300)).cpu().numpy()
+    res["mixed"]["rel_error_vs_f64"] = {"median": float(np.median(rel)), "q999": float(np.quantile(rel, 0.999)),
+                                        "max": float(rel.max())}
+    return res
+
+
 def dram_bytes_per_point():
     """DRAM bytes per point of the batch kernel, from the committed ncu summary (one capture of the
     same family mix), or None."""
@@ -529,6 +579,7 @@ def main():
             res["precision"] = [precision_line(torch, B, fams, ext, out, args.steps, args.warmup, k)
                                 for k in ("mixed", "mixed64", "df64")]
             res["precision_gg4g"] = six_gluon_line(torch, B)
+            res["pp4j"] = pp4j_line(torch, B)
     if world > 1:
         import torch.distributed as dist
 
