@@ -260,21 +260,24 @@ def write(f: PacudaFile, path):
 
 
 def from_processes(names, kernel=1, batch=0, reference_points=8, seed=7):
-    """A file of generated plans (pacuda_b200.processes), one colour each, with `reference_points`
-    RAMBO points and their f64 values computed by `evaluate(template, momenta) -> [point][output]`
-    when given (the caller's evaluator, e.g. the runner)."""
+    """A file of generated plans (pacuda_b200.processes): one colour "lc" per process, or, for a
+    process whose plan is split into parts of its colour orderings, one colour per part ("lc0",
+    "lc1", ...: their values add up), with `reference_points` RAMBO points (their values left zero)."""
     from . import phase_space, processes
 
     f = PacudaFile(kernel=kernel, batch=batch)
     for name in names:
         legs = processes.PROCESSES[name]
-        t = processes.template(name)
-        t.tile = 1 << 16
-        num, den = t.meta["group_factor"]
-        p = Process(key=name, legs=len(legs), helicities=t.outputs, alpha_s_name="aS", alpha_s=t.meta["alpha_s"],
-                    qcd_power=t.meta["qcd_power"], factor=(num, den))
+        parts = processes.parts(name)
+        t0 = parts[0]
+        num, den = t0.meta["group_factor"]
+        p = Process(key=name, legs=len(legs), helicities=t0.outputs, alpha_s_name="aS", alpha_s=t0.meta["alpha_s"],
+                    qcd_power=t0.meta["qcd_power"], factor=(num, den))
         mom = phase_space.sample(len(legs), reference_points, seed) if reference_points else np.zeros((0, len(legs), 4))
-        p.colours.append(Colour("lc", t, mom.reshape(-1), np.zeros(reference_points * t.outputs), reference_points))
+        for k, t in enumerate(parts):
+            t.tile = 1 << 16
+            cid = "lc" if len(parts) == 1 else f"lc{k}"
+            p.colours.append(Colour(cid, t, mom.reshape(-1), np.zeros(reference_points * t.outputs), reference_points))
         f.processes.append(p)
     return f
 

@@ -156,3 +156,57 @@ def test_a_call_of_several_chunks(umami, mode):
     assert same_bits(me[offset:offset + count], want_me)
     if mode == "sample":
         assert np.array_equal(hel[offset:offset + count], want_hel)
+
+
+
+@pytest.mark.gpu
+def test_six_gluon_subprocess_sums_its_colour_parts(tmp_path):
+    """A gg>gggg subprocess whose one flavour lists the process's three plan parts as three
+    colour contributions: the helicity sum of |M|^2 is their sum, as the reference library adds a
+    flavour's contributions, bit for bit against the oracle's values."""
+    from oracle import oracle as O
+    from pacuda_b200 import build, pacuda_file, phase_space, processes
+    from pacuda_b200.umami import build as ubuild, provider
+
+    build.build()
+    parts = processes.parts("gg>gggg")
+    spec = {"particles": 6, "masses": [0.0] * 6, "colors": 1,
+            "processes": [{"key": "gg>gggg", "helicities": 64, "parameters": [("aS", 0.118, 0.0, False, True)]}],
+            "channels": [[[{"process": 0, "colour": f"lc{k}", "permutation": list(range(6)), "factor": 1.0}
+                           for k in range(len(parts))]]],
+            "has_alpha_s": True, "has_color_flow": False}
+    hdr = tmp_path / "provider_6g.h"
+    hdr.write_text(provider.header(spec))
+    lib = C.CDLL(ubuild.build(str(hdr), str(tmp_path / "libumami_6g.so")))
+    lib.umami_initialize.argtypes = [C.POINTER(C.c_void_p), C.c_char_p]
+    lib.umami_matrix_element.argtypes = [C.c_void_p, C.c_size_t, C.c_size_t, C.c_size_t, C.c_size_t,
+                                         C.POINTER(C.c_int), C.POINTER(C.c_void_p), C.c_size_t,
+                                         C.POINTER(C.c_int), C.POINTER(C.c_void_p)]
+    lib.umami_free.argtypes = [C.c_void_p]
+    art = tmp_path / "artifact6"
+    art.mkdir()
+    pacuda_file.write(pacuda_file.from_processes(["gg>gggg"], reference_points=0), str(art) + ".pacuda")
+    h = C.c_void_p()
+    assert lib.umami_initialize(C.byref(h), str(art).encode()) == 0
+    n = 300
+    p = phase_space.sample(6, n, 17, ecm=13000.0)
+    m = np.ascontiguousarray(p.transpose(2, 1, 0).reshape(24, n))  # [6 k + leg][event]
+    me = np.zeros(n)
+    ik, ip = (C.c_int * 1)(0), (C.c_void_p * 1)(m.ctypes.data)
+    ok, op = (C.c_int * 1)(0), (C.c_void_p * 1)(me.ctypes.data)
+    try:
+        assert lib.umami_matrix_element(h, n, n, 0, 1, ik, ip, 1, ok, op) == 0
+    finally:
+        lib.umami_free(h)
+    num, den = parts[0].meta["group_factor"]
+    total = np.zeros(n)
+    for t in parts:
+        _, out = O.evaluate(t, p, kernel=1)
+        live = np.asarray(t.offsets[1:]) > np.asarray(t.offsets[:-1])
+        v = out * float(num) / float(den)
+        v[:, ~live] = 0.0
+        value = np.zeros(n)
+        for hel in range(v.shape[1]):
+            value = value + v[:, hel]
+        total = total + 1.0 * value
+    assert same_bits(me, total)
