@@ -179,7 +179,7 @@ def precision_line(torch, B, fams, ext, ref_out, steps, warmup, kind="mixed"):
             "rel_error_vs_f64": {"median": float(np.median(rel)), "q999": float(np.quantile(rel, 0.999)),
                                  "max": float(rel.max()), "frac_le_1e-10": float((rel <= 1e-10).mean())},
             "lanes_per_point": {nm: batch.lanes_per_point(k) for k, (nm, _, _) in enumerate(fams)},
-            "blocks_per_sm": batch.blocks_per_sm}
+            "blocks_per_sm": {nm: batch.plan_blocks_per_sm(k) for k, (nm, _, _) in enumerate(fams)}}
 
 
 def six_gluon_line(torch, B, points=1 << 20, steps=3, warmup=2):
@@ -560,7 +560,7 @@ def main():
                         "flops_per_point": {n: pl.flops for (n, _, _), pl in zip(fams, plans)}},
            "points_per_family": {n: p.shape[0] for n, _, p in fams},
            "lanes_per_point": {n: batch.lanes_per_point(k) for k, (n, _, _) in enumerate(fams)},
-           "blocks_per_sm": batch.blocks_per_sm,
+           "blocks_per_sm": {n: batch.plan_blocks_per_sm(k) for k, (n, _, _) in enumerate(fams)},
            "sum_m2_per_family": [float(x) for x in sums.cpu()],
            "sum_m2_squared_per_family": [float(x) for x in squares.cpu()],
            "max_m2_per_family": [float(x) for x in peak_m2.cpu()]}

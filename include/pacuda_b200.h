@@ -63,21 +63,27 @@ pacuda_b200_batch *pacuda_b200_batch_create(pacuda_b200_plan *const *plans, uint
 int pacuda_b200_batch_update(pacuda_b200_batch *batch, const double *const *external, const uint32_t *count,
                              double *const *output);
 /* Times each plan's lanes-per-point choices on its own points, with 1, 2 and 4 blocks per SM, and
- * keeps the fastest (the blocks-per-SM choice whose plans' times add up least). */
+ * keeps each plan's fastest pair; plans of the same blocks per SM share one launch (a run is then
+ * one launch per blocks-per-SM choice in use, one after the other on the stream). */
 int pacuda_b200_batch_tune(pacuda_b200_batch *batch, void *stream);
 /* One persistent launch over every plan's points, on `stream` (a cudaStream_t; NULL: default). */
 int pacuda_b200_batch_run(pacuda_b200_batch *batch, void *stream);
 /* Captures the launch into a CUDA graph on `stream`; later runs replay it. */
 int pacuda_b200_batch_capture(pacuda_b200_batch *batch, void *stream);
-/* Blocks per SM of the batch's launch: 1 (one block of all the warps the registers allow), 2 or 4
+/* Blocks per SM of every plan's launch: 1 (one block of all the warps the registers allow), 2 or 4
  * (independent blocks that share the SM's warps and shared memory: while one waits at a level's
- * barrier the others run); 0: 1. INVALID when the plans' points do not fit. */
+ * barrier the others run); 0: 1. Replaces the tuner's per-plan choices. INVALID when the plans'
+ * points do not fit. */
 int pacuda_b200_batch_set_blocks_per_sm(pacuda_b200_batch *batch, uint32_t blocks);
 uint32_t pacuda_b200_batch_blocks_per_sm(const pacuda_b200_batch *batch);
+/* the blocks per SM plan k runs with (its own choice, else the batch's); setting 0 returns it to
+ * the batch's. INVALID when its points do not fit. */
+int pacuda_b200_batch_set_plan_blocks_per_sm(pacuda_b200_batch *batch, uint32_t plan, uint32_t blocks);
+uint32_t pacuda_b200_batch_plan_blocks_per_sm(const pacuda_b200_batch *batch, uint32_t plan);
 /* the lanes per point plan k runs with in this batch's launch (its own choice where that fits the
  * launch's blocks, else the default for them), or 0 */
 uint32_t pacuda_b200_batch_lanes_per_point(const pacuda_b200_batch *batch, uint32_t plan);
-/* kernel launches of one run (1) */
+/* kernel launches of one run (one per blocks-per-SM choice in use) */
 uint32_t pacuda_b200_batch_launches(const pacuda_b200_batch *batch);
 void pacuda_b200_batch_destroy(pacuda_b200_batch *batch);
 

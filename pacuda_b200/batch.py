@@ -36,6 +36,9 @@ def lib(path=None):
         L.pacuda_b200_batch_blocks_per_sm.restype = C.c_uint32
         L.pacuda_b200_batch_lanes_per_point.argtypes = [C.c_void_p, C.c_uint32]
         L.pacuda_b200_batch_lanes_per_point.restype = C.c_uint32
+        L.pacuda_b200_batch_plan_blocks_per_sm.argtypes = [C.c_void_p, C.c_uint32]
+        L.pacuda_b200_batch_set_plan_blocks_per_sm.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32]
+        L.pacuda_b200_batch_plan_blocks_per_sm.restype = C.c_uint32
         L.pacuda_b200_batch_destroy.argtypes = [C.c_void_p]
     return _lib
 
@@ -120,6 +123,14 @@ class Batch:
     def lanes_per_point(self, k):
         """The lanes per point plan k runs with in this batch's launch."""
         return lib().pacuda_b200_batch_lanes_per_point(self.handle, k)
+
+    def plan_blocks_per_sm(self, k):
+        """The blocks per SM plan k runs with."""
+        return lib().pacuda_b200_batch_plan_blocks_per_sm(self.handle, k)
+
+    def set_plan_blocks_per_sm(self, k, blocks):
+        if lib().pacuda_b200_batch_set_plan_blocks_per_sm(self.handle, k, blocks) != 0:
+            raise RunnerError(f"plan {k}: {blocks} blocks per SM do not fit")
 
     @property
     def blocks_per_sm(self):

@@ -53,23 +53,31 @@ struct pacuda_b200_plan {
     bool fixed = false;
 };
 
-struct LaunchBlock;  // device and pinned host copies of a launch's descriptors
+// The plans of one launch: those that run with the same blocks per SM.
+struct LaunchGroup {
+    std::vector<uint32_t> plans;  // indices into the batch's plans
+    int blocks = 1, threads = 0;
+    size_t smem = 0, const_bytes = 0;
+    size_t at = 0;                // its section of the descriptor block
+};
 
 struct pacuda_b200_batch {
     std::vector<pacuda_b200_plan *> plans;
     std::vector<const double *> external;
     std::vector<uint32_t> count;
     std::vector<double *> output;
-    std::vector<uint32_t> points;  // per plan: its points per block in this batch's launch
-    // descriptor block: TiledPlan[n] | item_first[n + 1] | external[n] | output[n] | count[n] | counter
+    std::vector<uint32_t> points;      // per plan: its points per block in this batch's launch
+    std::vector<int> plan_blocks;      // per plan: its blocks per SM (0: the batch's)
+    int blocks = 1;                    // the batch's blocks per SM (tiled_host.h kMaxBlocks)
+    // one launch per group; the descriptor block holds a section per group:
+    // TiledPlan[n] | item_first[n + 1] | external[n] | output[n] | count[n] | counter
+    std::vector<LaunchGroup> groups;
     unsigned char *host = nullptr, *device = nullptr;
     size_t bytes = 0;
-    int threads = 0, sms = 0;
-    int blocks = 1;  // per SM (tiled_host.h kMaxBlocks)
-    size_t smem = 0, const_bytes = 0;
+    int sms = 0;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
-    cudaEvent_t copied = nullptr;  // recorded after each launch's descriptor copy
+    cudaEvent_t copied = nullptr;  // recorded after each run's descriptor copy
 };
 
 namespace {
@@ -106,70 +114,98 @@ Offsets layout(size_t n) {
     return o;
 }
 
-// the host block from the batch's current choices; the launch's shared memory and warps
+// The groups and the host block from the batch's current choices: each group's shared memory and
+// warps, each plan's points per block. The block is allocated again only when its size changes.
 bool prepare(pacuda_b200_batch *b) {
-    size_t n = b->plans.size();
-    Offsets o = layout(n);
-    if (!b->host) {
-        b->bytes = o.total;
+    const size_t n = b->plans.size();
+    const int kernel = b->plans[0]->kernel;
+    b->plan_blocks.resize(n, 0);
+    b->groups.clear();
+    for (size_t k = 0; k < n; k++) {
+        int blocks = b->plan_blocks[k] ? b->plan_blocks[k] : b->blocks;
+        size_t g = 0;
+        while (g < b->groups.size() && b->groups[g].blocks != blocks) g++;
+        if (g == b->groups.size()) {
+            b->groups.emplace_back();
+            b->groups.back().blocks = blocks;
+        }
+        b->groups[g].plans.push_back((uint32_t)k);
+    }
+    size_t bytes = 0;
+    for (LaunchGroup &g : b->groups) {
+        g.at = bytes;
+        bytes += layout(g.plans.size()).total;
+    }
+    if (!b->host || bytes != b->bytes) {
+        cudaFreeHost(b->host);
+        cudaFree(b->device);
+        b->host = nullptr;
+        b->device = nullptr;
+        b->bytes = bytes;
         if (failed(cudaMallocHost((void **)&b->host, b->bytes), "pinned descriptors") ||
             failed(cudaMalloc((void **)&b->device, b->bytes), "descriptors"))
             return false;
     }
     memset(b->host, 0, b->bytes);
     b->points.assign(n, 0);
-    TiledPlan *plans = (TiledPlan *)(b->host + o.plans);
-    unsigned long long *items = (unsigned long long *)(b->host + o.items);
-    const int kernel = b->plans[0]->kernel;
-    b->threads = tiled_threads(kernel, b->blocks);
-    b->const_bytes = 0;
-    for (size_t k = 0; k < n; k++)
-        b->const_bytes = std::max(b->const_bytes, tiled_const_bytes(b->plans[k]->scales, b->plans[k]->factors));
-    size_t room = tiled_max_smem(kernel, b->blocks);
-    if (room <= b->const_bytes) {
-        fprintf(stderr, "%s: the plans' constants do not fit a block's shared memory\n", kTag);
-        return false;
-    }
-    size_t max_smem = room - b->const_bytes;
-    b->smem = 0;
-    items[0] = 0;
-    for (size_t k = 0; k < n; k++) {
-        pacuda_b200_plan *p = b->plans[k];
-        uint32_t most = tiled_max_points(p->point_bytes, b->threads, max_smem);
-        if (!most || p->tiled.threads != tiled_threads(kernel)) {
-            fprintf(stderr, "%s: a plan's point does not fit a block's shared memory\n", kTag);
+    for (LaunchGroup &g : b->groups) {
+        const size_t m = g.plans.size();
+        Offsets o = layout(m);
+        unsigned char *base = b->host + g.at;
+        TiledPlan *plans = (TiledPlan *)(base + o.plans);
+        unsigned long long *items = (unsigned long long *)(base + o.items);
+        g.threads = tiled_threads(kernel, g.blocks);
+        g.const_bytes = 0;
+        for (uint32_t k : g.plans)
+            g.const_bytes = std::max(g.const_bytes, tiled_const_bytes(b->plans[k]->scales, b->plans[k]->factors));
+        size_t room = tiled_max_smem(kernel, g.blocks);
+        if (room <= g.const_bytes) {
+            fprintf(stderr, "%s: the plans' constants do not fit a block's shared memory\n", kTag);
             return false;
         }
-        // the plan's choice where it fits this launch, else the default for it
-        uint32_t per = tiled_points_fit(p->points, p->point_bytes, b->threads, max_smem)
-                           ? p->points
-                           : tiled_default_points(p->point_bytes, b->threads, max_smem);
-        b->points[k] = per;
-        fill_plan(p, plans[k], per, b->blocks);
-        b->smem = std::max<size_t>(b->smem, (size_t)per * p->point_bytes);
-        items[k + 1] = items[k] + (b->count[k] + per - 1) / per;
+        size_t max_smem = room - g.const_bytes;
+        g.smem = 0;
+        items[0] = 0;
+        for (size_t j = 0; j < m; j++) {
+            const uint32_t k = g.plans[j];
+            pacuda_b200_plan *p = b->plans[k];
+            uint32_t most = tiled_max_points(p->point_bytes, g.threads, max_smem);
+            if (!most || p->tiled.threads != tiled_threads(kernel)) {
+                fprintf(stderr, "%s: a plan's point does not fit a block's shared memory\n", kTag);
+                return false;
+            }
+            // the plan's choice where it fits this launch, else the default for it
+            uint32_t per = tiled_points_fit(p->points, p->point_bytes, g.threads, max_smem)
+                               ? p->points
+                               : tiled_default_points(p->point_bytes, g.threads, max_smem);
+            b->points[k] = per;
+            fill_plan(p, plans[j], per, g.blocks);
+            g.smem = std::max<size_t>(g.smem, (size_t)per * p->point_bytes);
+            items[j + 1] = items[j] + (b->count[k] + per - 1) / per;
+            ((const double **)(base + o.external))[j] = b->external[k];
+            ((double **)(base + o.output))[j] = b->output[k];
+            ((uint32_t *)(base + o.count))[j] = b->count[k];
+        }
+        g.smem += g.const_bytes;
     }
-    memcpy(b->host + o.external, b->external.data(), n * 8);
-    memcpy(b->host + o.output, b->output.data(), n * 8);
-    memcpy(b->host + o.count, b->count.data(), n * 4);
-    b->smem += b->const_bytes;
     return true;
 }
 
-TiledLaunch launch_args(const pacuda_b200_batch *b) {
-    size_t n = b->plans.size();
-    Offsets o = layout(n);
+TiledLaunch launch_args(const pacuda_b200_batch *b, const LaunchGroup &g) {
+    const size_t m = g.plans.size();
+    Offsets o = layout(m);
+    unsigned char *base = b->device + g.at;
     TiledLaunch L;
     memset(&L, 0, sizeof L);
-    L.plans = (const TiledPlan *)(b->device + o.plans);
-    L.nplans = (uint32_t)n;
-    L.item_first = (const unsigned long long *)(b->device + o.items);
-    L.external = (const double *const *)(b->device + o.external);
-    L.output = (double *const *)(b->device + o.output);
-    L.count = (const uint32_t *)(b->device + o.count);
-    L.counter = (unsigned long long *)(b->device + o.counter);
+    L.plans = (const TiledPlan *)(base + o.plans);
+    L.nplans = (uint32_t)m;
+    L.item_first = (const unsigned long long *)(base + o.items);
+    L.external = (const double *const *)(base + o.external);
+    L.output = (double *const *)(base + o.output);
+    L.count = (const uint32_t *)(base + o.count);
+    L.counter = (unsigned long long *)(base + o.counter);
     L.abi = false;
-    L.const_bytes = (uint32_t)b->const_bytes;
+    L.const_bytes = (uint32_t)g.const_bytes;
     return L;
 }
 
@@ -181,9 +217,10 @@ int launch(pacuda_b200_batch *b, cudaStream_t s) {
     cudaStreamIsCapturing(s, &capturing);
     if (capturing == cudaStreamCaptureStatusNone && b->copied && failed(cudaEventRecord(b->copied, s), "event"))
         return PACMAN_RECURRENCE_DEVICE_ERROR;
-    if (!launch_tiled(b->plans[0]->kernel, launch_args(b), b->threads, b->smem, b->sms * b->blocks, s) ||
-        failed(cudaGetLastError(), "launch"))
-        return PACMAN_RECURRENCE_DEVICE_ERROR;
+    for (const LaunchGroup &g : b->groups)
+        if (!launch_tiled(b->plans[0]->kernel, launch_args(b, g), g.threads, g.smem, b->sms * g.blocks, s) ||
+            failed(cudaGetLastError(), "launch"))
+            return PACMAN_RECURRENCE_DEVICE_ERROR;
     return PACMAN_RECURRENCE_OK;
 }
 
@@ -442,42 +479,34 @@ extern "C" int pacuda_b200_batch_tune(pacuda_b200_batch *b, void *stream) {
         p->points = keep;
         return ms;
     };
-    // per blocks-per-SM choice: each plan's fastest points per block (from the most that fit down
-    // to half of them: fewer leave more of a block's lanes idle at the levels' barriers); the
-    // choice whose plans' times add up least is kept
-    std::vector<uint32_t> choice[kMaxBlocks + 1];
-    float total[kMaxBlocks];
+    // per plan: its fastest points per block (from the most that fit down to half of them:
+    // fewer leave more of a block's lanes idle at the levels' barriers) for each blocks-per-SM
+    // choice, and the fastest pair; plans of the same blocks per SM share a launch
     const int kernel = b->plans[0]->kernel;
-    for (int blocks = 1; blocks <= kMaxBlocks; blocks++) {
-        total[blocks - 1] = -1.0f;
-        if (blocks == 3) continue;  // (16 warps do not split in three)
-        int threads = tiled_threads(kernel, blocks);
-        size_t room = tiled_max_smem(kernel, blocks);
-        total[blocks - 1] = 0.0f;
-        for (size_t k = 0; k < b->plans.size() && total[blocks - 1] >= 0.0f; k++) {
-            pacuda_b200_plan *p = b->plans[k];
-            size_t cb = tiled_const_bytes(p->scales, p->factors);
+    for (size_t k = 0; k < b->plans.size(); k++) {
+        pacuda_b200_plan *p = b->plans[k];
+        size_t cb = tiled_const_bytes(p->scales, p->factors);
+        float best = -1.0f;
+        uint32_t best_points = p->points;
+        int best_blocks = 0;
+        for (int blocks = 1; blocks <= kMaxBlocks; blocks *= 2) {
+            int threads = tiled_threads(kernel, blocks);
+            size_t room = tiled_max_smem(kernel, blocks);
             uint32_t most = room > cb ? tiled_max_points(p->point_bytes, threads, room - cb) : 0;
-            float best = -1.0f;
-            uint32_t best_points = 0;
             for (uint32_t points = most; points >= 1 && 2 * points >= most; points--) {
                 if (p->fixed && points != p->points) continue;
                 float ms = time_plan(k, points, blocks);
                 if (ms >= 0.0f && (best < 0.0f || ms < best)) {
                     best = ms;
                     best_points = points;
+                    best_blocks = blocks;
                 }
             }
-            choice[blocks - 1].push_back(best_points);
-            total[blocks - 1] = best < 0.0f ? -1.0f : total[blocks - 1] + best;
         }
-    }
-    int pick = 1;
-    for (int blocks = 2; blocks <= kMaxBlocks; blocks++)
-        if (total[blocks - 1] >= 0.0f && (total[pick - 1] < 0.0f || total[blocks - 1] < total[pick - 1])) pick = blocks;
-    if (total[pick - 1] >= 0.0f) {
-        for (size_t k = 0; k < b->plans.size(); k++) b->plans[k]->points = choice[pick - 1][k];
-        b->blocks = pick;
+        if (best >= 0.0f) {
+            p->points = best_points;
+            b->plan_blocks[k] = best_blocks;
+        }
     }
     cudaEventDestroy(t0);
     cudaEventDestroy(t1);
@@ -490,7 +519,7 @@ extern "C" int pacuda_b200_batch_tune(pacuda_b200_batch *b, void *stream) {
     return prepare(b) ? PACMAN_RECURRENCE_OK : PACMAN_RECURRENCE_DEVICE_ERROR;
 }
 
-extern "C" uint32_t pacuda_b200_batch_launches(const pacuda_b200_batch *b) { return b ? 1 : 0; }
+extern "C" uint32_t pacuda_b200_batch_launches(const pacuda_b200_batch *b) { return b ? (uint32_t)b->groups.size() : 0; }
 
 extern "C" int pacuda_b200_batch_set_blocks_per_sm(pacuda_b200_batch *b, uint32_t blocks) {
     if (!b || blocks > (uint32_t)kMaxBlocks || blocks == 3) return PACMAN_RECURRENCE_INVALID;
@@ -502,9 +531,12 @@ extern "C" int pacuda_b200_batch_set_blocks_per_sm(pacuda_b200_batch *b, uint32_
         b->graph = nullptr;
     }
     int before = b->blocks;
+    std::vector<int> before_plans = b->plan_blocks;
     b->blocks = blocks ? (int)blocks : 1;
+    std::fill(b->plan_blocks.begin(), b->plan_blocks.end(), 0);  // every plan the same
     if (!prepare(b)) {
         b->blocks = before;
+        b->plan_blocks = before_plans;
         prepare(b);
         return PACMAN_RECURRENCE_INVALID;
     }
@@ -513,8 +545,36 @@ extern "C" int pacuda_b200_batch_set_blocks_per_sm(pacuda_b200_batch *b, uint32_
 
 extern "C" uint32_t pacuda_b200_batch_blocks_per_sm(const pacuda_b200_batch *b) { return b ? (uint32_t)b->blocks : 0; }
 
+extern "C" int pacuda_b200_batch_set_plan_blocks_per_sm(pacuda_b200_batch *b, uint32_t plan, uint32_t blocks) {
+    if (!b || plan >= b->plans.size() || blocks > (uint32_t)kMaxBlocks || blocks == 3) return PACMAN_RECURRENCE_INVALID;
+    if (failed(cudaEventSynchronize(b->copied), "batch")) return PACMAN_RECURRENCE_DEVICE_ERROR;
+    if (b->exec) {
+        cudaGraphExecDestroy(b->exec);
+        cudaGraphDestroy(b->graph);
+        b->exec = nullptr;
+        b->graph = nullptr;
+    }
+    int before = b->plan_blocks[plan];
+    b->plan_blocks[plan] = (int)blocks;
+    if (!prepare(b)) {
+        b->plan_blocks[plan] = before;
+        prepare(b);
+        return PACMAN_RECURRENCE_INVALID;
+    }
+    return PACMAN_RECURRENCE_OK;
+}
+
+extern "C" uint32_t pacuda_b200_batch_plan_blocks_per_sm(const pacuda_b200_batch *b, uint32_t plan) {
+    if (!b || plan >= b->plan_blocks.size()) return 0;
+    return (uint32_t)(b->plan_blocks[plan] ? b->plan_blocks[plan] : b->blocks);
+}
+
 extern "C" uint32_t pacuda_b200_batch_lanes_per_point(const pacuda_b200_batch *b, uint32_t plan) {
-    return b && plan < b->points.size() && b->points[plan] ? tiled_lanes(b->points[plan], b->threads) : 0;
+    if (!b || plan >= b->points.size() || !b->points[plan]) return 0;
+    for (const LaunchGroup &g : b->groups)
+        for (uint32_t k : g.plans)
+            if (k == plan) return tiled_lanes(b->points[plan], g.threads);
+    return 0;
 }
 
 extern "C" void pacuda_b200_batch_destroy(pacuda_b200_batch *b) {

@@ -86,7 +86,29 @@ def test_tuned_and_captured_runs_give_the_same_bits():
     b.run()
     torch.cuda.synchronize()
     check(out, want)
-    assert b.launches == 1
+    assert b.launches == len({b.plan_blocks_per_sm(k) for k in range(len(plans))})
+
+
+@pytest.mark.gpu
+def test_plans_of_different_blocks_per_sm_run_as_launches_of_one_batch():
+    """Plans with 1, 2 and 4 blocks per SM in one batch: three launches, each plan's bits."""
+    from pacuda_b200 import batch as B
+    import torch
+
+    plans, ext, out, want = setup("f64", [300, 200, 100, 50])
+    b = B.Batch(plans, ext, out)
+    for k, blocks in enumerate([4, 2, 1, 2]):
+        b.set_plan_blocks_per_sm(k, blocks)
+    assert [b.plan_blocks_per_sm(k) for k in range(4)] == [4, 2, 1, 2] and b.launches == 3
+    b.run()
+    torch.cuda.synchronize()
+    check(out, want)
+    for o in out:
+        o.fill_(float("nan"))
+    b.capture()
+    b.run()
+    torch.cuda.synchronize()
+    check(out, want)
 
 
 @pytest.mark.gpu
