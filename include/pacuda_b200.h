@@ -72,8 +72,9 @@ int pacuda_b200_batch_run(pacuda_b200_batch *batch, void *stream);
 int pacuda_b200_batch_capture(pacuda_b200_batch *batch, void *stream);
 /* Blocks per SM of every plan's launch: 1 (one block of all the warps the registers allow), 2 or 4
  * (independent blocks that share the SM's warps and shared memory: while one waits at a level's
- * barrier the others run); 0: 1. Replaces the tuner's per-plan choices. INVALID when the plans'
- * points do not fit. */
+ * barrier the others run); 0: chosen per plan without timing (four for a plan of at most four
+ * points per 16-warp block, else two). Replaces the tuner's per-plan choices. INVALID when the
+ * plans' points do not fit. A new batch has 1. */
 int pacuda_b200_batch_set_blocks_per_sm(pacuda_b200_batch *batch, uint32_t blocks);
 uint32_t pacuda_b200_batch_blocks_per_sm(const pacuda_b200_batch *batch);
 /* the blocks per SM plan k runs with (its own choice, else the batch's); setting 0 returns it to

@@ -68,7 +68,7 @@ struct pacuda_b200_batch {
     std::vector<double *> output;
     std::vector<uint32_t> points;      // per plan: its points per block in this batch's launch
     std::vector<int> plan_blocks;      // per plan: its blocks per SM (0: the batch's)
-    int blocks = 1;                    // the batch's blocks per SM (tiled_host.h kMaxBlocks)
+    int blocks = 1;                    // the batch's blocks per SM (tiled_host.h kMaxBlocks); 0: automatic
     // one launch per group; the descriptor block holds a section per group:
     // TiledPlan[n] | item_first[n + 1] | external[n] | output[n] | count[n] | counter
     std::vector<LaunchGroup> groups;
@@ -114,6 +114,24 @@ Offsets layout(size_t n) {
     return o;
 }
 
+// Blocks per SM chosen without timing: four blocks (their points run on fewer, independent warps)
+// for a plan that fits at most four points in a block of all the warps, else two; fewer when the
+// points do not fit. (Measured on B200: gg>ggg, 4 points per 16 warps, gains 5 % at four blocks
+// over two; qg>qgg, 16 points, loses 14 % at four.)
+int auto_blocks(const pacuda_b200_plan *p) {
+    const int kernel = p->kernel;
+    const size_t cb = tiled_const_bytes(p->scales, p->factors);
+    auto fits = [&](int blocks) {
+        size_t room = tiled_max_smem(kernel, blocks);
+        return room > cb && tiled_max_points(p->point_bytes, tiled_threads(kernel, blocks), room - cb) > 0;
+    };
+    size_t room1 = tiled_max_smem(kernel, 1);
+    uint32_t one = room1 > cb ? tiled_default_points(p->point_bytes, tiled_threads(kernel, 1), room1 - cb) : 0;
+    int want = one && one <= 4 ? 4 : 2;
+    while (want > 1 && !fits(want)) want /= 2;
+    return want;
+}
+
 // The groups and the host block from the batch's current choices: each group's shared memory and
 // warps, each plan's points per block. The block is allocated again only when its size changes.
 bool prepare(pacuda_b200_batch *b) {
@@ -122,7 +140,7 @@ bool prepare(pacuda_b200_batch *b) {
     b->plan_blocks.resize(n, 0);
     b->groups.clear();
     for (size_t k = 0; k < n; k++) {
-        int blocks = b->plan_blocks[k] ? b->plan_blocks[k] : b->blocks;
+        int blocks = b->plan_blocks[k] ? b->plan_blocks[k] : b->blocks ? b->blocks : auto_blocks(b->plans[k]);
         size_t g = 0;
         while (g < b->groups.size() && b->groups[g].blocks != blocks) g++;
         if (g == b->groups.size()) {
@@ -532,7 +550,7 @@ extern "C" int pacuda_b200_batch_set_blocks_per_sm(pacuda_b200_batch *b, uint32_
     }
     int before = b->blocks;
     std::vector<int> before_plans = b->plan_blocks;
-    b->blocks = blocks ? (int)blocks : 1;
+    b->blocks = (int)blocks;
     std::fill(b->plan_blocks.begin(), b->plan_blocks.end(), 0);  // every plan the same
     if (!prepare(b)) {
         b->blocks = before;
@@ -566,7 +584,10 @@ extern "C" int pacuda_b200_batch_set_plan_blocks_per_sm(pacuda_b200_batch *b, ui
 
 extern "C" uint32_t pacuda_b200_batch_plan_blocks_per_sm(const pacuda_b200_batch *b, uint32_t plan) {
     if (!b || plan >= b->plan_blocks.size()) return 0;
-    return (uint32_t)(b->plan_blocks[plan] ? b->plan_blocks[plan] : b->blocks);
+    for (const LaunchGroup &g : b->groups)
+        for (uint32_t k : g.plans)
+            if (k == plan) return (uint32_t)g.blocks;
+    return 0;
 }
 
 extern "C" uint32_t pacuda_b200_batch_lanes_per_point(const pacuda_b200_batch *b, uint32_t plan) {

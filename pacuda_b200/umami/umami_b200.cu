@@ -416,9 +416,9 @@ UmamiStatus launch_chunk(Instance *in, int slot, const Chunk &ch, const double *
         batch = pacuda_b200_batch_create(plans.data(), (uint32_t)groups, ext_p.data(), points.data(), out_p.data());
         in->batch_plans[slot] = batch ? plans : std::vector<pacuda_b200_plan *>();
         if (!batch) return UMAMI_ERROR;
-        // two independent blocks per SM where the plans' points fit (one waits at a level's
-        // barrier while the other runs); else the batch keeps one
-        pacuda_b200_batch_set_blocks_per_sm(batch, 2);
+        // several independent blocks per SM, chosen per plan (one waits at a level's barrier while
+        // the others run); else the batch keeps one
+        pacuda_b200_batch_set_blocks_per_sm(batch, 0);
     }
     if (pacuda_b200_batch_run(batch, s) != PACMAN_RECURRENCE_OK) return UMAMI_ERROR;
     unsigned blocks = (unsigned)std::min<size_t>((ch.items + 255) / 256, 4096);

@@ -113,7 +113,7 @@ def test_plans_of_different_blocks_per_sm_run_as_launches_of_one_batch():
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("kind", ["f64", "mixed"])
-@pytest.mark.parametrize("blocks", [2, 4])
+@pytest.mark.parametrize("blocks", [0, 2, 4])
 def test_several_blocks_per_sm_give_the_same_bits(kind, blocks):
     """Independent blocks per SM (each with its share of the SM's shared memory and warps)."""
     from pacuda_b200 import batch as B
