@@ -114,22 +114,9 @@ Offsets layout(size_t n) {
     return o;
 }
 
-// Blocks per SM chosen without timing: four blocks (their points run on fewer, independent warps)
-// for a plan that fits at most four points in a block of all the warps, else two; fewer when the
-// points do not fit. (Measured on B200: gg>ggg, 4 points per 16 warps, gains 5 % at four blocks
-// over two; qg>qgg, 16 points, loses 14 % at four.)
+// blocks per SM chosen without timing (tiled_auto_blocks)
 int auto_blocks(const pacuda_b200_plan *p) {
-    const int kernel = p->kernel;
-    const size_t cb = tiled_const_bytes(p->scales, p->factors);
-    auto fits = [&](int blocks) {
-        size_t room = tiled_max_smem(kernel, blocks);
-        return room > cb && tiled_max_points(p->point_bytes, tiled_threads(kernel, blocks), room - cb) > 0;
-    };
-    size_t room1 = tiled_max_smem(kernel, 1);
-    uint32_t one = room1 > cb ? tiled_default_points(p->point_bytes, tiled_threads(kernel, 1), room1 - cb) : 0;
-    int want = one && one <= 4 ? 4 : 2;
-    while (want > 1 && !fits(want)) want /= 2;
-    return want;
+    return tiled_auto_blocks(p->kernel, p->point_bytes, tiled_const_bytes(p->scales, p->factors));
 }
 
 // The groups and the host block from the batch's current choices: each group's shared memory and

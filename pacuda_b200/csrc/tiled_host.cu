@@ -138,6 +138,18 @@ uint32_t tiled_max_points(size_t point_bytes, int threads, size_t max_smem) {
     return 0;
 }
 
+int tiled_auto_blocks(int kernel, size_t point_bytes, size_t const_bytes) {
+    auto most = [&](int blocks) {
+        size_t room = tiled_max_smem(kernel, blocks);
+        return room > const_bytes ? tiled_max_points(point_bytes, tiled_threads(kernel, blocks), room - const_bytes) : 0u;
+    };
+    size_t room1 = tiled_max_smem(kernel, 1);
+    uint32_t one = room1 > const_bytes ? tiled_default_points(point_bytes, tiled_threads(kernel, 1), room1 - const_bytes) : 0;
+    int want = one && one <= 4 ? 4 : 2;
+    while (want > 1 && !most(want)) want /= 2;
+    return want;
+}
+
 uint32_t tiled_default_points(size_t point_bytes, int threads, size_t max_smem) {
     uint32_t best = 0;
     for (uint32_t np = 1; np <= kMaxPoints; np++)

@@ -56,6 +56,12 @@ size_t tiled_max_smem(int kernel, int blocks = 1);
 bool tiled_points_fit(uint32_t points, size_t point_bytes, int threads, size_t max_smem);
 // the most points per block that fit, or 0
 uint32_t tiled_max_points(size_t point_bytes, int threads, size_t max_smem);
+// Blocks per SM chosen without timing for points of `point_bytes` and constants of `const_bytes`:
+// four (their points run on fewer, independent warps) when at most four points fit a block of all
+// the warps, else two; fewer when the points do not fit. (Measured on B200: gg>ggg, 4 points per
+// 16 warps, gains 5 % at four blocks over two; qg>qgg, 16 points, loses 14 % at four.)
+int tiled_auto_blocks(int kernel, size_t point_bytes, size_t const_bytes);
+
 // the default points per block: of those that fit, the count that leaves the fewest threads of a
 // warp without a lane (P * floor(32 / P) largest), the larger on ties; 0 when none fits
 uint32_t tiled_default_points(size_t point_bytes, int threads, size_t max_smem);
