@@ -447,7 +447,7 @@ def main():
     ap.add_argument("--no-tune", action="store_true", help="keep the default points per warp")
     ap.add_argument("--lanes-per-point", type=int, default=0)
     ap.add_argument("--no-precision", action="store_true", help="skip the mixed-precision lines")
-    ap.add_argument("--blocks-per-sm", type=int, default=0, help="1, 2 or 4 (with --no-tune or --lanes-per-point)")
+    ap.add_argument("--blocks-per-sm", type=int, default=0, help="1, 2, 3, 4, 5, 8 or 16 (with --no-tune or --lanes-per-point)")
     args = ap.parse_args()
     POINTS = args.points
     if args.family:

@@ -62,7 +62,8 @@ pacuda_b200_batch *pacuda_b200_batch_create(pacuda_b200_plan *const *plans, uint
  * copy of the launch descriptors, not for its kernel: the caller orders its use of the old arrays. */
 int pacuda_b200_batch_update(pacuda_b200_batch *batch, const double *const *external, const uint32_t *count,
                              double *const *output);
-/* Times each plan's lanes-per-point choices on its own points, with 1, 2 and 4 blocks per SM, and
+/* Times each plan's lanes-per-point choices on its own points, with 1, 2, 3, 4, 5, 8 and 16 blocks
+ * per SM (those its points fit), and
  * keeps each plan's fastest pair; plans of the same blocks per SM share one launch (a run is then
  * one launch per blocks-per-SM choice in use, one after the other on the stream). */
 int pacuda_b200_batch_tune(pacuda_b200_batch *batch, void *stream);
@@ -70,11 +71,12 @@ int pacuda_b200_batch_tune(pacuda_b200_batch *batch, void *stream);
 int pacuda_b200_batch_run(pacuda_b200_batch *batch, void *stream);
 /* Captures the launch into a CUDA graph on `stream`; later runs replay it. */
 int pacuda_b200_batch_capture(pacuda_b200_batch *batch, void *stream);
-/* Blocks per SM of every plan's launch: 1 (one block of all the warps the registers allow), 2 or 4
- * (independent blocks that share the SM's warps and shared memory: while one waits at a level's
- * barrier the others run); 0: chosen per plan without timing (four for a plan of at most four
- * points per 16-warp block, else two). Replaces the tuner's per-plan choices. INVALID when the
- * plans' points do not fit. A new batch has 1. */
+/* Blocks per SM of every plan's launch: 1 (one block of all the warps the registers allow), or 2, 3,
+ * 4, 5, 8 or 16 independent blocks of floor(warps / blocks) warps each that share the SM's warps and
+ * shared memory (while one waits at a level's barrier the others run); 0: chosen per plan without
+ * timing (five for a plan of at most four points per 16-warp block, else two). Replaces the tuner's
+ * per-plan choices. INVALID for another count or when the plans' points do not fit. A new batch
+ * has 1. */
 int pacuda_b200_batch_set_blocks_per_sm(pacuda_b200_batch *batch, uint32_t blocks);
 uint32_t pacuda_b200_batch_blocks_per_sm(const pacuda_b200_batch *batch);
 /* the blocks per SM plan k runs with (its own choice, else the batch's); setting 0 returns it to

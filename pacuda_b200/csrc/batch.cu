@@ -68,7 +68,7 @@ struct pacuda_b200_batch {
     std::vector<double *> output;
     std::vector<uint32_t> points;      // per plan: its points per block in this batch's launch
     std::vector<int> plan_blocks;      // per plan: its blocks per SM (0: the batch's)
-    int blocks = 1;                    // the batch's blocks per SM (tiled_host.h kMaxBlocks); 0: automatic
+    int blocks = 1;                    // the batch's blocks per SM (tiled_host.h kBlockChoices); 0: automatic
     // one launch per group; the descriptor block holds a section per group:
     // TiledPlan[n] | item_first[n + 1] | external[n] | output[n] | count[n] | counter
     std::vector<LaunchGroup> groups;
@@ -494,7 +494,7 @@ extern "C" int pacuda_b200_batch_tune(pacuda_b200_batch *b, void *stream) {
         float best = -1.0f;
         uint32_t best_points = p->points;
         int best_blocks = 0;
-        for (int blocks = 1; blocks <= kMaxBlocks; blocks *= 2) {
+        for (int blocks : kBlockChoices) {
             int threads = tiled_threads(kernel, blocks);
             size_t room = tiled_max_smem(kernel, blocks);
             uint32_t most = room > cb ? tiled_max_points(p->point_bytes, threads, room - cb) : 0;
@@ -527,7 +527,7 @@ extern "C" int pacuda_b200_batch_tune(pacuda_b200_batch *b, void *stream) {
 extern "C" uint32_t pacuda_b200_batch_launches(const pacuda_b200_batch *b) { return b ? (uint32_t)b->groups.size() : 0; }
 
 extern "C" int pacuda_b200_batch_set_blocks_per_sm(pacuda_b200_batch *b, uint32_t blocks) {
-    if (!b || blocks > (uint32_t)kMaxBlocks || blocks == 3) return PACMAN_RECURRENCE_INVALID;
+    if (!b || (blocks && !tiled_blocks_valid((int)blocks))) return PACMAN_RECURRENCE_INVALID;
     if (failed(cudaEventSynchronize(b->copied), "batch")) return PACMAN_RECURRENCE_DEVICE_ERROR;
     if (b->exec) {
         cudaGraphExecDestroy(b->exec);
@@ -551,7 +551,7 @@ extern "C" int pacuda_b200_batch_set_blocks_per_sm(pacuda_b200_batch *b, uint32_
 extern "C" uint32_t pacuda_b200_batch_blocks_per_sm(const pacuda_b200_batch *b) { return b ? (uint32_t)b->blocks : 0; }
 
 extern "C" int pacuda_b200_batch_set_plan_blocks_per_sm(pacuda_b200_batch *b, uint32_t plan, uint32_t blocks) {
-    if (!b || plan >= b->plans.size() || blocks > (uint32_t)kMaxBlocks || blocks == 3) return PACMAN_RECURRENCE_INVALID;
+    if (!b || plan >= b->plans.size() || (blocks && !tiled_blocks_valid((int)blocks))) return PACMAN_RECURRENCE_INVALID;
     if (failed(cudaEventSynchronize(b->copied), "batch")) return PACMAN_RECURRENCE_DEVICE_ERROR;
     if (b->exec) {
         cudaGraphExecDestroy(b->exec);

@@ -68,13 +68,19 @@ bool upload_schedule(TiledDevice &t, int threads, cudaStream_t s) {
     t.levels = (uint32_t)t.host.level_first.size() - 1;
     t.threads = threads;
     std::vector<uint32_t> ranges, firsts;
-    for (int b = 1; t.ok && b <= kMaxBlocks; b++)
-        for (uint32_t np = 1; np <= kMaxPoints; np++) {
+    // one order per distinct lane count: blocks of b per SM with P points give
+    // tiled_lanes(P, tiled_block_threads(threads, b)) lanes, and many pairs give the same count
+    std::vector<bool> made(kMaxLanes + 1, false);
+    for (int b : kBlockChoices)
+        for (uint32_t np = 1; t.ok && np <= kMaxPoints; np++) {
+            uint32_t lanes = tiled_lanes(np, tiled_block_threads(threads, b));
+            if (lanes == 0 || lanes > kMaxLanes || made[lanes]) continue;
+            made[lanes] = true;
             std::vector<uint32_t> order, lf;
-            lane_order(t.host, tiled_lanes(np, std::max(32, threads / b)), order, lf);
+            lane_order(t.host, lanes, order, lf);
             // each position holds its task's instruction range (first, end); (0, 0) for none
-            t.order_at[b - 1][np - 1] = ranges.size();
-            t.level_at[b - 1][np - 1] = firsts.size();
+            t.order_at[lanes] = ranges.size();
+            t.level_at[lanes] = firsts.size();
             for (uint32_t task : order) {
                 ranges.push_back(task == ~0u ? 0 : t.host.task_first[task]);
                 ranges.push_back(task == ~0u ? 0 : t.host.task_first[task + 1]);
@@ -109,7 +115,7 @@ int tiled_threads(int kernel, int blocks) {
     int warps = per_warp ? regs / per_warp : 16;
     warps = std::min(warps, attr.maxThreadsPerBlock / 32);
     warps = std::max(1, std::min(warps, 16));
-    return 32 * std::max(1, warps / std::max(1, blocks));
+    return tiled_block_threads(32 * warps, blocks);
 }
 
 size_t tiled_max_smem(int kernel, int blocks) {
@@ -145,9 +151,12 @@ int tiled_auto_blocks(int kernel, size_t point_bytes, size_t const_bytes) {
     };
     size_t room1 = tiled_max_smem(kernel, 1);
     uint32_t one = room1 > const_bytes ? tiled_default_points(point_bytes, tiled_threads(kernel, 1), room1 - const_bytes) : 0;
-    int want = one && one <= 4 ? 4 : 2;
-    while (want > 1 && !most(want)) want /= 2;
-    return want;
+    // the choices to try, most blocks first
+    static const int few[] = {5, 4, 2};
+    const int *first = one && one <= 4 ? few : few + 2;
+    for (const int *b = first; b != few + 3; b++)
+        if (most(*b)) return *b;
+    return 1;
 }
 
 uint32_t tiled_default_points(size_t point_bytes, int threads, size_t max_smem) {
@@ -161,15 +170,16 @@ uint32_t tiled_default_points(size_t point_bytes, int threads, size_t max_smem) 
 void describe(const TiledDevice &t, uint32_t forms, uint32_t points, size_t point_bytes, TiledPlan &p, int blocks) {
     p.ins = t.ins;
     p.task_first = t.task_first;
-    p.order = t.orders + t.order_at[blocks - 1][points - 1];
-    p.level_first = t.level_firsts + t.level_at[blocks - 1][points - 1];
+    const uint32_t lanes = tiled_lanes(points, tiled_block_threads(t.threads, blocks));
+    p.order = t.orders + t.order_at[lanes];
+    p.level_first = t.level_firsts + t.level_at[lanes];
     p.levels = t.levels;
     p.cur_slots = t.host.cur_slots;
     p.amp_slots = t.host.amp_slots;
     p.terms = t.host.terms;
     p.forms = forms;
     p.points = points;
-    p.lanes = tiled_lanes(points, std::max(32, t.threads / blocks));
+    p.lanes = lanes;
     p.point_bytes = (uint32_t)point_bytes;
     p.loads = t.loads;
     p.nloads = (uint32_t)t.host.loads.size() / 3;

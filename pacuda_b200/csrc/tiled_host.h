@@ -14,20 +14,33 @@ struct TiledLaunch;
 // points per block: 1 .. kMaxPoints; a point then has warps * floor(32 / P) lanes (a lane of all
 // P points is P adjacent threads of one warp)
 constexpr uint32_t kMaxPoints = 32;
-// blocks per SM: 1 (one block of all the warps the registers allow), 2 or 4 (independent blocks
-// that share them and reach their barriers at different times)
-constexpr int kMaxBlocks = 4;
+// blocks per SM: 1 (one block of all the warps the registers allow) or several independent blocks
+// that share those warps and reach their barriers at different times; a block of b per SM has
+// floor(warps / b) warps, so 3 and 5 leave one warp unused (16 warps: 5 x 3 = 15)
+constexpr int kBlockChoices[] = {1, 2, 3, 4, 5, 8, 16};
+inline bool tiled_blocks_valid(int blocks) {
+    for (int b : kBlockChoices)
+        if (b == blocks) return true;
+    return false;
+}
+// the threads of a block with `blocks` per SM when one block per SM has `threads`
+inline int tiled_block_threads(int threads, int blocks) {
+    int warps = threads / 32 / (blocks > 0 ? blocks : 1);
+    return 32 * (warps > 0 ? warps : 1);
+}
 inline uint32_t tiled_lanes(uint32_t points, int threads) { return (uint32_t)(threads / 32) * (32 / points); }
+// a point has at most 16 warps x 32 lanes
+constexpr uint32_t kMaxLanes = 512;
 
 struct TiledDevice {
     Schedule host;
     uint4 *ins = nullptr;  // the schedule's instructions, packed (pack_ins)
     uint32_t *task_first = nullptr, *loads = nullptr, *amp_planes = nullptr;
-    // per points-per-block count P: the lane order for threads / P lanes and its level
-    // boundaries, concatenated (offsets in 32-bit words, index P - 1)
+    // per lane count G (of every blocks-per-SM choice and points per block): the lane order for G
+    // lanes and its level boundaries, concatenated (offsets in 32-bit words, index G)
     uint32_t *orders = nullptr, *level_firsts = nullptr;
-    size_t order_at[kMaxBlocks][kMaxPoints] = {{0}}, level_at[kMaxBlocks][kMaxPoints] = {{0}};
-    int threads = 0;  // the threads of one block per SM (blocks of b per SM have threads / b)
+    size_t order_at[kMaxLanes + 1] = {0}, level_at[kMaxLanes + 1] = {0};
+    int threads = 0;  // the threads of one block per SM (tiled_block_threads for several)
     uint32_t levels = 0;
     bool ok = false;
     void release();
@@ -57,9 +70,10 @@ bool tiled_points_fit(uint32_t points, size_t point_bytes, int threads, size_t m
 // the most points per block that fit, or 0
 uint32_t tiled_max_points(size_t point_bytes, int threads, size_t max_smem);
 // Blocks per SM chosen without timing for points of `point_bytes` and constants of `const_bytes`:
-// four (their points run on fewer, independent warps) when at most four points fit a block of all
-// the warps, else two; fewer when the points do not fit. (Measured on B200: gg>ggg, 4 points per
-// 16 warps, gains 5 % at four blocks over two; qg>qgg, 16 points, loses 14 % at four.)
+// five (their points run on fewer, independent warps: 3 each) when at most four points fit a block
+// of all the warps, else two; fewer when the points do not fit. (Measured on B200: gg>ggg, 4 points
+// per 16 warps, gains 5 % at four blocks over two and 4 % more at five, whose 96 lanes per point
+// take its last level's 192 tasks in two full rounds; qg>qgg, 16 points, loses 14 % at four.)
 int tiled_auto_blocks(int kernel, size_t point_bytes, size_t const_bytes);
 
 // the default points per block: of those that fit, the count that leaves the fewest threads of a

@@ -130,6 +130,46 @@ def test_several_blocks_per_sm_give_the_same_bits(kind, blocks):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("kind", ["f64", "mixed"])
+@pytest.mark.parametrize("blocks", [3, 5, 8, 16])
+def test_blocks_of_fewer_warps_give_the_same_bits(kind, blocks):
+    """3 and 5 blocks per SM (5 and 3 warps each, one warp of 16 unused), 8 and 16 (2 warps and
+    1): every plan whose points fit such a block runs there, the others keep one block per SM;
+    the plans then run as two launches, each plan's bits unchanged."""
+    from pacuda_b200 import batch as B
+    import torch
+
+    plans, ext, out, want = setup(kind, [70, 33, 129, 5])
+    b = B.Batch(plans, ext, out)
+    moved = []
+    for k in range(len(plans)):
+        try:
+            b.set_plan_blocks_per_sm(k, blocks)
+            moved.append(k)
+        except B.RunnerError:
+            assert b.plan_blocks_per_sm(k) == 1
+    assert moved and all(b.plan_blocks_per_sm(k) == blocks for k in moved)
+    assert b.launches == (1 if len(moved) == len(plans) else 2)
+    b.run()
+    torch.cuda.synchronize()
+    check(out, want)
+
+
+@pytest.mark.gpu
+def test_other_block_counts_are_refused():
+    from pacuda_b200 import batch as B
+
+    plans, ext, out, _ = setup("f64", [7, 7, 7, 7])
+    b = B.Batch(plans, ext, out)
+    for blocks in (6, 7, 9, 17, 32):
+        with pytest.raises(B.RunnerError):
+            b.blocks_per_sm = blocks
+        with pytest.raises(B.RunnerError):
+            b.set_plan_blocks_per_sm(1, blocks)
+    assert b.blocks_per_sm == 1 and b.plan_blocks_per_sm(1) == 1
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", ["f64", "mixed"])
 def test_six_gluon_parts_match_oracle_bitwise(kind):
     """gg>gggg as its parts (subsets of the colour orderings), in one batch: each part's outputs
     equal the oracle's bit for bit (one point per block, 512 lanes, 5 levels)."""
