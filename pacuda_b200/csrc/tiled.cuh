@@ -101,7 +101,8 @@ struct AbiItem {
 };
 static __shared__ AbiItem abi_item;
 
-template <class K, bool ABI> struct SlotView {
+// ONE: a block of one point (P = 1, this thread's point 0), where a slot's index is its offset
+template <class K, bool ABI, bool ONE = false> struct SlotView {
     typedef typename K::R R;
     typedef typename K::Den Den;
     typedef typename K::Amp Amp;
@@ -113,7 +114,23 @@ template <class K, bool ABI> struct SlotView {
     const Den *mom;
     const Const *sre, *sim, *fre, *fim;  // the plan's constants, in shared memory
     uint32_t np, pw;      // the block's points (interleaved) and this thread's
-    __device__ __forceinline__ uint32_t at(uint32_t slot) const { return slot * np + pw; }
+    __device__ __forceinline__ uint32_t at(uint32_t slot) const { return ONE ? slot : slot * np + pw; }
+    // the same view with the one-point addressing (valid when np == 1)
+    __device__ __forceinline__ SlotView<K, ABI, true> one_point() const {
+        SlotView<K, ABI, true> o;
+        o.cur_ = cur_;
+        o.amp_ = amp_;
+        o.term_ = term_;
+        o.tw = tw;
+        o.mom = mom;
+        o.sre = sre;
+        o.sim = sim;
+        o.fre = fre;
+        o.fim = fim;
+        o.np = 1;
+        o.pw = 0;
+        return o;
+    }
     __device__ __forceinline__ Cx<R> cur(uint32_t slot) const {
         Pair<R> v = cur_[at(slot)];
         return cx(v.re, v.im);
@@ -159,6 +176,71 @@ template <class K, bool ABI> struct SlotView {
 };
 
 
+// the levels of one item: level 0's sources, then each level's tasks in the lane order, a block
+// barrier after each level (ONE views give one-point blocks their slots' offsets directly)
+template <class K, class V>
+__device__ __forceinline__ void run_levels(const V &v, const TiledPlan &p, double *forms64, uint32_t tl, bool active) {
+    typedef typename K::R R;
+    typedef typename K::Den Den;
+    const uint32_t lanes = p.lanes, levels = p.levels;
+    const uint4 *ins = p.ins;
+    const uint2 *order = reinterpret_cast<const uint2 *>(p.order);
+    for (uint32_t lv = 0; lv < levels; lv++) {
+        const uint32_t j0 = __ldg(p.level_first + lv), j1 = active ? __ldg(p.level_first + lv + 1) : 0;
+        if (lv == 0) {
+            for (uint32_t j = j0 + tl; j < j1; j += lanes) {
+                uint2 r = __ldg(order + j);
+                // sources: f64 wavefunctions from the f64 forms and constants, narrowed
+                for (uint32_t n = r.x; n < r.y; n++) {
+                    Ins o = unpack_ins(__ldg(ins + n));
+                    double mom[4];
+                    for (int c = 0; c < 4; c++) mom[c] = forms64[v.at(o.f * 4 + c)];
+                    double fr = __ldg(p.f64 + o.x), fi = __ldg(p.f64 + p.factors + o.x), mass = __ldg(p.s64 + o.s);
+                    W w[4];
+                    int m = source_values(o.y, mass, mom, w);
+                    Cx<R> vals[4];
+                    for (int c = 0; c < m; c++) {
+                        double sr = fr * w[c].re - fi * w[c].im, si = fr * w[c].im + fi * w[c].re;
+                        vals[c] = cx(narrow<R>(sr), narrow<R>(si));
+                        v.put(o.a + c, vals[c]);
+                    }
+                    if (ins_flags(o) & 8) v.writeback(o.c, vals, m);
+                }
+            }
+        } else {
+            // the next task's range is fetched while a task runs
+            uint32_t j = j0 + tl;
+            uint2 r = j < j1 ? __ldg(order + j) : make_uint2(0, 0);
+            while (j < j1) {
+                uint2 cur = r;
+                j += lanes;
+                if (j < j1) r = __ldg(order + j);
+                if (cur.x == cur.y) continue;
+                Cx<R> acc[6];
+#pragma unroll
+                for (int c = 0; c < 6; c++) acc[c] = cx(konst<R>(0.0), konst<R>(0.0));
+                // each next instruction is fetched while its predecessor runs
+                uint4 next = __ldg(ins + cur.x);
+                for (uint32_t n = cur.x; n < cur.y; n++) {
+                    const uint4 now = next;
+                    if (n + 1 < cur.y) next = __ldg(ins + n + 1);
+                    exec_row<K>(v, unpack_ins(now), acc);
+                }
+            }
+        }
+        __syncthreads();
+        if (lv == 0 && !is_f64<Den>::value) {
+            // the forms into df64 pairs, in place
+            if (active)
+                for (uint32_t q = tl; q < 4 * p.forms; q += lanes) {
+                    uint32_t at = v.at(q);
+                    reinterpret_cast<D *>(forms64)[at] = narrow<D>(forms64[at]);
+                }
+            __syncthreads();
+        }
+    }
+}
+
 // ABI: the C ABI's mode (arena in and out) or a batch's (outputs only)
 template <class K, bool ABI>
 __global__ void __launch_bounds__(512, 1) run_tiled(TiledLaunch L) {
@@ -177,7 +259,7 @@ __global__ void __launch_bounds__(512, 1) run_tiled(TiledLaunch L) {
         uint32_t k = 0;
         while (item >= L.item_first[k + 1]) k++;
         const TiledPlan &p = L.plans[k];
-        const uint32_t np = p.points, lanes = p.lanes, levels = p.levels;
+        const uint32_t np = p.points, lanes = p.lanes;
         if (ABI && threadIdx.x == 0) {
             abi_item.cre = L.cre;
             abi_item.cim = L.cim;
@@ -248,62 +330,11 @@ __global__ void __launch_bounds__(512, 1) run_tiled(TiledLaunch L) {
             }
         }
         __syncthreads();  // the constants, forms and live-in values are in
-        const uint4 *ins = p.ins;
-        const uint2 *order = reinterpret_cast<const uint2 *>(p.order);
-        for (uint32_t lv = 0; lv < levels; lv++) {
-            const uint32_t j0 = __ldg(p.level_first + lv), j1 = active ? __ldg(p.level_first + lv + 1) : 0;
-            if (lv == 0) {
-                for (uint32_t j = j0 + tl; j < j1; j += lanes) {
-                    uint2 r = __ldg(order + j);
-                    // sources: f64 wavefunctions from the f64 forms and constants, narrowed
-                    for (uint32_t n = r.x; n < r.y; n++) {
-                        Ins o = unpack_ins(__ldg(ins + n));
-                        double mom[4];
-                        for (int c = 0; c < 4; c++) mom[c] = forms64[(o.f * 4 + c) * np + pw];
-                        double fr = __ldg(p.f64 + o.x), fi = __ldg(p.f64 + p.factors + o.x), mass = __ldg(p.s64 + o.s);
-                        W w[4];
-                        int m = source_values(o.y, mass, mom, w);
-                        Cx<R> vals[4];
-                        for (int c = 0; c < m; c++) {
-                            double sr = fr * w[c].re - fi * w[c].im, si = fr * w[c].im + fi * w[c].re;
-                            vals[c] = cx(narrow<R>(sr), narrow<R>(si));
-                            v.put(o.a + c, vals[c]);
-                        }
-                        if (ins_flags(o) & 8) v.writeback(o.c, vals, m);
-                    }
-                }
-            } else {
-                // the next task's range is fetched while a task runs
-                uint32_t j = j0 + tl;
-                uint2 r = j < j1 ? __ldg(order + j) : make_uint2(0, 0);
-                while (j < j1) {
-                    uint2 cur = r;
-                    j += lanes;
-                    if (j < j1) r = __ldg(order + j);
-                    if (cur.x == cur.y) continue;
-                    Cx<R> acc[6];
-#pragma unroll
-                    for (int c = 0; c < 6; c++) acc[c] = cx(konst<R>(0.0), konst<R>(0.0));
-                    // each next instruction is fetched while its predecessor runs
-                    uint4 next = __ldg(ins + cur.x);
-                    for (uint32_t n = cur.x; n < cur.y; n++) {
-                        const uint4 now = next;
-                        if (n + 1 < cur.y) next = __ldg(ins + n + 1);
-                        exec_row<K>(v, unpack_ins(now), acc);
-                    }
-                }
-            }
-            __syncthreads();
-            if (lv == 0 && !is_f64<Den>::value) {
-                // the forms into df64 pairs, in place
-                if (active)
-                    for (uint32_t q = tl; q < 4 * p.forms; q += lanes) {
-                        uint32_t at = q * np + pw;
-                        reinterpret_cast<D *>(forms64)[at] = narrow<D>(forms64[at]);
-                    }
-                __syncthreads();
-            }
-        }
+        // (batches only: in the C ABI's kernel the second copy of the levels costs registers)
+        if (!ABI && np == 1)
+            run_levels<K>(v.one_point(), p, forms64, tl, active);
+        else
+            run_levels<K>(v, p, forms64, tl, active);
         if (ABI) {
             // (the point again from the item: nothing of it stays in registers through the levels)
             const unsigned long long at = abi_item.first + pw;
