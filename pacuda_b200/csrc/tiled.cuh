@@ -101,8 +101,9 @@ struct AbiItem {
 };
 static __shared__ AbiItem abi_item;
 
-// ONE: a block of one point (P = 1, this thread's point 0), where a slot's index is its offset
-template <class K, bool ABI, bool ONE = false> struct SlotView {
+// NP: the block's points when known at compile time (0: np at run time); with NP a slot's
+// address is a shift of its index and its components' addresses constant offsets from it
+template <class K, bool ABI, int NP = 0> struct SlotView {
     typedef typename K::R R;
     typedef typename K::Den Den;
     typedef typename K::Amp Amp;
@@ -114,10 +115,10 @@ template <class K, bool ABI, bool ONE = false> struct SlotView {
     const Den *mom;
     const Const *sre, *sim, *fre, *fim;  // the plan's constants, in shared memory
     uint32_t np, pw;      // the block's points (interleaved) and this thread's
-    __device__ __forceinline__ uint32_t at(uint32_t slot) const { return ONE ? slot : slot * np + pw; }
-    // the same view with the one-point addressing (valid when np == 1)
-    __device__ __forceinline__ SlotView<K, ABI, true> one_point() const {
-        SlotView<K, ABI, true> o;
+    __device__ __forceinline__ uint32_t at(uint32_t slot) const { return NP ? slot * NP + pw : slot * np + pw; }
+    // the same view with the addressing of N points per block (valid when np == N)
+    template <int N> __device__ __forceinline__ SlotView<K, ABI, N> with_points() const {
+        SlotView<K, ABI, N> o;
         o.cur_ = cur_;
         o.amp_ = amp_;
         o.term_ = term_;
@@ -127,8 +128,8 @@ template <class K, bool ABI, bool ONE = false> struct SlotView {
         o.sim = sim;
         o.fre = fre;
         o.fim = fim;
-        o.np = 1;
-        o.pw = 0;
+        o.np = N;
+        o.pw = pw;
         return o;
     }
     __device__ __forceinline__ Cx<R> cur(uint32_t slot) const {
@@ -177,7 +178,7 @@ template <class K, bool ABI, bool ONE = false> struct SlotView {
 
 
 // the levels of one item: level 0's sources, then each level's tasks in the lane order, a block
-// barrier after each level (ONE views give one-point blocks their slots' offsets directly)
+// barrier after each level (views of a compile-time point count address slots without products)
 template <class K, class V>
 __device__ __forceinline__ void run_levels(const V &v, const TiledPlan &p, double *forms64, uint32_t tl, bool active) {
     typedef typename K::R R;
@@ -330,9 +331,13 @@ __global__ void __launch_bounds__(512, 1) run_tiled(TiledLaunch L) {
             }
         }
         __syncthreads();  // the constants, forms and live-in values are in
-        // (batches only: in the C ABI's kernel the second copy of the levels costs registers)
+        // batches of one point per block (six-leg plans, gg>ggg) and of eight (the 5-leg quark
+        // plans at two blocks per SM) run a copy of the levels with that count built in; in the C
+        // ABI's kernel more copies of the levels cost registers
         if (!ABI && np == 1)
-            run_levels<K>(v.one_point(), p, forms64, tl, active);
+            run_levels<K>(v.template with_points<1>(), p, forms64, tl, active);
+        else if (!ABI && np == 8)
+            run_levels<K>(v.template with_points<8>(), p, forms64, tl, active);
         else
             run_levels<K>(v, p, forms64, tl, active);
         if (ABI) {
