@@ -86,12 +86,15 @@ __device__ __forceinline__ void exec_contribution(const V &v, const Ins &o, Cx<t
         }
     }
     contribution<OP>(l, r, q0, q1, val);
+    if (!(flags & F_FIRST)) {
 #pragma unroll
-    for (int k = 0; k < cd; k++) {
-        Cx<R> c = val[k] * scale;
-        if (!(flags & F_FIRST)) acc[k] = acc[k] + c;
-        else if (flags & F_INIT) acc[k] = c;
-        else acc[k] = v.cur(o.c + k) + c;
+        for (int k = 0; k < cd; k++) acc[k] = acc[k] + val[k] * scale;
+    } else if (flags & F_INIT) {
+#pragma unroll
+        for (int k = 0; k < cd; k++) acc[k] = val[k] * scale;
+    } else {
+#pragma unroll
+        for (int k = 0; k < cd; k++) acc[k] = v.cur(o.c + k) + val[k] * scale;
     }
     if (flags & F_LAST) {
         if (!(flags & 32))  // else the sums stay in registers for the task's closures
@@ -183,25 +186,20 @@ __device__ __forceinline__ void exec_clear(const V &v, const Ins &o) {
 // one row of any kind but a source, its sum kept in `acc` across a destination's run
 template <class K, class V>
 __device__ __forceinline__ void exec_row(const V &v, const Ins &o, Cx<typename K::R> *acc) {
-    uint32_t kind = ins_kind(o), op = ins_op(o);
-    if (kind == K_CONTRIB) {
-        switch (op) {
-        case 2: exec_contribution<K, 2>(v, o, acc); break;
-        case 3: exec_contribution<K, 3>(v, o, acc); break;
-        case 4: exec_contribution<K, 4>(v, o, acc); break;
-        case 5: exec_contribution<K, 5>(v, o, acc); break;
-        default: exec_contribution<K, 6>(v, o, acc); break;
-        }
-    } else if (kind == K_PROP) {
-        if (op == 7) exec_propagator<K, 7>(v, o);
-        else if (op == 8) exec_propagator<K, 8>(v, o);
-        else exec_propagator<K, 9>(v, o);
-    } else if (kind == K_CLOSURE) {
-        exec_closure<K>(v, o, acc);
-    } else if (kind == K_IDENTITY) {
-        exec_identity<K>(v, o);
-    } else if (kind == K_CLEAR) {
-        exec_clear<K>(v, o);
+    // one jump on kind | op << 4 (the program holds no other pairs)
+    switch (o.head & 0xff) {
+    case K_CONTRIB | 2 << 4: exec_contribution<K, 2>(v, o, acc); break;
+    case K_CONTRIB | 3 << 4: exec_contribution<K, 3>(v, o, acc); break;
+    case K_CONTRIB | 4 << 4: exec_contribution<K, 4>(v, o, acc); break;
+    case K_CONTRIB | 5 << 4: exec_contribution<K, 5>(v, o, acc); break;
+    case K_CONTRIB | 6 << 4: exec_contribution<K, 6>(v, o, acc); break;
+    case K_PROP | 7 << 4: exec_propagator<K, 7>(v, o); break;
+    case K_PROP | 8 << 4: exec_propagator<K, 8>(v, o); break;
+    case K_PROP | 9 << 4: exec_propagator<K, 9>(v, o); break;
+    case K_CLOSURE | 11 << 4: exec_closure<K>(v, o, acc); break;
+    case K_IDENTITY | 10 << 4: exec_identity<K>(v, o); break;
+    case K_CLEAR | 1 << 4: exec_clear<K>(v, o); break;
+    default: break;
     }
 }
 

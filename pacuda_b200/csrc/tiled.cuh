@@ -210,12 +210,14 @@ __device__ __forceinline__ void run_levels(const V &v, const TiledPlan &p, doubl
             }
         } else {
             // the next task's range is fetched while a task runs
+            // (the order arrays end with a lane count's worth of padding and the instructions
+            // with one padding instruction, so these fetches need no bounds test)
             uint32_t j = j0 + tl;
             uint2 r = j < j1 ? __ldg(order + j) : make_uint2(0, 0);
             while (j < j1) {
                 uint2 cur = r;
                 j += lanes;
-                if (j < j1) r = __ldg(order + j);
+                r = __ldg(order + j);
                 if (cur.x == cur.y) continue;
                 Cx<R> acc[6];
 #pragma unroll
@@ -224,7 +226,7 @@ __device__ __forceinline__ void run_levels(const V &v, const TiledPlan &p, doubl
                 uint4 next = __ldg(ins + cur.x);
                 for (uint32_t n = cur.x; n < cur.y; n++) {
                     const uint4 now = next;
-                    if (n + 1 < cur.y) next = __ldg(ins + n + 1);
+                    next = __ldg(ins + n + 1);
                     exec_row<K>(v, unpack_ins(now), acc);
                 }
             }

@@ -63,6 +63,7 @@ bool upload_schedule(TiledDevice &t, int threads, cudaStream_t s) {
             t.ok = false;
             return false;
         }
+    packed.push_back(make_uint4(0, 0, 0, 0));  // read (not run) by the prefetch after a task's last row
     t.ok = threads > 0 && put(&t.ins, packed, s) && put(&t.task_first, t.host.task_first, s) &&
            put(&t.loads, t.host.loads, s) && put(&t.amp_planes, t.host.amp_planes, s);
     t.levels = (uint32_t)t.host.level_first.size() - 1;
@@ -87,6 +88,9 @@ bool upload_schedule(TiledDevice &t, int threads, cudaStream_t s) {
             }
             firsts.insert(firsts.end(), lf.begin(), lf.end());
         }
+    // the executor fetches the next position of a lane before testing it against the level's end:
+    // up to a lane count past the last one
+    ranges.insert(ranges.end(), 2 * kMaxLanes, 0);
     t.ok = t.ok && put(&t.orders, ranges, s) && put(&t.level_firsts, firsts, s);
     // the host vectors must outlive the asynchronous copies
     cudaStreamSynchronize(s);
