@@ -83,6 +83,9 @@ __device__ __forceinline__ Ins unpack_ins(uint4 w) {
     return o;
 }
 
+// a hint: the line holding `p` into L1 (no register waits for it)
+__device__ __forceinline__ void prefetch_l1(const void *p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
+
 // a complex value as shared memory holds it: (re, im) side by side, one 8- or 16-byte access
 template <class R> struct alignas(2 * sizeof(R)) Pair {
     R re, im;
@@ -115,6 +118,7 @@ template <class K, bool ABI, int NP = 0> struct SlotView {
     const Den *mom;
     const Const *sre, *sim, *fre, *fim;  // the plan's constants, in shared memory
     uint32_t np, pw;      // the block's points (interleaved) and this thread's
+    static constexpr int kPoints = NP;
     __device__ __forceinline__ uint32_t at(uint32_t slot) const { return NP ? slot * NP + pw : slot * np + pw; }
     // the same view with the addressing of N points per block (valid when np == N)
     template <int N> __device__ __forceinline__ SlotView<K, ABI, N> with_points() const {
@@ -211,7 +215,11 @@ __device__ __forceinline__ void run_levels(const V &v, const TiledPlan &p, doubl
         } else {
             // the next task's range is fetched while a task runs
             // (the order arrays end with a lane count's worth of padding and the instructions
-            // with one padding instruction, so these fetches need no bounds test)
+            // with one padding instruction, so these fetches need no bounds test). In blocks of one
+            // point every lane fetches its own instructions, and five blocks' shared memory leaves
+            // L1 little room for them: once a task's first row has run, the next task's range has
+            // arrived, and that task's first and last instruction lines are prefetched into L1
+            // while the rest of this one runs.
             uint32_t j = j0 + tl;
             uint2 r = j < j1 ? __ldg(order + j) : make_uint2(0, 0);
             while (j < j1) {
@@ -228,6 +236,10 @@ __device__ __forceinline__ void run_levels(const V &v, const TiledPlan &p, doubl
                     const uint4 now = next;
                     next = __ldg(ins + n + 1);
                     exec_row<K>(v, unpack_ins(now), acc);
+                    if (V::kPoints == 1 && n == cur.x) {
+                        prefetch_l1(ins + r.x);
+                        prefetch_l1(ins + (r.y > r.x ? r.y - 1 : r.x));
+                    }
                 }
             }
         }
