@@ -65,26 +65,50 @@ def workload(rank=0):
 
 
 class Clocks:
-    """nvidia-smi samples (every 200 ms) during the timed region."""
+    """nvidia-smi samples (every 50 ms) during the timed region: the sampler starts before it and
+    has written its first sample when `mark()` is called at the region's start; `stop()` at its
+    end keeps only the samples written in between (at least the first one after the mark)."""
 
     def __init__(self, index=0):
         self.path = f"/tmp/bench_clocks_{os.getpid()}.csv"
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
              "clocks_event_reasons.sw_power_cap")
+        self.first = 0
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "200",
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "50",
                                           "-i", str(index)], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
+        t0 = time.time()
+        while self.proc and self.proc.poll() is None and self._lines() == 0 and time.time() - t0 < 10:
+            time.sleep(0.02)
+
+    def _lines(self):
+        try:
+            with open(self.path) as f:
+                return sum(1 for line in f if line.endswith("\n"))
+        except OSError:
+            return 0
+
+    def mark(self):
+        self.first = self._lines()
 
     def stop(self):
         if not self.proc:
             return None
+        last = self._lines()
+        if last <= self.first:  # a region shorter than the sampling interval: the next sample
+            t0 = time.time()
+            while self.proc.poll() is None and self._lines() <= self.first and time.time() - t0 < 1:
+                time.sleep(0.01)
+            last = self.first + 1
         self.proc.terminate()
         self.proc.wait()
         sm, mx, reasons = [], 0.0, set()
-        for line in open(self.path):
+        with open(self.path) as f:
+            lines = [line for line in f if line.endswith("\n")][self.first:last]
+        for line in lines:
             f = [x.strip() for x in line.split(",")]
             if len(f) < 9:
                 continue
@@ -220,7 +244,37 @@ def six_gluon_line(torch, B, points=1 << 20, steps=3, warmup=2):
         "median": float(np.median(rel)), "q999": float(np.quantile(rel, 0.999)), "max": float(rel.max()),
         "frac_le_1e-10": float((rel <= 1e-10).mean()),
         "histogram": {"edges_log10": list(range(-16, 1)), "counts": [int(c) for c in hist]}}
+    res["stability"] = stability_line(torch, parts, ext, totals["f64"], points, steps, warmup)
     return res
+
+
+def stability_line(torch, templates, ext, want, points, steps, warmup, tols=(1e-10, 1e-6)):
+    """The mixed kernel with the rotated-momentum stability check (pacuda_b200/stability.py):
+    per tolerance, the whole pipeline's points/s (two mixed evaluations, the check, the f64
+    evaluation of the points that fail it), the fraction of points sent back to f64, and the
+    relative error of the result's |M|^2 against f64."""
+    from pacuda_b200 import stability
+
+    lines = []
+    for tol in tols:
+        s = stability.StableMixed(templates, points, tol)
+        for _ in range(warmup):
+            s.run(ext)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            outs, m = s.run(ext)
+        e1.record()
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        total = sum(o.view(points, t.outputs).sum(dim=1) for o, t in zip(outs, templates))
+        rel = ((total - want).abs() / want.abs().clamp_min(1e-300)).cpu().numpy()
+        lines.append({"tol": tol, "value": points / (ms * 1e-3), "unit": "points/s", "ms_per_step": ms,
+                      "fraction_to_f64": m / points,
+                      "rel_error_vs_f64": {"median": float(np.median(rel)), "q999": float(np.quantile(rel, 0.999)),
+                                           "max": float(rel.max()), "frac_le_1e-10": float((rel <= 1e-10).mean())}})
+        del s, outs
+    return lines
 
 
 def pp4j_line(torch, B, points=1 << 22, steps=3, warmup=2):
@@ -437,7 +491,7 @@ def main():
     global POINTS, FAMILIES
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=60)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
@@ -466,7 +520,7 @@ def main():
             return
         fams = workload(0)
         for _ in range(max(0, args.warmup)):
-            pass
+            cpu_baseline(fams, sample=512)
         vals = []
         for _ in range(args.steps):
             vals.append(cpu_baseline(fams, sample=512)["value"])
@@ -515,11 +569,13 @@ def main():
         batch.capture(stream)
     for _ in range(args.warmup):
         batch.run(stream)
+    clocks = Clocks(int(os.environ.get("LOCAL_RANK", 0))) if rank == 0 else None
     stream.synchronize()
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
-    clocks = Clocks(int(os.environ.get("LOCAL_RANK", 0))) if rank == 0 else None
+    if clocks:
+        clocks.mark()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(args.steps):

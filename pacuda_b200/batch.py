@@ -39,6 +39,7 @@ def lib(path=None):
         L.pacuda_b200_batch_plan_blocks_per_sm.argtypes = [C.c_void_p, C.c_uint32]
         L.pacuda_b200_batch_set_plan_blocks_per_sm.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32]
         L.pacuda_b200_batch_plan_blocks_per_sm.restype = C.c_uint32
+        L.pacuda_b200_batch_update.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.pacuda_b200_batch_destroy.argtypes = [C.c_void_p]
     return _lib
 
@@ -97,6 +98,24 @@ class Batch:
         self.handle = lib().pacuda_b200_batch_create(handles, n, ext, cnt, out)
         if not self.handle:
             raise RunnerError("pacuda_b200_batch_create failed")
+
+    def update(self, external, counts, output):
+        """Points the plans at other momenta, point counts and outputs (pacuda_b200_batch_update:
+        no allocation; a captured graph is dropped)."""
+        import torch
+
+        n = len(self.plans)
+        external, output, counts = list(external), list(output), [int(c) for c in counts]
+        assert len(external) == len(output) == len(counts) == n
+        for p, e, o, c in zip(self.plans, external, output, counts):
+            assert e.dtype == torch.float64 and e.is_cuda and e.numel() >= 4 * p.template.external_count * c
+            assert o.dtype == torch.float64 and o.is_cuda and o.numel() >= c * p.template.outputs
+        ext = (C.c_void_p * n)(*[e.data_ptr() for e in external])
+        out = (C.c_void_p * n)(*[o.data_ptr() for o in output])
+        cnt = (C.c_uint32 * n)(*counts)
+        if lib().pacuda_b200_batch_update(self.handle, ext, cnt, out) != 0:
+            raise RunnerError("batch update failed")
+        self.external, self.output, self.counts = external, output, counts
 
     def _stream(self, stream):
         import torch
