@@ -113,6 +113,25 @@ def test_statuses(umami):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("first", ["random", "sampling"])
+def test_the_first_failing_event_decides_the_status(umami, first):
+    """Events checked in parallel ranges: of two failing events in different ranges, the earlier
+    one's status is the call's, as one pass in event order gives it (a random number outside
+    [0, 1): 1; sampling over two contributions: 3)."""
+    count = stride = 100000
+    m, p, channel, flavour = U.events(count, stride, 0, seed=5, single=True)
+    random = np.random.default_rng(3).random(stride)
+    me, hel = np.zeros(stride), np.zeros(stride, np.int32)
+    early, late = 20000, 80000
+    bad_random, two = (early, late) if first == "random" else (late, early)
+    random[bad_random] = 1.0
+    channel[two], flavour[two] = 1, 2
+    status = call(umami, [(0, m), (2, flavour), (8, channel), (4, random)], [(0, me), (3, hel)], count=count,
+                  stride=stride, offset=0)
+    assert status == (1 if first == "random" else 3)
+
+
+@pytest.mark.gpu
 def test_parameters(umami):
     from oracle import oracle as O
 
@@ -137,12 +156,15 @@ def test_parameters(umami):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("mode", ["sum", "sample"])
-def test_a_call_of_several_chunks(umami, mode):
-    """A call of more than 2^17 events is evaluated in chunks whose host and device work overlap."""
+@pytest.mark.parametrize("mode,count", [("sum", 3 * 65536 + 123), ("sample", 3 * 65536 + 123),
+                                        ("sum", 6 * 65536 + 5)])
+def test_a_call_of_several_chunks(umami, mode, count):
+    """A call of more than 2^17 events is evaluated in chunks whose host and device work overlap
+    (three equal chunks, or the six of a full call), each chunk's host passes over parallel event
+    ranges."""
     from oracle import oracle as O
 
-    count, stride, offset = 3 * 65536 + 123, 3 * 65536 + 200, 11
+    stride, offset = count + 77, 11
     m, p, channel, flavour = U.events(count, stride, offset, seed=23, single=mode == "sample")
     random = np.random.default_rng(9).random(stride)
     me, hel = np.full(stride, -1.0), np.full(stride, -1, np.int32)
