@@ -115,9 +115,9 @@ def test_statuses(umami):
 @pytest.mark.gpu
 @pytest.mark.parametrize("first", ["random", "sampling"])
 def test_the_first_failing_event_decides_the_status(umami, first):
-    """Events checked in parallel ranges: of two failing events in different ranges, the earlier
-    one's status is the call's, as one pass in event order gives it (a random number outside
-    [0, 1): 1; sampling over two contributions: 3)."""
+    """Of two failing events far apart in one chunk, the earlier one's status is the call's, as
+    the reference's checks in event order give it (a random number outside [0, 1): 1; sampling
+    over two contributions: 3)."""
     count = stride = 100000
     m, p, channel, flavour = U.events(count, stride, 0, seed=5, single=True)
     random = np.random.default_rng(3).random(stride)
@@ -160,8 +160,7 @@ def test_parameters(umami):
                                         ("sum", 6 * 65536 + 5)])
 def test_a_call_of_several_chunks(umami, mode, count):
     """A call of more than 2^17 events is evaluated in chunks whose host and device work overlap
-    (three equal chunks, or the six of a full call), each chunk's host passes over parallel event
-    ranges."""
+    (three equal chunks, or the five growing chunks of a full call)."""
     from oracle import oracle as O
 
     stride, offset = count + 77, 11
