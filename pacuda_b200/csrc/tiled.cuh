@@ -11,7 +11,9 @@
 // ([slot][P], interleaved) are contiguous, and their global stores cover P consecutive points of
 // a plane. All points take the same lane order, so a block's points move through the levels
 // together and meet at the block's barrier. A block takes one work item at a time: one plan's
-// next P points.
+// next P points. An SM runs 1 to 16 such blocks (each with its share of the warps and shared
+// memory), which reach their barriers at different times; batch blocks of 1 and 8 points run a
+// copy of the levels with that count built in (run_levels over SlotView<K, ABI, NP>).
 #pragma once
 #include <stdint.h>
 

@@ -11,13 +11,16 @@
 //      n * k + leg for component k of a leg, one value per event), and each item's inputs;
 //   3. gathers every group's external momenta on the device (the permutation and the process's
 //      crossing applied: external leg l = sign_l x input leg permutation[crossing_l]);
-//   4. evaluates every group in ONE persistent launch of the batched executor, each point's
-//      helicity values reduced in the kernel from its amplitudes (pacuda_b200_batch_*);
+//   4. evaluates every group in one run of the batched executor (a persistent launch per
+//      blocks-per-SM choice), each point's helicity values reduced in the kernel from its
+//      amplitudes (pacuda_b200_batch_*);
 //   5. finishes each item on the device (the process-group factor, the alpha_s scale, then the
 //      helicity sum, a fixed helicity's value, or the helicity drawn in proportion to its value,
 //      with the reference's arithmetic in its order: recurrence_runner.cu:1532-1572) and copies
 //      back one value per item (and the draw);
 //   6. combines each event's contributions on the host as the reference does.
+// Steps 1-5 run per chunk of events (kChunkParts), the host's steps for the next chunk while the
+// device runs the previous one.
 // The values equal the reference library's bit for bit: the same f64 arithmetic in the same
 // order, from the same resolved reduction.
 //
