@@ -74,7 +74,7 @@ int pacuda_b200_batch_capture(pacuda_b200_batch *batch, void *stream);
 /* Blocks per SM of every plan's launch: 1 (one block of all the warps the registers allow), or 2, 3,
  * 4, 5, 8 or 16 independent blocks of floor(warps / blocks) warps each that share the SM's warps and
  * shared memory (while one waits at a level's barrier the others run); 0: chosen per plan without
- * timing (five for a plan of at most four points per 16-warp block, else two). Replaces the tuner's
+ * timing (four for a plan of at most four points per 16-warp block, else two). Replaces the tuner's
  * per-plan choices. INVALID for another count or when the plans' points do not fit. A new batch
  * has 1. */
 int pacuda_b200_batch_set_blocks_per_sm(pacuda_b200_batch *batch, uint32_t blocks);

@@ -364,6 +364,22 @@ bool build_schedule(const Program &p, uint32_t P, uint32_t A, Schedule &out) {
             }
         }
     };
+    // Spread placement. A block of one point reads one slot per lane, 16 bytes at a time; eight
+    // lanes share a shared-memory wavefront over eight 16-byte bank groups, and values packed at
+    // slots 4m (the 4-component currents) fall into two of them. So, when no group is wider than
+    // kWindow slots, no group crosses a multiple of kWindow (a group that would starts at the next
+    // one), and each window of kWindow slots is followed by one unused slot: window w starts at
+    // 13w, so the windows' values start in all eight bank groups. (12 = 4 x 3 = 6 x 2 packs the
+    // 4- and 6-slot values of the gluon plans without loss; 8 % more slots.)
+    constexpr uint32_t kWindow = 12;
+    uint32_t widest = 0;
+    for (uint32_t g = 0; g < G; g++)
+        if (!in_register[g]) widest = std::max(widest, gsize[g]);
+    const bool spread = widest <= kWindow;
+    // the first start at or after s where z slots cross no multiple of kWindow
+    auto start_at = [&](uint32_t s, uint32_t z) -> uint32_t {
+        return !spread || z == 0 || s / kWindow == (s + z - 1) / kWindow ? s : (s + kWindow - 1) / kWindow * kWindow;
+    };
     for (uint32_t g : order) {
         if (in_register[g]) continue;  // kept in a task's registers
         // a slot is reused only after the last level that touches its previous occupant
@@ -371,21 +387,32 @@ bool build_schedule(const Program &p, uint32_t P, uint32_t A, Schedule &out) {
             release(active.begin()->second.first, active.begin()->second.second);
             active.erase(active.begin());
         }
+        const uint32_t z = gsize[g];
         uint32_t slot = ~0u;
-        for (auto it = free.begin(); it != free.end(); ++it)
-            if (it->second >= gsize[g]) {
-                slot = it->first;
-                uint32_t rest = it->second - gsize[g];
+        for (auto it = free.begin(); it != free.end(); ++it) {
+            const uint32_t s = it->first, size = it->second, a = start_at(s, z);
+            if (a + z <= s + size) {
                 free.erase(it);
-                if (rest) free.emplace(slot + gsize[g], rest);
+                if (a > s) free.emplace(s, a - s);
+                if (a + z < s + size) free.emplace(a + z, s + size - a - z);
+                slot = a;
                 break;
             }
+        }
         if (slot == ~0u) {
-            slot = top;
-            top += gsize[g];
+            const uint32_t a = start_at(top, z);
+            if (a > top) release(top, a - top);
+            slot = a;
+            top = a + z;
         }
         gslot[g] = slot;
-        active.emplace(glast[g], std::make_pair(slot, gsize[g]));
+        active.emplace(glast[g], std::make_pair(slot, z));
+    }
+    if (spread) {
+        auto place = [](uint32_t s) { return (kWindow + 1) * (s / kWindow) + s % kWindow; };
+        for (uint32_t g = 0; g < G; g++)
+            if (!in_register[g]) gslot[g] = place(gslot[g]);
+        top = top ? place(top - 1) + 1 : 0;
     }
     out.cur_slots = top;
     {

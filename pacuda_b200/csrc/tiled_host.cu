@@ -156,9 +156,9 @@ int tiled_auto_blocks(int kernel, size_t point_bytes, size_t const_bytes) {
     size_t room1 = tiled_max_smem(kernel, 1);
     uint32_t one = room1 > const_bytes ? tiled_default_points(point_bytes, tiled_threads(kernel, 1), room1 - const_bytes) : 0;
     // the choices to try, most blocks first
-    static const int few[] = {5, 4, 2};
-    const int *first = one && one <= 4 ? few : few + 2;
-    for (const int *b = first; b != few + 3; b++)
+    static const int few[] = {4, 2};
+    const int *first = one && one <= 4 ? few : few + 1;
+    for (const int *b = first; b != few + 2; b++)
         if (most(*b)) return *b;
     return 1;
 }

@@ -70,10 +70,11 @@ bool tiled_points_fit(uint32_t points, size_t point_bytes, int threads, size_t m
 // the most points per block that fit, or 0
 uint32_t tiled_max_points(size_t point_bytes, int threads, size_t max_smem);
 // Blocks per SM chosen without timing for points of `point_bytes` and constants of `const_bytes`:
-// five (their points run on fewer, independent warps: 3 each) when at most four points fit a block
-// of all the warps, else two; fewer when the points do not fit. (Measured on B200: gg>ggg, 4 points
-// per 16 warps, gains 5 % at four blocks over two and 4 % more at five, whose 96 lanes per point
-// take its last level's 192 tasks in two full rounds; qg>qgg, 16 points, loses 14 % at four.)
+// four (their points run on fewer, independent warps: 4 each) when at most four points fit a
+// block of all the warps, else two; fewer when the points do not fit. (Measured on B200: gg>ggg,
+// 4 points per 16 warps, gains 5 % at four blocks over two; five blocks' shared memory leaves L1
+// too little room for its instruction stream since the spread slot layout; qg>qgg, 16 points,
+// loses 14 % at four.)
 int tiled_auto_blocks(int kernel, size_t point_bytes, size_t const_bytes);
 
 // the default points per block: of those that fit, the count that leaves the fewest threads of a
