@@ -64,3 +64,28 @@ def test_six_gluon_part_plan():
     t = processes.parts("gg>gggg")[0]
     check(t.words, t.width, t.current_planes, t.amplitude_planes, t.momentum_planes // 4, len(t.scale_re),
           len(t.factor_re))
+
+
+@pytest.mark.parametrize("name", ["gg>ggg", "qg>qgg"])
+def test_spread_slots(name):
+    """The spread slot placement: every operand's slots lie in one window of 12 slots (the
+    13th of each 13 is never used), and the 4-slot currents start in all eight 16-byte bank
+    groups (slot mod 8)."""
+    t = processes.template(name)
+    args = (t.words, t.width, t.current_planes, t.amplitude_planes, t.momentum_planes // 4, len(t.scale_re),
+            len(t.factor_re))
+    applied, ins, tf, lf, terms, slots = E.export_terms(*args, t.offsets, t.planes)
+    shape = {2: (2, 4, 2), 3: (2, 4, 2), 4: (6, 4, 4), 5: (4, 4, 6), 6: (4, 4, 4)}
+    starts = set()
+    for row in ins:
+        kind, op = int(row[0]) & 15, (int(row[0]) >> 4) & 15
+        a, b, c = int(row[1]), int(row[2]), int(row[3])
+        if kind != 1:
+            continue
+        c0, c1, cd = shape[op]
+        for base, n in ((a, c0), (b, c1), (c, cd)):
+            assert base // 13 == (base + n - 1) // 13 and (base + n - 1) % 13 != 12, (base, n)
+            assert base + n <= slots
+        if c1 == 4:
+            starts.add(b % 8)
+    assert starts == set(range(8))
