@@ -5,8 +5,9 @@ Workload (one step): 2^20 seeded RAMBO points at sqrt(s) = 13 TeV with jet cuts 
 gg>qq~g in proportion to seeded random weights; every point's |M|^2 resolved per helicity, all
 colour orderings summed, in f64 (bit for bit the reference runner's f64 arithmetic).
 
-* value: the batched device API, every family in one persistent launch (captured in a CUDA
-  graph), momenta resident in HBM (168 MB of inputs: larger than L2, so no flush is needed);
+* value: the batched device API, every family in one CUDA-graph replay (a persistent launch per
+  blocks-per-SM choice the tuner made), momenta resident in HBM (168 MB of inputs: larger than
+  L2, so no flush is needed); clocks: nvidia-smi samples taken inside the timed region;
 * e2e: the call a generator makes, umami_matrix_element of the p p -> 3 jets UMAMI library
   (pacuda_b200/umami), one call per step over all events from pinned host momenta to |M|^2 in
   host memory, the copies in the timed region; e2e_abi: the runner's own C ABI
@@ -14,7 +15,10 @@ colour orderings summed, in f64 (bit for bit the reference runner's f64 arithmet
 * roofline: the dominant kernel's algorithmic flops (fixed per-op counts) per launch over its
   CUDA-event time, against this GPU's f64 FMA throughput measured in the same run;
 * cpu_baseline: the CPU oracle (the runner's arithmetic restated in C++, OpenMP over all cores)
-  on a bounded sample of the same families.
+  on a bounded sample of the same families;
+* precision, precision_gg4g (with the stability check), pp4j: the other kinds and the 6-leg
+  configurations (--no-precision skips them).
+--impl reference prints the reference arm's line: the CPU oracle on the same sample per step.
 
 usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 """
