@@ -97,9 +97,11 @@ void pacuda_b200_batch_destroy(pacuda_b200_batch *batch);
  * For callers that cannot allocate device or pinned memory when they evaluate.
  * Limits: 1 to PACUDA_B200_STATIC_MAX_PLANS plans, else INVALID (with a message on stderr). Calls
  * on one device must not overlap in time (they share the array): use one stream, or order them.
- * The first call on each device, with that device current, looks up the array's address (which
- * may load the library's device code); make it before capturing any stream on that device. Each
- * plan runs with its own lanes per point when the launch's shared memory allows, as in a batch. */
+ * The first call in each context of a device (so the first on each device, and the first after a
+ * device reset), with that device current, looks up the array's address (which may load the
+ * library's device code); make it before capturing any stream on that device. The launch is one
+ * block per SM (a batch may run several), each plan with its own points per block when the
+ * launch's shared memory allows: the same values as a batch, not always its speed. */
 #define PACUDA_B200_STATIC_MAX_PLANS 8
 int pacuda_b200_run_static(pacuda_b200_plan *const *plans, uint32_t nplans, const double *const *external,
                            const uint32_t *count, double *const *output, void *stream);

@@ -645,10 +645,43 @@ __global__ void static_setup(StaticBlock block, unsigned char *scratch) {
 }
 
 std::mutex g_static_mutex;
-void *g_static_address[kStaticDevices] = {nullptr};
 
-// the scratch's address on the current device, looked up on the first call with that device
-// current (the lookup may load this library's device code; later calls only read the cache)
+// the driver's context id of the calling thread's current context, or 0 when it cannot be read
+// (cuCtxGetId through the runtime's entry-point table: this library links no driver library)
+unsigned long long current_context_id() {
+    typedef int (*CtxGetCurrent)(void **);
+    typedef int (*CtxGetId)(void *, unsigned long long *);
+    static CtxGetCurrent get_current = nullptr;
+    static CtxGetId get_id = nullptr;
+    static bool looked_up = false;
+    if (!looked_up) {
+        looked_up = true;
+        void *f = nullptr, *g = nullptr;
+        cudaDriverEntryPointQueryResult q1, q2;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q1) == cudaSuccess &&
+            cudaGetDriverEntryPoint("cuCtxGetId", &g, cudaEnableDefault, &q2) == cudaSuccess &&
+            q1 == cudaDriverEntryPointSuccess && q2 == cudaDriverEntryPointSuccess) {
+            get_current = (CtxGetCurrent)f;
+            get_id = (CtxGetId)g;
+        }
+        cudaGetLastError();
+    }
+    void *ctx = nullptr;
+    unsigned long long id = 0;
+    if (!get_current || !get_id || get_current(&ctx) != 0 || !ctx || get_id(ctx, &id) != 0) return 0;
+    return id;
+}
+
+struct StaticAddress {
+    unsigned long long context = 0;  // the context the address belongs to (0: none)
+    void *address = nullptr;
+};
+StaticAddress g_static_address[kStaticDevices];
+
+// the scratch's address on the current device. It is looked up (cudaGetSymbolAddress, which may
+// load this library's device code) on the first call in each context of a device, so again after
+// a device reset or under another context on the same device; later calls compare the context
+// id and read the cache. Where the context id cannot be read, it is looked up on every call.
 unsigned char *static_scratch() {
     int dev = -1;
     if (failed(cudaGetDevice(&dev), "current device")) return nullptr;
@@ -656,14 +689,19 @@ unsigned char *static_scratch() {
         fprintf(stderr, "%s: run_static: device %d beyond the %d this entry point serves\n", kTag, dev, kStaticDevices);
         return nullptr;
     }
+    // 0 until the thread has a current context (the symbol lookup below makes the runtime's one
+    // current, so only a thread's first call looks up the address for that reason)
+    const unsigned long long context = current_context_id();
     std::lock_guard<std::mutex> lock(g_static_mutex);
-    if (!g_static_address[dev]) {
+    StaticAddress &c = g_static_address[dev];
+    if (!context || c.context != context || !c.address) {
         void *address = nullptr;
         if (failed(cudaGetSymbolAddress(&address, g_static_scratch), "static scratch address") || !address)
             return nullptr;
-        g_static_address[dev] = address;
+        c.context = context;
+        c.address = address;
     }
-    return (unsigned char *)g_static_address[dev];
+    return (unsigned char *)c.address;
 }
 
 }  // namespace
@@ -689,7 +727,16 @@ extern "C" int pacuda_b200_run_static(pacuda_b200_plan *const *plans, uint32_t n
     size_t const_bytes = 0;
     for (uint32_t k = 0; k < nplans; k++)
         const_bytes = std::max(const_bytes, tiled_const_bytes(plans[k]->scales, plans[k]->factors));
-    size_t max_smem = tiled_max_smem(kernel) - const_bytes;
+    // the shared memory a block may have, less the plan constants every block holds (checked
+    // before anything is queued)
+    const size_t room = tiled_max_smem(kernel);
+    if (room == 0) return PACMAN_RECURRENCE_DEVICE_ERROR;
+    if (room <= const_bytes) {
+        fprintf(stderr, "%s: run_static: the plans' constants (%zu bytes) fill a block's shared memory\n", kTag,
+                const_bytes);
+        return PACMAN_RECURRENCE_INVALID;
+    }
+    const size_t max_smem = room - const_bytes;
     StaticBlock block;
     memset(&block, 0, sizeof block);
     size_t smem = 0;

@@ -1,12 +1,17 @@
 // Host compilation of a plan's words into the device instruction stream.
 //
-// decode: the row layout of runner/recurrence_runner.cu:10-36 (fields of variable width after
-// a 4-bit op; op 14 followed by its data words), as that file's `decode` (:920-975) and
-// convert/src/program.rs (:60-114) read it. The sort: a run of contribution rows whose
-// destinations do not overlap and that reads none of them is stably sorted by destination
-// (:980-1007), which keeps every destination's own order of rows and so its value bit for bit.
-// The F_FIRST / F_LAST flags mark a destination's run of rows so that its sum stays in
-// registers (:1017-1054).
+// The row words follow the format of runner/recurrence_runner.cu:10-36 and
+// convert/src/program.rs:24-114 (`convert/CONVENTIONS.md` names the operands): a 4-bit op in the
+// low bits, then the op's operands from the least significant bit up, each as wide as the call's
+// `width` entry for its kind (or 1 or 10 bits); op 14 is followed by data words of two 32-bit
+// codes each. Here the layouts are a table of (operand, width) per op and a word is read at bit
+// offsets, so a field that would start past bit 63 reads 0, as shifting the word does.
+//
+// Contribution runs: a run whose destinations are disjoint and which reads none of them may run
+// its rows in any order that keeps each destination's own order (the reference sorts such runs
+// by destination, recurrence_runner.cu:977-1007). Here each destination's rows are gathered at
+// the place of its first row, so a destination's sum becomes one run of rows (F_FIRST .. F_LAST,
+// its sum kept in registers) with the same operations in the same order.
 #include "program.h"
 
 #include <algorithm>
@@ -15,109 +20,163 @@
 namespace pacuda {
 
 void contribution_shape(int op, int *c0, int *c1, int *cd) {
-    *c0 = op == 4 ? 6 : (op == 5 || op == 6) ? 4 : 2;
-    *c1 = 4;
-    *cd = (op == 4 || op == 6) ? 4 : op == 5 ? 6 : 2;
+    // (parent 0 components, parent 1 components, written components): CONVENTIONS.md's vertex types
+    static const int shape[5][3] = {{2, 4, 2}, {2, 4, 2}, {6, 4, 4}, {4, 4, 6}, {4, 4, 4}};
+    const int *s = shape[op - 2];
+    *c0 = s[0];
+    *c1 = s[1];
+    *cd = s[2];
 }
 
-bool decode_rows(const uint64_t *words, uint32_t count, const uint8_t *width, std::vector<Row> &rows,
-                 std::vector<uint32_t> &binding_data) {
-    rows.clear();
-    binding_data.clear();
-    for (uint32_t n = 0; n < count; n++) {
-        uint64_t w = words[n];
-        if ((w & 15) == 14) {
-            Row r{};
-            r.op = 14;
-            r.f[0] = (uint32_t)(w >> 4) & 0xffff;
-            r.f[1] = (uint32_t)(w >> 20) & 0xff;
-            r.f[2] = (uint32_t)(w >> 28) & 0xff;
-            r.f[3] = (uint32_t)(w >> 36) & 1;
-            uint32_t codes = r.f[1] + r.f[2];
-            r.data_first = (uint32_t)binding_data.size();
-            r.data_count = codes;
-            for (uint32_t k = 0; k < codes; k++) {
-                uint64_t d = n + 1 + k / 2 < count ? words[n + 1 + k / 2] : 0;
-                binding_data.push_back((uint32_t)(k % 2 ? d >> 32 : d));
-            }
-            n += (codes + 1) / 2;
-            rows.push_back(r);
-            continue;
-        }
-        bool wide = false;
-        auto take = [&](int bits) -> uint32_t {
-            if (bits > 32) { wide = true; return 0; }
-            uint32_t v = (uint32_t)(w & ((1ull << bits) - 1));
-            w >>= bits;
-            return v;
-        };
-        Row r{};
-        r.op = (int)take(4);
-        const int P = width[WP], A = width[WA], F = width[WF], X = width[WX], S = width[WS], K = width[WK];
-        int fields[8] = {0}, nf = 0;
-        switch (r.op) {
-        case 1: fields[0] = P; fields[1] = P; nf = 2; break;
-        case 2: case 3: case 4: case 5: case 6: {
-            int f[8] = {1, S, P, P, P, F, F, X};
-            std::copy(f, f + 8, fields);
-            nf = 8;
-            break;
-        }
-        case 7: case 8: case 9: fields[0] = P; fields[1] = F; fields[2] = X; nf = 3; break;
-        case 10: fields[0] = P; fields[1] = K; fields[2] = X; nf = 3; break;
-        case 11: {
-            int f[6] = {P, P, A, X, X, K};
-            std::copy(f, f + 6, fields);
-            nf = 6;
-            break;
-        }
-        case 12: {
-            int f[5] = {P, F, X, S, 10};
-            std::copy(f, f + 5, fields);
-            nf = 5;
-            break;
-        }
-        case 13: {
-            int f[7] = {1, P, P, P, F, F, X};
-            std::copy(f, f + 7, fields);
-            nf = 7;
-            break;
-        }
-        default: return false;  // ops 0 and 15 do not exist
-        }
-        for (int k = 0; k < nf; k++) r.f[k] = take(fields[k]);
-        if (wide) return false;
-        rows.push_back(r);
+namespace {
+
+// the width of a field: an index into the call's `width` table, or a fixed width
+enum FieldWidth : uint8_t { ONE_BIT = 6, TEN_BITS = 7 };
+
+struct Field {
+    uint32_t Row::*operand;
+    uint8_t width;
+};
+
+struct Layout {
+    uint8_t fields;
+    Field field[8];
+};
+
+// the operands of each op, least significant first (ops 1 .. 13; 14 is read apart)
+const Layout &layout_of(uint32_t op) {
+    static const Layout contribution{8, {{&Row::init, ONE_BIT}, {&Row::slot, WS}, {&Row::p0, WP}, {&Row::p1, WP},
+                                         {&Row::dst, WP}, {&Row::f0, WF}, {&Row::f1, WF}, {&Row::factor, WX}}};
+    static const Layout clear{2, {{&Row::dst, WP}, {&Row::count, WP}}};
+    static const Layout propagator{3, {{&Row::dst, WP}, {&Row::f0, WF}, {&Row::factor, WX}}};
+    static const Layout identity{3, {{&Row::dst, WP}, {&Row::count, WK}, {&Row::factor, WX}}};
+    static const Layout closure{6, {{&Row::p0, WP}, {&Row::p1, WP}, {&Row::amplitude, WA}, {&Row::factor, WX},
+                                    {&Row::first, WX}, {&Row::count, WK}}};
+    static const Layout source{5, {{&Row::dst, WP}, {&Row::f0, WF}, {&Row::factor, WX}, {&Row::slot, WS},
+                                   {&Row::code, TEN_BITS}}};
+    static const Layout symjit{7, {{&Row::init, ONE_BIT}, {&Row::p0, WP}, {&Row::p1, WP}, {&Row::dst, WP},
+                                   {&Row::f0, WF}, {&Row::f1, WF}, {&Row::factor, WX}}};
+    switch (op) {
+    case 1: return clear;
+    case 7: case 8: case 9: return propagator;
+    case 10: return identity;
+    case 11: return closure;
+    case 12: return source;
+    case 13: return symjit;
+    default: return contribution;
+    }
+}
+
+// `n` (at most 32) bits of `word` from bit `at`; bits past the word's end are 0
+uint32_t bits_at(uint64_t word, unsigned at, unsigned n) {
+    if (n == 0 || at >= 64) return 0;
+    return (uint32_t)((word >> at) & ((1ull << n) - 1));
+}
+
+// the component interval [lo, hi) a row touches
+struct Span {
+    uint32_t lo, hi;
+};
+
+bool meets(const std::vector<Span> &sorted, Span s) {
+    // the first interval that ends after s starts; s meets it if it starts before s ends
+    auto it = std::upper_bound(sorted.begin(), sorted.end(), s.lo, [](uint32_t v, const Span &x) { return v < x.hi; });
+    return it != sorted.end() && it->lo < s.hi;
+}
+
+// whether the contribution rows [begin, end) may be regrouped (see group_contribution_runs)
+bool regroupable(const std::vector<Row> &rows, size_t begin, size_t end) {
+    std::vector<Span> dest;  // one interval per destination, as wide as its widest row
+    for (size_t k = begin; k < end; k++) {
+        int c0, c1, cd;
+        contribution_shape((int)rows[k].op, &c0, &c1, &cd);
+        dest.push_back({rows[k].dst, rows[k].dst + (uint32_t)cd});
+    }
+    std::sort(dest.begin(), dest.end(), [](const Span &x, const Span &y) { return x.lo != y.lo ? x.lo < y.lo : x.hi > y.hi; });
+    std::vector<Span> merged;  // equal starts merged into the widest
+    for (const Span &s : dest)
+        if (merged.empty() || merged.back().lo != s.lo) merged.push_back(s);
+    for (size_t k = 1; k < merged.size(); k++)
+        if (merged[k].lo < merged[k - 1].hi) return false;  // two destinations share components
+    for (size_t k = begin; k < end; k++) {
+        int c0, c1, cd;
+        contribution_shape((int)rows[k].op, &c0, &c1, &cd);
+        if (meets(merged, {rows[k].p0, rows[k].p0 + (uint32_t)c0}) || meets(merged, {rows[k].p1, rows[k].p1 + (uint32_t)c1}))
+            return false;  // the run reads what it writes
     }
     return true;
 }
 
-void sort_contribution_runs(std::vector<Row> &rows) {
-    size_t n = 0;
-    while (n < rows.size()) {
-        if (rows[n].op < 2 || rows[n].op > 6) { n++; continue; }
-        size_t end = n;
-        while (end < rows.size() && rows[end].op >= 2 && rows[end].op <= 6) end++;
-        std::unordered_map<uint32_t, uint32_t> owner;  // component -> its destination's base
-        bool safe = true;
-        for (size_t k = n; k < end && safe; k++) {
-            int c0, c1, cd;
-            contribution_shape(rows[k].op, &c0, &c1, &cd);
-            for (int q = 0; q < cd; q++) {
-                auto it = owner.emplace(rows[k].f[4] + q, rows[k].f[4]);
-                if (it.first->second != rows[k].f[4]) safe = false;
-            }
+}  // namespace
+
+DecodeStatus decode_rows(const uint64_t *words, uint32_t count, const uint8_t *width, std::vector<Row> &rows,
+                         std::vector<uint32_t> &binding_data) {
+    rows.clear();
+    binding_data.clear();
+    uint8_t w[8];
+    for (int k = 0; k < 6; k++) {
+        if (width[k] > 32) return DECODE_BAD_WORD;
+        w[k] = width[k];
+    }
+    w[ONE_BIT] = 1;
+    w[TEN_BITS] = 10;
+    uint32_t n = 0;
+    while (n < count) {
+        const uint64_t word = words[n++];
+        Row r;
+        r.op = (uint32_t)(word & 15);
+        if (r.op == 0 || r.op == 15) return DECODE_BAD_WORD;
+        if (r.op == 14) {
+            // kernel (16 bits from bit 4), inputs (8 from 20), output pairs (8 from 28), direct (1 from 36)
+            r.kernel = bits_at(word, 4, 16);
+            r.inputs = bits_at(word, 20, 8);
+            r.pairs = bits_at(word, 28, 8);
+            r.direct = bits_at(word, 36, 1);
+            r.data_first = (uint32_t)binding_data.size();
+            const uint32_t codes = r.inputs + r.pairs, data_words = (codes + 1) / 2;
+            if (data_words > count - n) return DECODE_TRUNCATED_BINDING;
+            for (uint32_t k = 0; k < codes; k++) binding_data.push_back(bits_at(words[n + k / 2], 32 * (k & 1), 32));
+            n += data_words;
+            rows.push_back(r);
+            continue;
         }
-        for (size_t k = n; k < end && safe; k++) {
-            int c0, c1, cd;
-            contribution_shape(rows[k].op, &c0, &c1, &cd);
-            for (int q = 0; q < c0 && safe; q++) safe = !owner.count(rows[k].f[2] + q);
-            for (int q = 0; q < c1 && safe; q++) safe = !owner.count(rows[k].f[3] + q);
+        const Layout &l = layout_of(r.op);
+        unsigned at = 4;
+        for (unsigned k = 0; k < l.fields; k++) {
+            const unsigned width_k = w[l.field[k].width];
+            r.*(l.field[k].operand) = bits_at(word, at, width_k);
+            at += width_k;
         }
-        if (safe)
-            std::stable_sort(rows.begin() + n, rows.begin() + end,
-                             [](const Row &x, const Row &y) { return x.f[4] < y.f[4]; });
-        n = end;
+        rows.push_back(r);
+    }
+    return DECODE_OK;
+}
+
+void group_contribution_runs(std::vector<Row> &rows) {
+    std::vector<uint32_t> rank;
+    std::vector<Row> grouped;
+    size_t begin = 0;
+    while (begin < rows.size()) {
+        if (!is_contribution(rows[begin].op)) {
+            begin++;
+            continue;
+        }
+        size_t end = begin;
+        while (end < rows.size() && is_contribution(rows[end].op)) end++;
+        if (end - begin > 1 && regroupable(rows, begin, end)) {
+            // rank = the order of each destination's first row; a stable counting sort by rank
+            std::unordered_map<uint32_t, uint32_t> rank_of;  // destination -> rank
+            rank.assign(end - begin, 0);
+            for (size_t k = begin; k < end; k++)
+                rank[k - begin] = rank_of.emplace(rows[k].dst, (uint32_t)rank_of.size()).first->second;
+            std::vector<uint32_t> start(rank_of.size() + 1, 0);
+            for (uint32_t x : rank) start[x + 1]++;
+            for (size_t g = 1; g < start.size(); g++) start[g] += start[g - 1];
+            grouped.resize(end - begin);
+            for (size_t k = begin; k < end; k++) grouped[start[rank[k - begin]]++] = rows[k];
+            std::copy(grouped.begin(), grouped.end(), rows.begin() + begin);
+        }
+        begin = end;
     }
 }
 
@@ -161,15 +220,15 @@ BuildError build_program(const uint64_t *words, uint32_t count, const uint8_t *w
     BuildError err;
     std::vector<Row> rows;
     std::vector<uint32_t> binding_data;
-    for (int k = 0; k < 6; k++)
-        if (width[k] > 32) {
-            err.status = 2;
-            err.message = "a field width above 32 bits";
-            return err;
-        }
-    if (!decode_rows(words, count, width, rows, binding_data)) {
+    switch (decode_rows(words, count, width, rows, binding_data)) {
+    case DECODE_OK: break;
+    case DECODE_TRUNCATED_BINDING:  // a symjit binding: refused as the rows below
+        err.status = 3;
+        err.message = "a symjit binding whose codes run past the last word";
+        return err;
+    default:
         err.status = 2;
-        err.message = "a word with an op outside 1..14";
+        err.message = "a word with an op outside 1..14 or a field width above 32 bits";
         return err;
     }
     for (const Row &r : rows)
@@ -179,51 +238,52 @@ BuildError build_program(const uint64_t *words, uint32_t count, const uint8_t *w
             err.message = "a symjit row, but this runner has no symjit kernels";
             return err;
         }
-    if (sort) sort_contribution_runs(rows);
+    if (sort) group_contribution_runs(rows);
     out.ins.clear();
     out.ins.reserve(rows.size());
     out.flops = 0;
     uint64_t P = lim.current_planes;
+    auto same_destination = [&](size_t k, uint32_t dst) {
+        return k < rows.size() && is_contribution(rows[k].op) && rows[k].dst == dst;
+    };
     for (size_t n = 0; n < rows.size(); n++) {
         const Row &r = rows[n];
-        const uint32_t *f = r.f;
         Ins i{};
         bool ok = true;
-        if (r.op >= 2 && r.op <= 6) {
-            bool first = n == 0 || rows[n - 1].op < 2 || rows[n - 1].op > 6 || rows[n - 1].f[4] != f[4];
-            bool last = n + 1 == rows.size() || rows[n + 1].op < 2 || rows[n + 1].op > 6 || rows[n + 1].f[4] != f[4];
-            i = make(K_CONTRIB, r.op, (f[0] ? F_INIT : 0) | (first ? F_FIRST : 0) | (last ? F_LAST : 0), 0);
-            i.s = f[1]; i.a = f[2]; i.b = f[3]; i.c = f[4]; i.x = f[7];
+        if (is_contribution(r.op)) {
+            const bool first = n == 0 || !same_destination(n - 1, r.dst), last = !same_destination(n + 1, r.dst);
+            i = make(K_CONTRIB, r.op, (r.init ? F_INIT : 0) | (first ? F_FIRST : 0) | (last ? F_LAST : 0), 0);
+            i.s = r.slot; i.a = r.p0; i.b = r.p1; i.c = r.dst; i.x = r.factor;
             // the forms are read by op 6 only (a form index must fit 16 bits here)
-            i.f = r.op == 6 ? ((f[5] & 0xffff) | (f[6] << 16)) : 0;
+            i.f = r.op == 6 ? ((r.f0 & 0xffff) | (r.f1 << 16)) : 0;
             int c0, c1, cd;
-            contribution_shape(r.op, &c0, &c1, &cd);
-            ok = within(f[2], c0, P) && within(f[3], c1, P) && within(f[4], cd, P) && f[1] < lim.scales &&
-                 f[7] < lim.factors &&
-                 (r.op != 6 || (f[5] < lim.forms && f[6] < lim.forms && f[5] < 65536 && f[6] < 65536));
+            contribution_shape((int)r.op, &c0, &c1, &cd);
+            ok = within(r.p0, c0, P) && within(r.p1, c1, P) && within(r.dst, cd, P) && r.slot < lim.scales &&
+                 r.factor < lim.factors &&
+                 (r.op != 6 || (r.f0 < lim.forms && r.f1 < lim.forms && r.f0 < 65536 && r.f1 < 65536));
         } else if (r.op == 1) {
             i = make(K_CLEAR, 1, 0, 0);
-            i.a = f[0]; i.b = f[1];
-            ok = within(f[0], f[1], P);
+            i.a = r.dst; i.b = r.count;
+            ok = within(r.dst, r.count, P);
         } else if (r.op >= 7 && r.op <= 9) {
             i = make(K_PROP, r.op, 0, 0);
-            i.a = f[0]; i.f = f[1]; i.x = f[2];
-            ok = within(f[0], r.op == 9 ? 4 : 2, P) && f[1] < lim.forms && f[2] < lim.factors;
+            i.a = r.dst; i.f = r.f0; i.x = r.factor;
+            ok = within(r.dst, r.op == 9 ? 4 : 2, P) && r.f0 < lim.forms && r.factor < lim.factors;
         } else if (r.op == 10) {
             i = make(K_IDENTITY, 10, 0, 0);
-            i.a = f[0]; i.b = f[1]; i.x = f[2];
-            ok = within(f[0], f[1], P) && f[2] < lim.factors;
+            i.a = r.dst; i.b = r.count; i.x = r.factor;
+            ok = within(r.dst, r.count, P) && r.factor < lim.factors;
         } else if (r.op == 11) {
             i = make(K_CLOSURE, 11, 0, 0);
-            i.a = f[0]; i.b = f[1]; i.c = f[2]; i.x = f[3]; i.y = f[4];
-            i.s = f[5];  // the component count
-            ok = within(f[0], f[5], P) && within(f[1], f[5], P) && f[2] < lim.amplitude_planes && f[3] < lim.factors &&
-                 within(f[4], f[5], lim.factors);
+            i.a = r.p0; i.b = r.p1; i.c = r.amplitude; i.x = r.factor; i.y = r.first;
+            i.s = r.count;  // the component count
+            ok = within(r.p0, r.count, P) && within(r.p1, r.count, P) && r.amplitude < lim.amplitude_planes &&
+                 r.factor < lim.factors && within(r.first, r.count, lim.factors);
         } else {  // 12
             i = make(K_SOURCE, 12, 0, 0);
-            i.a = f[0]; i.f = f[1]; i.x = f[2]; i.s = f[3]; i.y = f[4];
-            int comps = (f[4] & 7) == 0 ? 1 : (f[4] & 7) == 1 ? 2 : 4;
-            ok = within(f[0], comps, P) && f[1] < lim.forms && f[2] < lim.factors && f[3] < lim.scales;
+            i.a = r.dst; i.f = r.f0; i.x = r.factor; i.s = r.slot; i.y = r.code;
+            int comps = (r.code & 7) == 0 ? 1 : (r.code & 7) == 1 ? 2 : 4;
+            ok = within(r.dst, comps, P) && r.f0 < lim.forms && r.factor < lim.factors && r.slot < lim.scales;
         }
         if (!ok) {
             err.status = 2;

@@ -9,7 +9,7 @@ helicity and chirality, both energy signs and the pT = 0 and p = 0 edge cases, a
 cases and the legend's values. The oracle must agree with them to 1e-13 relative, the
 reference's own bar (check_sources.py:105).
 
-usage: python tests/golden/make_sources_golden.py [/root/reference]
+usage: python tests/golden/make_sources_golden.py [reference source tree]
 """
 import ast
 import math
@@ -19,8 +19,11 @@ import sys
 
 import numpy as np
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
 HERE = os.path.dirname(os.path.abspath(__file__))
+# the reference's source tree: the first argument, $PACUDA_REFERENCE, else a checkout named
+# `reference` beside this repository
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get(
+    "PACUDA_REFERENCE", os.path.join(os.path.dirname(os.path.dirname(os.path.dirname(HERE))), "reference"))
 
 
 def legend():

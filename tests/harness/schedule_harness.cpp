@@ -35,16 +35,31 @@ int schedule_stats(const uint64_t *words, uint32_t count, const uint8_t *width, 
     return 0;
 }
 
-// the program's instructions (reference order, after the sort): count, then 8 u32 each
-int program_export(const uint64_t *words, uint32_t count, const uint8_t *width, uint32_t planes, uint32_t amps,
-                   uint32_t forms, uint32_t scales, uint32_t factors, uint32_t *n, uint32_t *ins) {
+// the program's instructions (the plan's row order, contribution runs grouped when `group`):
+// count, then 8 u32 each
+int program_export_order(const uint64_t *words, uint32_t count, const uint8_t *width, uint32_t planes, uint32_t amps,
+                         uint32_t forms, uint32_t scales, uint32_t factors, int group, uint32_t *n, uint32_t *ins) {
     Program p;
     Limits lim{planes, amps, forms, scales, factors};
-    BuildError e = build_program(words, count, width, true, lim, p);
+    BuildError e = build_program(words, count, width, group != 0, lim, p);
     if (e.status) return e.status;
     *n = (uint32_t)p.ins.size();
     if (ins) memcpy(ins, p.ins.data(), p.ins.size() * sizeof(Ins));
     return 0;
+}
+
+// the program's instructions as the device runs them (contribution runs grouped)
+int program_export(const uint64_t *words, uint32_t count, const uint8_t *width, uint32_t planes, uint32_t amps,
+                   uint32_t forms, uint32_t scales, uint32_t factors, uint32_t *n, uint32_t *ins) {
+    return program_export_order(words, count, width, planes, amps, forms, scales, factors, 1, n, ins);
+}
+
+// build_program's status for a plan (0, or the runner's status code)
+int program_status(const uint64_t *words, uint32_t count, const uint8_t *width, uint32_t planes, uint32_t amps,
+                   uint32_t forms, uint32_t scales, uint32_t factors) {
+    Program p;
+    Limits lim{planes, amps, forms, scales, factors};
+    return build_program(words, count, width, true, lim, p).status;
 }
 
 // the schedule's arrays (for the emulator): sizes first (ins, tasks + 1, levels + 1, loads, amp planes)

@@ -22,6 +22,19 @@ LIB = os.path.join(ROOT, "pacuda_b200", "librecurrence.so")
 REF = os.path.join(ROOT, "oracle", "_ref", "librecurrence.so")
 KINDS = ["f64", "df64", "mixed", "mixed64"]
 _cache = {}
+_dir = []
+
+
+def _tmp():
+    """A private temporary folder for the workers' outputs (removed at exit)."""
+    if not _dir:
+        import atexit
+        import shutil
+        import tempfile
+
+        _dir.append(tempfile.mkdtemp(prefix="pacuda_parity_"))
+        atexit.register(shutil.rmtree, _dir[0], True)
+    return _dir[0]
 
 
 def worker(lib, kind, nosort=False, executor=None, lanes=0):
@@ -29,8 +42,7 @@ def worker(lib, kind, nosort=False, executor=None, lanes=0):
     if key not in _cache:
         tag = f"{os.path.basename(os.path.dirname(lib))}_{kind}{'_nosort' if nosort else ''}{'_' + executor if executor else ''}" \
             f"{f'_lanes{lanes}' if lanes else ''}"
-        out = os.path.join(ROOT, "gpurun_out", f"parity_{tag}.npz") if os.path.isdir(os.path.join(ROOT, "gpurun_out")) \
-            else f"/tmp/parity_{tag}.npz"
+        out = os.path.join(_tmp(), f"parity_{tag}.npz")
         cmd = [sys.executable, os.path.join(ROOT, "tests", "gpu_worker.py"), lib, kind, out] + (["nosort"] if nosort else []) \
             + ([executor] if executor else []) + ([f"lanes={lanes}"] if lanes else [])
         subprocess.run(cmd, check=True, timeout=600)
