@@ -210,11 +210,24 @@ def precision_line(torch, B, fams, ext, ref_out, steps, warmup, kind="mixed"):
             "blocks_per_sm": {nm: batch.plan_blocks_per_sm(k) for k, (nm, _, _) in enumerate(fams)}}
 
 
-def six_gluon_line(torch, B, points=1 << 20, steps=3, warmup=2):
+def oracle_parity(cases):
+    """Bitwise parity of device outputs with the oracle: cases (label, template, point-major
+    momenta, device outputs [point][helicity])."""
+    from oracle import oracle as O
+
+    pairs = []
+    for label, t, p, o in cases:
+        _, want = O.evaluate(t, p, kernel=1)
+        pairs.append((label, o.cpu().numpy(), want))
+    return parity(pairs)
+
+
+def six_gluon_line(torch, B, points=1 << 20, steps=3, warmup=2, check=256):
     """The precision configuration: g g -> 4 g, leading colour (60 orderings x 64 helicities, as
     the plan parts that fit 64-bit words), `points` seeded RAMBO points at 13 TeV with the loosened
     cuts pT > 5 GeV and Delta R > 0.1; points/s in f64 and in mixed precision, and the histogram of
-    each point's relative error in |M|^2 (mixed against f64)."""
+    each point's relative error in |M|^2 (mixed against f64). The f64 outputs of the first `check`
+    points of every plan are compared bit for bit with the oracle's."""
     from pacuda_b200 import phase_space, processes
 
     parts = processes.parts("gg>gggg")
@@ -240,6 +253,9 @@ def six_gluon_line(torch, B, points=1 << 20, steps=3, warmup=2):
                      "tflops": flops / (ms * 1e-3) / 1e12,
                      "lanes_per_point": [batch.lanes_per_point(k) for k in range(len(plans))]}
         totals[kind] = sum(o.view(points, t.outputs).sum(dim=1) for o, t in zip(outs, parts))
+        if kind == "f64":
+            res["parity"] = oracle_parity([(f"gg>gggg part {k}", t, p[:check], o.view(points, t.outputs)[:check])
+                                           for k, (t, o) in enumerate(zip(parts, outs))])
         del batch, outs
     rel = ((totals["mixed"] - totals["f64"]).abs() / totals["f64"].abs().clamp_min(1e-300)).cpu().numpy()
     edges = [0.0] + [10.0 ** e for e in range(-16, 1)] + [np.inf]
@@ -281,11 +297,12 @@ def stability_line(torch, templates, ext, want, points, steps, warmup, tols=(1e-
     return lines
 
 
-def pp4j_line(torch, B, points=1 << 22, steps=3, warmup=2):
+def pp4j_line(torch, B, points=1 << 22, steps=3, warmup=2, check=256):
     """p p -> 4 jets, every massless family the intrinsic ops express (gg>gggg as its plan parts,
     qg>qggg, qq~>gggg, gg>qq~gg), `points` seeded RAMBO points at 13 TeV with pT > 20 GeV and
     Delta R > 0.4 split over the families by seeded random weights, all in one persistent launch:
-    points/s in f64 and in mixed precision, with the mixed kernel's relative error in |M|^2."""
+    points/s in f64 and in mixed precision, with the mixed kernel's relative error in |M|^2; the f64
+    outputs of the first `check` points of every plan bit for bit against the oracle's."""
     from pacuda_b200 import phase_space, processes
 
     names = processes.PP4J
@@ -293,9 +310,10 @@ def pp4j_line(torch, B, points=1 << 22, steps=3, warmup=2):
     w = rng.dirichlet(np.ones(len(names)))
     counts = np.maximum(1024, np.floor(w * points).astype(int))
     counts[int(np.argmax(counts))] += points - counts.sum()
-    fams = []
+    fams, moms = [], {}
     for k, (name, n) in enumerate(zip(names, counts)):
         p = phase_space.sample(6, int(n), SEED + 40 + k, ecm=ECM)
+        moms[name] = p[:check]
         e = torch.tensor(phase_space.source_major(p), dtype=torch.float64, device="cuda")
         for t in processes.parts(name):
             fams.append((name, t, int(n), e))
@@ -324,6 +342,9 @@ def pp4j_line(torch, B, points=1 << 22, steps=3, warmup=2):
             x = o.view(n, t.outputs).sum(dim=1)
             per_family[name] = per_family[name] + x if name in per_family else x
         totals[kind] = torch.cat([per_family[nm] for nm in names])
+        if kind == "f64":
+            res["parity"] = oracle_parity([(f"{name} plan {k}", t, moms[name][:check], o.view(n, t.outputs)[:check])
+                                           for k, ((name, t, n, _), o) in enumerate(zip(fams, outs))])
         del batch, outs
     rel = ((totals["mixed"] - totals["f64"]).abs() / totals["f64"].abs().clamp_min(1e-300)).cpu().numpy()
     res["mixed"]["rel_error_vs_f64"] = {"median": float(np.median(rel)), "q999": float(np.quantile(rel, 0.999)),
@@ -351,30 +372,55 @@ def hbm_peak():
         return 6650.0
 
 
-def cpu_baseline(fams, sample=2048):
+def cpu_baseline(fams, sample=2048, keep=None):
     """The oracle on the first `sample` points of each family, all host cores; points/s of the
-    family mix (each family's rate weighted by its share of the workload)."""
+    family mix (each family's rate weighted by its share of the workload). With a dict `keep`,
+    each family's oracle outputs [point][helicity] are kept there by name (the parity check)."""
     from oracle import oracle as O
 
     counts = [p.shape[0] for _, _, p in fams]
     total = sum(counts)
     secs = 0.0
-    done = 0
     for (name, t, p), n in zip(fams, counts):
         m = min(sample, n)
         t0 = time.perf_counter()
-        O.evaluate(t, p[:m], kernel=1)
+        _, out = O.evaluate(t, p[:m], kernel=1)
         dt = time.perf_counter() - t0
         secs += dt * (n / m)  # the time of the family's full share at this rate
-        done += n
+        if keep is not None:
+            keep[name] = out
     return {"value": total / secs, "unit": "points/s", "cores": os.cpu_count(), "kind": "port",
             "sample": f"first {sample} points of each family (of {total}), OpenMP over all host cores, "
                       f"rates weighted by the families' shares"}
 
 
-def e2e_abi(fams, steps, warmup, lib=None, kernel="f64"):
+def same_bits(a, b):
+    a, b = np.ascontiguousarray(a, dtype=np.float64), np.ascontiguousarray(b, dtype=np.float64)
+    return a.shape == b.shape and bool(np.all((a.view(np.uint64) == b.view(np.uint64)) | (np.isnan(a) & np.isnan(b))))
+
+
+def parity(pairs):
+    """Bitwise comparison of (label, got, want) arrays: values checked and values that differ."""
+    checked, bad, where = 0, 0, []
+    for label, got, want in pairs:
+        got = np.ascontiguousarray(got, dtype=np.float64)
+        want = np.ascontiguousarray(want, dtype=np.float64)
+        checked += want.size
+        if got.shape != want.shape:
+            bad += want.size
+            where.append(label)
+            continue
+        diff = ~((got.view(np.uint64) == want.view(np.uint64)) | (np.isnan(got) & np.isnan(want)))
+        if diff.any():
+            bad += int(diff.sum())
+            where.append(label)
+    return {"values_checked": checked, "mismatches": bad, "differing": where}
+
+
+def e2e_abi(fams, steps, warmup, lib=None, kernel="f64", events=None):
     """points/s through the C ABI: per tile one run (forms on the device, amplitudes kept) and one
-    resolved reduction, from pinned host buffers."""
+    resolved reduction, from pinned host buffers. With `events` (two CUDA events), also the rate
+    between them recorded on the default stream around the timed steps."""
     import ctypes as C
 
     from pacuda_b200 import abi, phase_space
@@ -406,13 +452,67 @@ def e2e_abi(fams, steps, warmup, lib=None, kernel="f64"):
 
     for _ in range(warmup):
         step()
+    if events:
+        events[0].record()
     t0 = time.perf_counter()
     for _ in range(steps):
         step()
+    if events:
+        events[1].record()
+        events[1].synchronize()
     dt = (time.perf_counter() - t0) / steps
     total = sum(p.shape[0] for _, _, p in fams)
-    return {"value": total / dt, "unit": "points/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-            "tile": TILE, "calls_per_step": 2 * len(jobs)}, [j[3] for j in jobs]
+    res = {"value": total / dt, "unit": "points/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+           "tile": TILE, "calls_per_step": 2 * len(jobs), "steps": steps}
+    if events:
+        ms = events[0].elapsed_time(events[1]) / steps
+        res["device_value"] = total / (ms * 1e-3)
+        res["device_ms_per_step"] = ms
+    return res, [j[3] for j in jobs]
+
+
+REF_LIB = os.path.join(ROOT, "oracle", "_ref", "librecurrence.so")
+
+
+def reference_gpu_worker(kind, steps, warmup, keep_path):
+    """In its own process (a runner takes its kernel kind once, before its first run): the
+    reference's runner built from its own sources for sm_100a (oracle/_ref/librecurrence.so,
+    recurrence_runner.cu unmodified) through its stock C ABI, the same points as this benchmark,
+    per tile of 2^16 points one run (forms on the device, amplitudes kept) and one resolved
+    reduction from pinned host buffers. Prints one JSON line: points/s from CUDA events on the
+    default stream (which the reference runner's synchronous copies and launches use) and from
+    the host clock; with `keep_path`, the first 2048 outputs of each family go there."""
+    import torch
+
+    fams = workload(0)
+    torch.cuda.init()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    line, outs = e2e_abi(fams, steps, warmup, lib=REF_LIB, kernel=kind, events=(e0, e1))
+    line["kernel"] = kind
+    if keep_path:
+        first = {}
+        for (name, t, p), o in zip(fams, outs):
+            if name not in first:
+                first[name] = np.array(o[: min(2048, p.shape[0]) * t.outputs]).reshape(-1, t.outputs)
+        np.savez(keep_path, **first)
+    print(json.dumps(line))
+
+
+def reference_gpu(kinds=("f64", "df64", "mixed"), steps=2, warmup=1, keep_path=None):
+    """The reference runner's rate per kernel kind (one worker process each; see
+    reference_gpu_worker). None when the reference runner is not built."""
+    if not os.path.exists(REF_LIB):
+        return None
+    res = {}
+    for kind in kinds:
+        cmd = [sys.executable, os.path.abspath(__file__), "--reference-gpu-kind", kind, "--steps", str(steps),
+               "--warmup", str(warmup), "--points", str(POINTS)] + (["--keep", keep_path] if keep_path and kind == "f64" else [])
+        p = subprocess.run(cmd, capture_output=True, text=True, timeout=900)
+        if p.returncode != 0:
+            res[kind] = {"error": (p.stderr or p.stdout).strip().splitlines()[-1:]}
+            continue
+        res[kind] = json.loads(p.stdout.strip().splitlines()[-1])
+    return res
 
 
 def e2e_umami(fams, steps, warmup, outs=None):
@@ -506,8 +606,14 @@ def main():
     ap.add_argument("--lanes-per-point", type=int, default=0)
     ap.add_argument("--no-precision", action="store_true", help="skip the mixed-precision lines")
     ap.add_argument("--blocks-per-sm", type=int, default=0, help="1, 2, 3, 4, 5, 8 or 16 (with --no-tune or --lanes-per-point)")
+    ap.add_argument("--no-reference-gpu", action="store_true", help="skip timing the reference's own GPU runner")
+    ap.add_argument("--reference-gpu-kind", default=None, help=argparse.SUPPRESS)  # the worker of reference_gpu()
+    ap.add_argument("--keep", default=None, help=argparse.SUPPRESS)
     args = ap.parse_args()
     POINTS = args.points
+    if args.reference_gpu_kind:
+        reference_gpu_worker(args.reference_gpu_kind, args.steps, args.warmup, args.keep)
+        return
     if args.family:
         FAMILIES = [args.family]
     rank = int(os.environ.get("RANK", 0))
@@ -634,8 +740,41 @@ def main():
             abi_line, _ = e2e_abi(fams, max(1, args.steps // 5), 1)
             abi_line["api"] = "pacman_recurrence_v1_run + _reduce_resolved per tile of 2^16 points"
             res["e2e_abi"] = abi_line
+        oracle_out = {}
         if not args.no_cpu:
-            res["cpu_baseline"] = cpu_baseline(fams)
+            res["cpu_baseline"] = cpu_baseline(fams, keep=oracle_out)
+        # parity of what was timed: the first 2048 points of every family, bit for bit
+        first = {name: o.view(p.shape[0], t.outputs)[: min(2048, p.shape[0])].cpu().numpy()
+                 for o, (name, t, p) in zip(out, fams)}
+        if not oracle_out:
+            from oracle import oracle as O
+
+            for name, t, p in fams:
+                oracle_out[name] = O.evaluate(t, p[: min(2048, p.shape[0])], kernel=1)[1]
+        pairs = [(f"{name} vs oracle", first[name], oracle_out[name]) for name, _, _ in fams]
+        if not args.no_reference_gpu and not args.family:
+            import tempfile
+
+            keep = os.path.join(tempfile.mkdtemp(prefix="bench_ref_"), "ref_f64.npz")
+            ref = reference_gpu(steps=2, warmup=1, keep_path=keep)
+            if ref:
+                res["reference_gpu"] = ref
+                res["reference_gpu"]["runner"] = ("the reference's recurrence_runner.cu built from its own sources for "
+                                                  "sm_100a (oracle/Makefile, runner/build.sh flags), unmodified, through its "
+                                                  "C ABI: per tile of 2^16 points a run and a resolved reduction from pinned "
+                                                  "host buffers")
+                f64 = ref.get("f64", {})
+                if "device_value" in f64:
+                    res["vs_reference_gpu"] = {"value_over_device_f64": value / f64["device_value"],
+                                               "e2e_over_e2e_f64": (res["e2e"]["value"] / f64["value"]) if "e2e" in res else None,
+                                               "e2e_abi_over_e2e_f64": (res["e2e_abi"]["value"] / f64["value"])
+                                               if "e2e_abi" in res else None}
+                if os.path.exists(keep):
+                    ref_out = dict(np.load(keep))
+                    pairs += [(f"{name} vs reference runner f64", first[name], ref_out[name]) for name, _, _ in fams]
+        res["parity"] = parity(pairs)
+        res["parity"]["what"] = ("the timed run's outputs of the first 2048 points of each family against the oracle "
+                                 "and the reference runner's f64 kernel, bit for bit")
         if not args.no_precision:
             res["precision"] = [precision_line(torch, B, fams, ext, out, args.steps, args.warmup, k)
                                 for k in ("mixed", "mixed64", "df64")]
