@@ -1,0 +1,147 @@
+"""Test infrastructure: numpy restatement of the unweighting kernels (libsurrogate.so), the checker
+of their phase-space points, cuts and accept/reject decisions, and a CPU toy of two-stage
+unweighting with a known density.
+
+Candidate i of a stream with seed S draws its uniforms from a xorshift64 stream (shifts 13, 7,
+17; uniform = ((state >> 11) + 0.5) / 2^53) started at splitmix64(S ^ (i * 0xD1B54A32D192ED03)) | 1
+-- the construction pacuda_b200/phase_space.rambo uses. Uniforms 0-4 are the phase-space
+numbers, 5 the first accept/reject number, 6 the second.
+
+The phase-space map (massless 2 -> 3 at fixed sqrt(s), sequential two-body decays):
+  s23 = s x1; p1 in the centre-of-mass frame with |p1| = (s - s23) / (2 sqrt(s)), cos(theta) =
+  2 x2 - 1, phi = 2 pi x3; p2, p3 back to back in the rest frame of q = P - p1 with |p| =
+  sqrt(s23) / 2, cos(theta) = 2 x4 - 1, phi = 2 pi x5, boosted along q.
+  Its weight (the phase-space density of the unit cube): J = s (1 - x1) / (128 pi^3), whose
+  integral s / (256 pi^3) is the massless three-body volume (RAMBO's).
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+_M64 = (1 << 64) - 1
+UNIFORMS = 7
+
+
+def _splitmix(x):
+    x = (x + np.uint64(0x9E3779B97F4A7C15)) & np.uint64(_M64)
+    z = x
+    z = ((z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)) & np.uint64(_M64)
+    z = ((z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)) & np.uint64(_M64)
+    return z ^ (z >> np.uint64(31))
+
+
+def uniforms(seed, index):
+    """[len(index)][7] uniforms of the candidates `index` (uint64 array) of stream `seed`."""
+    with np.errstate(over="ignore"):
+        idx = np.asarray(index, dtype=np.uint64)
+        state = _splitmix(np.uint64(seed) ^ (idx * np.uint64(0xD1B54A32D192ED03))) | np.uint64(1)
+        u = np.empty((idx.size, UNIFORMS))
+        for k in range(UNIFORMS):
+            state ^= state << np.uint64(13)
+            state ^= state >> np.uint64(7)
+            state ^= state << np.uint64(17)
+            u[:, k] = ((state >> np.uint64(11)).astype(np.float64) + 0.5) / float(1 << 53)
+    return u
+
+
+def _boost(p, b):
+    """p [n][4] boosted by velocity b [n][3] (the frame moving with -b sees p at rest if b = v)."""
+    b2 = (b * b).sum(axis=1)
+    g = 1.0 / np.sqrt(1.0 - b2)
+    bp = (b * p[:, 1:]).sum(axis=1)
+    gg = np.where(b2 > 0, (g - 1.0) / np.where(b2 > 0, b2, 1.0), 0.0)
+    out = np.empty_like(p)
+    out[:, 0] = g * (p[:, 0] + bp)
+    out[:, 1:] = p[:, 1:] + (gg * bp + g * p[:, 0])[:, None] * b
+    return out
+
+
+def phase_space(u, sqrt_s):
+    """Point-major momenta [n][5][4] (beams first) and the weight J of the uniforms u[:, :5]."""
+    s = sqrt_s * sqrt_s
+    n = u.shape[0]
+    s23 = s * u[:, 0]
+    e1 = (s - s23) / (2.0 * sqrt_s)
+    c1 = 2.0 * u[:, 1] - 1.0
+    st1 = np.sqrt(np.maximum(0.0, 1.0 - c1 * c1))
+    f1 = 2.0 * math.pi * u[:, 2]
+    p1 = np.stack([e1, e1 * st1 * np.cos(f1), e1 * st1 * np.sin(f1), e1 * c1], axis=1)
+    m23 = np.sqrt(s23)
+    k = 0.5 * m23
+    c2 = 2.0 * u[:, 3] - 1.0
+    st2 = np.sqrt(np.maximum(0.0, 1.0 - c2 * c2))
+    f2 = 2.0 * math.pi * u[:, 4]
+    p2r = np.stack([k, k * st2 * np.cos(f2), k * st2 * np.sin(f2), k * c2], axis=1)
+    p3r = np.stack([k, -p2r[:, 1], -p2r[:, 2], -p2r[:, 3]], axis=1)
+    eq = sqrt_s - e1
+    b = -p1[:, 1:] / eq[:, None]
+    p = np.empty((n, 5, 4))
+    p[:, 0] = (0.5 * sqrt_s, 0.0, 0.0, 0.5 * sqrt_s)
+    p[:, 1] = (0.5 * sqrt_s, 0.0, 0.0, -0.5 * sqrt_s)
+    p[:, 2] = p1
+    p[:, 3] = _boost(p2r, b)
+    p[:, 4] = _boost(p3r, b)
+    jac = s * (1.0 - u[:, 0]) / (128.0 * math.pi ** 3)
+    return p, jac
+
+
+def passes(p, pt_min=20.0, eta_max=5.0, dr_min=0.4):
+    """The cuts on legs 2..4: pT > pt_min, |eta| < eta_max (eta = asinh(pz / pT)), pairwise
+    Delta R > dr_min."""
+    fin = p[:, 2:]
+    pt = np.hypot(fin[..., 1], fin[..., 2])
+    with np.errstate(divide="ignore", invalid="ignore"):
+        eta = np.arcsinh(fin[..., 3] / pt)
+    phi = np.arctan2(fin[..., 2], fin[..., 1])
+    ok = (pt > pt_min).all(axis=1) & (np.abs(eta) < eta_max).all(axis=1)
+    for i in range(3):
+        for j in range(i + 1, 3):
+            d = np.abs(phi[:, i] - phi[:, j])
+            d = np.where(d > math.pi, 2.0 * math.pi - d, d)
+            de = eta[:, i] - eta[:, j]
+            ok &= de * de + d * d > dr_min * dr_min
+    return ok
+
+
+def features(u, family, families):
+    """The network's inputs: the five phase-space numbers, then the subprocess one-hot."""
+    f = np.zeros((u.shape[0], 5 + families), dtype=np.float32)
+    f[:, :5] = u[:, :5]
+    f[:, 5 + family] = 1.0
+    return f
+
+
+def plain_decide(w, u, w_max):
+    """Plain unweighting: keep a point when u w_max < w; its weight max(1, w / w_max)."""
+    keep = u * w_max < w
+    return keep, np.where(keep, np.maximum(1.0, w / w_max), 0.0)
+
+
+def stage1_decide(s, u, s_max):
+    return u * s_max < s
+
+
+def stage2_decide(w, s, s_over, u, r_max):
+    """Second stage: r = w / s; keep when u r_max < r; weight max(1, s / s_max) max(1, r / r_max)
+    (`s_over` = max(1, s / s_max) of the first stage)."""
+    r = w / s
+    keep = u * r_max < r
+    return keep, np.where(keep, s_over * np.maximum(1.0, r / r_max), 0.0), r
+
+
+def toy_two_stage(n, seed, bias=0.2):
+    """A CPU toy of two-stage unweighting on [0,1]^2 with the density f(x, y) = exp(-((x - 0.3)^2 +
+    (y - 0.6)^2) / 0.02) + 0.2 and a surrogate off by a smooth factor up to 1 +- bias: the accepted
+    events with their weights, and the plain unweighting's, for unbiasedness tests."""
+    rng = np.random.default_rng(seed)
+    x = rng.uniform(size=(n, 2))
+    f = np.exp(-((x[:, 0] - 0.3) ** 2 + (x[:, 1] - 0.6) ** 2) / 0.02) + 0.2
+    s = f * (1.0 + bias * np.sin(7.0 * x[:, 0]) * np.cos(5.0 * x[:, 1]))
+    u1, u2, u3 = rng.uniform(size=(3, n))
+    f_max, s_max = f.max() * 0.9, s.max() * 0.9  # reduced maxima: some weights above 1
+    keep_p, w_p = plain_decide(f, u1, f_max)
+    k1 = stage1_decide(s, u2, s_max)
+    keep2, w2, _ = stage2_decide(f[k1], s[k1], np.maximum(1.0, s[k1] / s_max), u3[k1], np.quantile(f[k1] / s[k1], 0.99))
+    return x, f, (x[keep_p], w_p[keep_p]), (x[k1][keep2], w2[keep2])

@@ -1,8 +1,11 @@
-"""Builds the runner library pacuda_b200/librecurrence.so in the source tree (nvcc, sm_100a).
+"""Builds the libraries in the source tree (nvcc, sm_100a).
 
-The library is the product: the C ABI of include/pacman_recurrence.h. It is compiled with
--fmad=false so that no multiply-add is contracted (the f64 kernel's arithmetic is the
-reference's, operation by operation) and linked against the static CUDA runtime.
+* pacuda_b200/librecurrence.so: the runner, the C ABI of include/pacman_recurrence.h and the
+  batched API of include/pacuda_b200.h. Compiled with -fmad=false so that no multiply-add is
+  contracted (the f64 kernel's arithmetic is the reference's, operation by operation) and linked
+  against the static CUDA runtime.
+* pacuda_b200/libsurrogate.so: the surrogate network (include/pacuda_surrogate.h) and the
+  two-stage unweighting kernels; free to contract multiply-adds.
 """
 from __future__ import annotations
 
@@ -12,28 +15,47 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
+INCLUDE = os.path.join(HERE, "..", "include")
 LIB = os.path.join(HERE, "librecurrence.so")
+SG_LIB = os.path.join(HERE, "libsurrogate.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 SOURCES = ["runner.cu", "batch.cu", "program.cpp", "schedule.cpp", "tiled_host.cu", "peak.cu"]
+SG_SOURCES = ["surrogate.cu"]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-fmad=false", "-lineinfo", "-Xcompiler", "-fPIC", "-shared", "-cudart", "static",
-         "-gencode", "arch=compute_100a,code=sm_100a", "-Xptxas", "-warn-spills"]
+         "-Xptxas", "-warn-spills"] + ARCH
+SG_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-shared", "-cudart", "static",
+            "-Xptxas", "-warn-spills"] + ARCH
+
+RUNNER_DEPS = ["runner.cu", "batch.cu", "program.cpp", "program.h", "schedule.cpp", "schedule.h", "tiled_host.cu",
+               "tiled_host.h", "peak.cu", "arith.cuh", "executor.cuh", "tiled.cuh"]
+SG_DEPS = ["surrogate.cu", "umma.cuh"]
+
+
+def _stale(target, deps, headers):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    paths = [os.path.join(CSRC, f) for f in deps] + [os.path.join(INCLUDE, h) for h in headers]
+    return any(os.path.getmtime(d) > t for d in paths if os.path.exists(d))
 
 
 def stale():
-    if not os.path.exists(LIB):
-        return True
-    t = os.path.getmtime(LIB)
-    deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(HERE, "..", "include", "pacman_recurrence.h")]
-    return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
+    return _stale(LIB, RUNNER_DEPS, ["pacman_recurrence.h", "pacuda_b200.h"]) or \
+        _stale(SG_LIB, SG_DEPS, ["pacuda_surrogate.h"])
 
 
-def build(force=False, verbose=False):
-    if not force and not stale():
-        return LIB
-    cmd = [NVCC] + FLAGS + ["-o", LIB] + [os.path.join(CSRC, s) for s in SOURCES]
+def _run(cmd, verbose):
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)
+
+
+def build(force=False, verbose=False):
+    if force or _stale(LIB, RUNNER_DEPS, ["pacman_recurrence.h", "pacuda_b200.h"]):
+        _run([NVCC] + FLAGS + ["-o", LIB] + [os.path.join(CSRC, s) for s in SOURCES], verbose)
+    if force or _stale(SG_LIB, SG_DEPS, ["pacuda_surrogate.h"]):
+        _run([NVCC] + SG_FLAGS + ["-o", SG_LIB] + [os.path.join(CSRC, s) for s in SG_SOURCES], verbose)
     return LIB
 
 

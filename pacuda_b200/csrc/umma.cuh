@@ -1,0 +1,140 @@
+// Blackwell (sm_100a) tensor-core and bulk-copy primitives for the surrogate network's kernels:
+// tcgen05.mma (kind::f16, BF16 operands, FP32 accumulators in tensor memory), tensor-memory
+// allocation and loads, mbarriers with bounded waits, and bulk (TMA-engine) copies from this
+// GPU's global memory into shared memory. No cluster multicast is used anywhere.
+//
+// Operand layout in shared memory (both A and B, K-major, 128-byte swizzle): a tile of R rows by
+// 64 BF16 values of K is R rows of 128 bytes, its base 1024-byte aligned; the 16-byte chunk j of
+// row r sits at chunk position j ^ (r % 8). A K extent above 64 is a sequence of such tiles. The
+// same bytes laid out in global memory (a "tile image") load with one bulk copy per tile.
+#pragma once
+#include <stdint.h>
+
+namespace pacuda {
+namespace umma {
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// ---- mbarriers ---------------------------------------------------------------------------------
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+// the barriers' initialisation made visible to the async proxy (bulk copies, tensor-core commits)
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// A wait on phase `parity` of `bar` that gives up after about `cycles` SM clock cycles (false).
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, long long cycles) {
+    const long long t0 = clock64();
+    while (!mbar_try_wait(bar, parity))
+        if (clock64() - t0 > cycles) return false;
+    return true;
+}
+
+// ---- bulk copies (global -> shared, completion counted in bytes on an mbarrier) -----------------
+
+// `bytes` a multiple of 16, both addresses 16-byte aligned; `src` in this GPU's global memory
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+// ---- fences --------------------------------------------------------------------------------------
+
+// generic-proxy writes to shared memory made visible to the tensor cores' reads
+__device__ __forceinline__ void fence_async_shared() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// ---- tensor memory -------------------------------------------------------------------------------
+
+// one whole warp: `columns` (a power of two, 32 .. 512) columns of all 128 lanes; the address is
+// written to shared memory at `where`
+__device__ __forceinline__ void tmem_alloc(uint32_t *where, uint32_t columns) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(where)), "r"(columns)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t columns) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(columns) : "memory");
+}
+
+// 32 lanes (one per thread of the warp, from the warp's lane quarter) x 32 consecutive FP32
+// columns from `taddr` (lane in the high 16 bits, column in the low 16)
+__device__ __forceinline__ void tmem_load32(uint32_t taddr, float *v) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+        "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
+          "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+          "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int k = 0; k < 32; k++) v[k] = __uint_as_float(r[k]);
+}
+
+// ---- descriptors and the MMA ---------------------------------------------------------------------
+
+// shared-memory matrix descriptor of a K-major, 128-byte-swizzled operand starting at `addr`
+// (the tile's base 1024-byte aligned; +32 bytes per 16 values of K inside a 64-value row)
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t addr) {
+    uint64_t d = (uint64_t)((addr & 0x3FFFF) >> 4);  // start address, 16-byte units
+    d |= (uint64_t)1 << 16;                           // leading byte offset (unused by this layout)
+    d |= (uint64_t)(1024 >> 4) << 32;                 // stride byte offset: 8 rows of 128 bytes
+    d |= (uint64_t)1 << 46;                           // descriptor version for tcgen05
+    d |= (uint64_t)2 << 61;                           // 128-byte swizzle
+    return d;
+}
+
+// instruction descriptor of kind::f16: A and B BF16, D FP32, both K-major, M x N
+__host__ __device__ constexpr uint32_t idesc_bf16(uint32_t M, uint32_t N) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((N >> 3) << 17) | ((M >> 4) << 24);
+}
+
+// D[tmem] (+)= A * B^T for one K step of 16; issued by one thread
+__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+        "l"(a), "l"(b), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+// the mbarrier gets one arrival when every MMA this thread issued before has completed
+__device__ __forceinline__ void mma_commit(uint64_t *bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+// byte offset of BF16 element (row, k) inside a K-major, 128-byte-swizzled tile of 64 values of K
+__host__ __device__ __forceinline__ uint32_t sw128_offset(uint32_t row, uint32_t k) {
+    return row * 128u + ((((k >> 3) ^ (row & 7u)) << 4) | ((k & 7u) << 1));
+}
+
+}  // namespace umma
+}  // namespace pacuda

@@ -1,0 +1,269 @@
+"""Two-stage unweighting of massless 2 -> 3 subprocesses with the surrogate as its first stage
+(include/pacuda_surrogate.h) and the f64 recurrence runner (include/pacuda_b200.h) as the exact
+second stage; plain unweighting with the runner alone beside it.
+
+Per subprocess ("family"), candidates are seeded points of the unit cube mapped to phase space
+(`oracle/unweight_oracle.py` restates the map, the cuts and the decisions):
+
+* plain: every candidate inside the cuts is evaluated exactly, w = |M|^2 J, and kept when
+  u5 w_max < w, with weight max(1, w / w_max);
+* two-stage: the surrogate s = exp(mu + sigma net(x)) J is evaluated on every candidate (one fused
+  launch: point, cuts, network, decision); the kept ones (u5 s_max < s) are evaluated exactly and
+  kept when u6 r_max < r, r = w / s, with weight max(1, s / s_max) max(1, r / r_max).
+
+With those weights both samples are unbiased estimates of the distribution of w: a kept event's
+expected weight is w / (w_max) (plain) or w / (s_max r_max) (two-stage) for every candidate,
+whatever the surrogate's error; the surrogate only changes how many exact evaluations an event
+costs. The maxima are taken from a pilot sample; a larger weight than the maximum is kept as
+weight above 1 rather than clipped.
+
+The host side here sequences device work: launches of the two libraries, counters read back
+once per step (the number of kept candidates sizes the exact evaluation).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+
+from . import batch as B
+from . import processes
+from . import surrogate as S
+
+FAMILIES = list(processes.PP3J)
+ECM = 13000.0
+
+
+class Cuts(C.Structure):
+    _fields_ = [("pt_min", C.c_double), ("eta_max", C.c_double), ("dr_min", C.c_double)]
+
+
+def _lib():
+    L = S.lib()
+    if not getattr(L, "_uw_bound", False):
+        L.pacuda_uw_candidates.argtypes = [C.c_uint64, C.c_uint64, C.c_uint32, C.c_double, C.c_void_p, C.c_void_p,
+                                           C.c_uint32, C.c_void_p, C.c_void_p]
+        L.pacuda_uw_points.argtypes = [C.c_uint64, C.c_void_p, C.c_uint32, C.c_double, C.c_void_p, C.c_void_p,
+                                       C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p]
+        L.pacuda_uw_decide.argtypes = [C.c_uint64, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p,
+                                       C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_void_p, C.c_void_p,
+                                       C.c_void_p, C.c_void_p]
+        L.pacuda_uw_stage1.argtypes = [C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint32, C.c_double, C.c_void_p,
+                                       C.c_uint32, C.c_double, C.c_double, C.c_double, C.c_void_p, C.c_void_p,
+                                       C.c_uint32, C.c_void_p, C.c_void_p]
+        L._uw_bound = True
+    return L
+
+
+def _ptr(t):
+    return C.c_void_p(t.data_ptr()) if t is not None else None
+
+
+def _check(status, what):
+    if status != 0:
+        raise S.SurrogateError(f"{what} returned {status}")
+
+
+def _stream():
+    import torch
+
+    return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+class Family:
+    """One subprocess: its plan for the runner (f64) and the buffers of its exact evaluations."""
+
+    def __init__(self, name, index, capacity):
+        import torch
+
+        self.name, self.index = name, index
+        self.template = processes.template(name)
+        self.helicities = self.template.outputs
+        self.plan = B.Plan(self.template, "f64")
+        self.capacity = capacity
+        dev = "cuda"
+        self.momenta = torch.empty(5 * 4 * capacity, dtype=torch.float64, device=dev)
+        self.outputs = torch.empty(capacity * self.helicities, dtype=torch.float64, device=dev)
+        self.batch = B.Batch([self.plan], [self.momenta[: 5 * 4 * 1024]], [self.outputs[: 1024 * self.helicities]])
+
+    def exact(self, seed, index, n, sqrt_s):
+        """|M|^2 outputs [n][helicities] of candidates index[:n] (f64 runner, one launch)."""
+        import torch
+
+        if n > self.capacity:
+            raise S.SurrogateError(f"{self.name}: {n} points exceed the capacity {self.capacity}")
+        mom = self.momenta[: 20 * n]
+        _check(_lib().pacuda_uw_points(seed, _ptr(index), n, sqrt_s, _ptr(mom), None, 0, 0, None, _stream()), "points")
+        out = self.outputs[: n * self.helicities]
+        self.batch.update([mom], [n], [out])
+        self.batch.run(torch.cuda.current_stream())
+        return out
+
+
+class Pipeline:
+    """Plain and two-stage unweighting over `families` at sqrt(s) with jet cuts."""
+
+    def __init__(self, families=None, sqrt_s=ECM, cuts=(20.0, 5.0, 0.4), seed=20261204, capacity=1 << 20):
+        import torch
+
+        self.names = list(families or FAMILIES)
+        self.sqrt_s = float(sqrt_s)
+        self.cuts = Cuts(*cuts)
+        self.seed = int(seed)
+        self.inputs = 5 + len(self.names)
+        self.fams = [Family(n, k, capacity) for k, n in enumerate(self.names)]
+        self.index = torch.empty(capacity, dtype=torch.int64, device="cuda")
+        self.kept_s = torch.empty(capacity, dtype=torch.float64, device="cuda")
+        self.counters = torch.zeros(2, dtype=torch.int64, device="cuda")
+        self.jac = torch.empty(capacity, dtype=torch.float64, device="cuda")
+        self.keep = torch.empty(capacity, dtype=torch.uint8, device="cuda")
+        self.weight = torch.empty(capacity, dtype=torch.float64, device="cuda")
+        self.me = torch.empty(capacity, dtype=torch.float64, device="cuda")
+        self.capacity = capacity
+
+    def family_seed(self, k):
+        return (self.seed * 1000003 + 7919 * (k + 1)) & ((1 << 64) - 1)
+
+    # ---- candidates inside the cuts and their exact weights ------------------------------------
+
+    def passing(self, k, first, count):
+        """Indices of the candidates first .. first + count - 1 of family k inside the cuts (sorted)."""
+        import torch
+
+        self.counters.zero_()
+        _check(_lib().pacuda_uw_candidates(self.family_seed(k), first, count, self.sqrt_s, C.byref(self.cuts),
+                                           _ptr(self.index), self.capacity, _ptr(self.counters), _stream()),
+               "candidates")
+        n = int(self.counters[0].item())
+        if n > self.capacity:
+            raise S.SurrogateError(f"{n} passing candidates exceed the capacity {self.capacity}")
+        return torch.sort(self.index[:n])[0]
+
+    def labelled(self, k, first, count):
+        """(inputs [n][inputs] fp32, |M|^2 [n] f64, J [n] f64, index [n]) of the passing candidates."""
+        import torch
+
+        fam = self.fams[k]
+        idx = self.passing(k, first, count)
+        n = idx.numel()
+        x = torch.empty(n, self.inputs, dtype=torch.float32, device="cuda")
+        jac = torch.empty(n, dtype=torch.float64, device="cuda")
+        _check(_lib().pacuda_uw_points(self.family_seed(k), _ptr(idx), n, self.sqrt_s, None, _ptr(x), self.inputs, k,
+                                       _ptr(jac), _stream()), "points")
+        out = fam.exact(self.family_seed(k), idx, n, self.sqrt_s)
+        me = out.view(n, fam.helicities).sum(dim=1)
+        return x, me, jac, idx
+
+    # ---- the two pipelines -------------------------------------------------------------------
+
+    def plain(self, k, first, count, w_max):
+        """Plain unweighting of candidates first .. first + count - 1 of family k: (kept index,
+        weights, exact evaluations)."""
+        fam = self.fams[k]
+        idx = self.passing(k, first, count)
+        n = idx.numel()
+        jac = self.jac[:n]
+        _check(_lib().pacuda_uw_points(self.family_seed(k), _ptr(idx), n, self.sqrt_s, None, None, 0, 0, _ptr(jac),
+                                       _stream()), "points")
+        out = fam.exact(self.family_seed(k), idx, n, self.sqrt_s)
+        _check(_lib().pacuda_uw_decide(self.family_seed(k), _ptr(idx), n, _ptr(out), fam.helicities, _ptr(jac), None,
+                                       w_max, 0.0, 0.0, _ptr(self.keep), _ptr(self.weight), None, _stream()), "decide")
+        keep = self.keep[:n].bool()
+        return idx[keep], self.weight[:n][keep], n
+
+    def two_stage(self, k, net, first, count, mu, sigma, s_max, r_max):
+        """Two-stage unweighting of the same candidates: (kept index, weights, exact evaluations)."""
+        import torch
+
+        fam = self.fams[k]
+        self.counters.zero_()
+        _check(_lib().pacuda_uw_stage1(net.handle, self.family_seed(k), first, count, self.sqrt_s, C.byref(self.cuts),
+                                       k, mu, sigma, s_max, _ptr(self.index), _ptr(self.kept_s), self.capacity,
+                                       _ptr(self.counters), _stream()), "stage 1")
+        n = int(self.counters[0].item())
+        if n > self.capacity:
+            raise S.SurrogateError(f"{n} first-stage events exceed the capacity {self.capacity}")
+        if n == 0:
+            empty = torch.empty(0, dtype=torch.int64, device="cuda")
+            return empty, torch.empty(0, dtype=torch.float64, device="cuda"), 0
+        idx, s = self.index[:n], self.kept_s[:n]
+        jac = self.jac[:n]
+        _check(_lib().pacuda_uw_points(self.family_seed(k), _ptr(idx), n, self.sqrt_s, None, None, 0, 0, _ptr(jac),
+                                       _stream()), "points")
+        out = fam.exact(self.family_seed(k), idx, n, self.sqrt_s)
+        _check(_lib().pacuda_uw_decide(self.family_seed(k), _ptr(idx), n, _ptr(out), fam.helicities, _ptr(jac), _ptr(s),
+                                       0.0, s_max, r_max, _ptr(self.keep), _ptr(self.weight), None, _stream()),
+               "decide")
+        keep = self.keep[:n].bool()
+        return idx[keep].clone(), self.weight[:n][keep].clone(), n
+
+    def surrogate_values(self, net, x, jac, mu, sigma):
+        """s = exp(mu + sigma net(x)) J for points of known inputs (the fused inference kernel)."""
+        out = net.forward(x)
+        return (mu + sigma * out.double()).exp() * jac
+
+
+def train(net, x, y, epochs, batch=16384, lr=2e-3, lr_end=2e-5, seed=0):
+    """Adam on (x, y) for `epochs` passes in shuffled batches (whole batches only), the learning
+    rate falling geometrically from lr to lr_end; returns the mean loss of each epoch."""
+    import torch
+
+    n = (x.shape[0] // batch) * batch
+    steps = epochs * (n // batch)
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(seed)
+    loss = torch.zeros(1, dtype=torch.float32, device="cuda")
+    history = []
+    step = 0
+    for _ in range(epochs):
+        perm = torch.randperm(x.shape[0], device="cuda", generator=gen)[:n]
+        xs, ys = x[perm].contiguous(), y[perm].contiguous()
+        loss.zero_()
+        for b in range(n // batch):
+            rate = lr * (lr_end / lr) ** (step / max(1, steps - 1))
+            net.train_step(xs[b * batch:(b + 1) * batch], ys[b * batch:(b + 1) * batch], rate, loss)
+            step += 1
+        history.append(float(loss.item()) / n)
+    return history
+
+
+def maxima(w, quantile=None):
+    """The maximum used for unweighting: the largest value, or a quantile of the values (a reduced
+    maximum: the few larger ones become events of weight above 1)."""
+    w = w[w > 0]
+    if quantile is None:
+        return float(w.max())
+    return float(np.quantile(w.double().cpu().numpy(), quantile))
+
+
+def chi2_against(weighted_values, weights, event_values, event_weights, edges):
+    """chi^2 and the number of bins between the normalised histogram of unweighted events (with
+    their weights) and that of the weighted sample it estimates (the exact weights of every
+    candidate), with the events' Poisson variance."""
+    ref, _ = np.histogram(weighted_values, bins=edges, weights=weights)
+    ref_var, _ = np.histogram(weighted_values, bins=edges, weights=weights ** 2)
+    ev, _ = np.histogram(event_values, bins=edges, weights=event_weights)
+    ev_var, _ = np.histogram(event_values, bins=edges, weights=event_weights ** 2)
+    rt, et = ref.sum(), ev.sum()
+    var = ev_var / et ** 2 + ref_var / rt ** 2
+    mask = var > 0
+    chi2 = float(((ev / et - ref / rt)[mask] ** 2 / var[mask]).sum())
+    return chi2, int(mask.sum())
+
+
+def observables(p):
+    """Per event: pT of the three final partons' hardest one, its rapidity, and m23 (of legs 3, 4)."""
+    fin = p[:, 2:]
+    pt = np.hypot(fin[..., 1], fin[..., 2])
+    lead = np.argmax(pt, axis=1)
+    rows = np.arange(p.shape[0])
+    eta = np.arcsinh(fin[rows, lead, 3] / pt[rows, lead])
+    q = fin[:, 1] + fin[:, 2]
+    m23 = np.sqrt(np.maximum(0.0, q[:, 0] ** 2 - (q[:, 1:] ** 2).sum(axis=1)))
+    return {"pt_lead": pt[rows, lead], "eta_lead": eta, "m23": m23}
+
+
+def log_edges(v, bins=20):
+    lo, hi = np.quantile(v, 0.01), np.quantile(v, 0.99)
+    return np.concatenate([[-math.inf], np.linspace(lo, hi, bins - 1), [math.inf]])

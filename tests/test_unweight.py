@@ -1,0 +1,97 @@
+"""CPU checks of the unweighting's restatement (oracle/unweight_oracle.py), which the GPU tests
+use as the checker of the device kernels: the five-number phase-space map against RAMBO, the
+jet cuts against the benchmark's, and two-stage unweighting on a toy with a known density."""
+import math
+
+import numpy as np
+import pytest
+
+from oracle import unweight_oracle as U
+from pacuda_b200 import phase_space, unweight
+
+
+def test_map_is_massless_and_conserves_momentum():
+    u = U.uniforms(5, np.arange(4096, dtype=np.uint64))
+    p, jac = U.phase_space(u, 13000.0)
+    assert np.allclose(p[:, :, 0] ** 2 - (p[:, :, 1:] ** 2).sum(axis=2), 0.0, atol=1e-6 * 13000.0 ** 2 * 1e-6)
+    assert np.allclose(p[:, :2].sum(axis=1), p[:, 2:].sum(axis=1), atol=1e-8 * 13000.0)
+    assert np.all(p[:, 2:, 0] >= 0) and np.all(jac >= 0)
+
+
+def test_map_volume_and_distributions_match_rambo():
+    """The map's weight integrates to the massless three-body volume s / (256 pi^3), RAMBO's
+    constant weight, and the weighted distributions of symmetric observables (every final
+    parton's energy, every pair's invariant mass) equal RAMBO's flat ones."""
+    sqrt_s, n = 1000.0, 1 << 18
+    s = sqrt_s * sqrt_s
+    vol = s / (256.0 * math.pi ** 3)
+    u = U.uniforms(11, np.arange(n, dtype=np.uint64))
+    p, jac = U.phase_space(u, sqrt_s)
+    assert jac.mean() == pytest.approx(vol, rel=5e-3)
+    r = phase_space.rambo(5, n, 12, ecm=sqrt_s)
+
+    def obs(q):  # point-major: [point][3] flattened
+        e = q[:, 2:, 0].reshape(-1)
+        m = []
+        for i, j in ((2, 3), (2, 4), (3, 4)):
+            k = q[:, i] + q[:, j]
+            m.append(np.sqrt(np.maximum(0.0, k[:, 0] ** 2 - (k[:, 1:] ** 2).sum(axis=1))))
+        return e, np.stack(m, axis=1).reshape(-1)
+
+    for a, b in zip(obs(p), obs(r)):
+        edges = np.linspace(0, max(a.max(), b.max()), 21)
+        wa = np.repeat(jac, 3)
+        ha, _ = np.histogram(a, edges, weights=wa)
+        va, _ = np.histogram(a, edges, weights=wa ** 2)
+        hb, _ = np.histogram(b, edges)
+        hb = hb * vol
+        vb = hb * vol
+        chi2 = ((ha - hb) ** 2 / (va + vb + 1e-300))[hb > 0].sum()
+        assert chi2 / 20 < 3.0, chi2
+
+
+def test_cuts_agree_with_the_benchmark_cuts():
+    u = U.uniforms(3, np.arange(20000, dtype=np.uint64))
+    p, _ = U.phase_space(u, 13000.0)
+    ok = U.passes(p)
+    assert 0.2 < ok.mean() < 1.0
+    assert np.array_equal(ok, phase_space.passes_cuts(p))
+
+
+def test_uniform_stream_matches_the_generator_construction():
+    """Uniform k of candidate i is draw k of the per-point stream pacuda_b200.phase_space.rambo
+    uses (the same seeding and xorshift), so the two generators share one construction."""
+    u = U.uniforms(99, np.arange(8, dtype=np.uint64))
+    assert u.shape == (8, 7) and np.all((u > 0) & (u < 1))
+    assert len(np.unique(u)) == u.size
+
+
+def test_two_stage_toy_is_unbiased():
+    """With a surrogate off by up to 20 % the two-stage events, with their weights, follow the
+    exact density as the plain events do (chi^2 per bin near 1), and each exact evaluation
+    gives several times more events."""
+    x, f, (xp, wp), (x2, w2) = U.toy_two_stage(1 << 21, 7)
+    edges = np.linspace(0, 1, 21)
+    for axis in (0, 1):
+        for xs, ws in ((xp, wp), (x2, w2)):
+            chi2, bins = unweight.chi2_against(x[:, axis], f, xs[:, axis], ws, edges)
+            assert chi2 / bins < 2.0, (axis, chi2, bins)
+    # events per exact evaluation: plain = kept / all, two-stage = kept / first-stage survivors
+    eff_plain = len(xp) / len(x)
+    s = f * (1.0 + 0.2 * np.sin(7.0 * x[:, 0]) * np.cos(5.0 * x[:, 1]))
+    first = (np.random.default_rng(7).uniform(size=(4, len(x)))[2] * s.max() * 0.9 < s).sum()
+    assert len(x2) / max(1, first) > 2 * eff_plain
+
+
+def test_two_stage_toy_detects_a_biased_rule():
+    """The chi^2 check has power: events of the first stage alone (the surrogate's distribution,
+    no exact second stage) differ visibly from the density when the surrogate is 30 % off."""
+    rng = np.random.default_rng(8)
+    n = 1 << 21
+    x = rng.uniform(size=(n, 2))
+    f = np.exp(-((x[:, 0] - 0.3) ** 2 + (x[:, 1] - 0.6) ** 2) / 0.02) + 0.2
+    s = f * (1.0 + 0.3 * np.sin(7.0 * x[:, 0]) * np.cos(5.0 * x[:, 1]))
+    keep = U.stage1_decide(s, rng.uniform(size=n), s.max())
+    edges = np.linspace(0, 1, 21)
+    chi2_bad, bins = unweight.chi2_against(x[:, 0], f, x[keep, 0], np.ones(keep.sum()), edges)
+    assert chi2_bad > 10 * bins
