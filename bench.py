@@ -210,6 +210,148 @@ def precision_line(torch, B, fams, ext, ref_out, steps, warmup, kind="mixed"):
             "blocks_per_sm": {nm: batch.plan_blocks_per_sm(k) for k, (nm, _, _) in enumerate(fams)}}
 
 
+def surrogate_line(torch, train_points=1 << 22, candidates=1 << 22, epochs=10, batch=16384, steps=3, check=2048):
+    """The learned part: a surrogate of log |M|^2 per p p -> 3 jets subprocess (one network, the
+    five unit-cube numbers and a subprocess one-hot as inputs, 4 x 256 SiLU, BF16 tensor-core
+    products), trained by this library's kernels on `train_points` points labelled by the f64
+    recurrence, then two-stage unweighting of `candidates` seeded candidates (split over the
+    families as the benchmark's points are) against plain unweighting of the same candidates
+    with the f64 runner alone. Reports the training, the surrogate's relative errors on held-out
+    points, both pipelines' efficiencies and unweighted events/s (device time, CUDA events around
+    each step, the host's reads of the kept counts inside), the events' agreement with the exact
+    weighted distribution (chi^2 per bin of three observables), and the fused first-stage
+    kernel's tensor throughput."""
+    from pacuda_b200 import surrogate as S
+    from pacuda_b200 import unweight as UW
+
+    fams = list(FAMILIES)
+    counts = split_points(candidates, SEED)
+    train_counts = split_points(train_points, SEED + 1)
+    pl = UW.Pipeline(families=fams, capacity=max(max(counts), max(train_counts)) + 1024)
+    res = {"workload": f"pp>3j LC: {', '.join(fams)}; 13 TeV, pT>20 GeV, |eta|<5, dR>0.4; network 4 x 256 SiLU, "
+                       f"inputs 5 + {len(fams)} one-hot; {train_points} labelled candidates, {candidates} unweighted",
+           "candidates_per_family": dict(zip(fams, counts))}
+    # labels: the f64 recurrence on the passing candidates of a training stream (candidates from 2^40 on)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    data = [pl.labelled(k, 1 << 40, c) for k, c in enumerate(train_counts)]
+    e1.record()
+    e1.synchronize()
+    label_ms = e0.elapsed_time(e1)
+    x = torch.cat([d[0] for d in data])
+    me = torch.cat([d[1] for d in data])
+    jac = torch.cat([d[2] for d in data])
+    logm = me.log()
+    mu, sigma = float(logm.mean()), float(logm.std())
+    y = ((logm - mu) / sigma).float()
+    held = torch.randperm(x.shape[0], device="cuda", generator=torch.Generator(device="cuda").manual_seed(5))
+    n_hold = 1 << 16
+    hx, hy, hme, hjac = x[held[:n_hold]], y[held[:n_hold]], me[held[:n_hold]], jac[held[:n_hold]]
+    tx, ty = x[held[n_hold:]].contiguous(), y[held[n_hold:]].contiguous()
+    net = S.Network(pl.inputs, max_batch=batch, seed=7)
+    e0.record()
+    hist = UW.train(net, tx, ty, epochs=epochs, batch=batch, lr=2e-3, lr_end=2e-5)
+    e1.record()
+    e1.synchronize()
+    train_ms = e0.elapsed_time(e1)
+    if net.error():
+        raise RuntimeError(f"surrogate kernels reported error {net.error()}")
+    pred = net.forward(hx)
+    rel = ((mu + sigma * pred.double()).exp() / hme - 1.0).abs().cpu().numpy()
+    res["training"] = {"points": int(tx.shape[0]), "epochs": epochs, "batch": batch, "loss_per_epoch": hist,
+                       "label_ms": label_ms, "train_ms": train_ms,
+                       "train_steps": epochs * (tx.shape[0] // batch),
+                       "held_out_points": n_hold,
+                       "surrogate_rel_error": {q: float(np.quantile(rel, float(q))) for q in ("0.5", "0.9", "0.99")}}
+    # maxima from the labelled sample, per family
+    maxima = []
+    start = 0
+    for k, d in enumerate(data):
+        n = d[0].shape[0]
+        w = d[1] * d[2]
+        sv = pl.surrogate_values(net, d[0], d[2], mu, sigma)
+        maxima.append((UW.maxima(w), UW.maxima(sv), UW.maxima(w / sv, 0.999)))
+        start += n
+    del data, x, me, jac, tx, ty
+    # the two pipelines on the same candidates (stream from 0), timed per step
+    first = 0
+
+    def run(kind):
+        kept, exact, events_w = 0, 0, []
+        out = []
+        for k, c in enumerate(counts):
+            w_max, s_max, r_max = maxima[k]
+            if kind == "plain":
+                idx, wts, ne = pl.plain(k, first, c, w_max)
+            else:
+                idx, wts, ne = pl.two_stage(k, net, first, c, mu, sigma, s_max, r_max)
+            kept += idx.numel()
+            exact += ne
+            out.append((idx, wts))
+        return kept, exact, out
+
+    lines = {}
+    for kind in ("plain", "two_stage"):
+        run(kind)  # warm-up (and the batch plans' first launches)
+        e0.record()
+        for _ in range(steps):
+            kept, exact, out = run(kind)
+        e1.record()
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        lines[kind] = {"ms_per_step": ms, "events": kept, "exact_evaluations": exact,
+                       "events_per_s": kept / (ms * 1e-3), "candidates_per_s": candidates / (ms * 1e-3),
+                       "efficiency_per_exact": kept / max(1, exact), "efficiency_per_candidate": kept / candidates,
+                       "overweight_events": int(sum(int((w > 1).sum()) for _, w in out))}
+        lines[kind]["_events"] = out
+    res["plain"] = {k: v for k, v in lines["plain"].items() if not k.startswith("_")}
+    res["two_stage"] = {k: v for k, v in lines["two_stage"].items() if not k.startswith("_")}
+    res["events_per_s_ratio"] = lines["two_stage"]["events_per_s"] / lines["plain"]["events_per_s"]
+    res["exact_error"] = ("0: the kept events' |M|^2 and weights come from the f64 runner (bit for bit the reference "
+                          "runner's f64 arithmetic); the surrogate only decides which candidates are evaluated")
+    # unbiasedness: each sample's histograms against the exact weighted distribution of all candidates
+    from oracle import unweight_oracle as UO
+
+    chi = {}
+    for k, name in enumerate(fams):
+        seed = pl.family_seed(k)
+        idx_all = pl.passing(k, first, counts[k])
+        _, ma, ja, _ = pl.labelled(k, first, counts[k])
+        wa = (ma * ja).cpu().numpy()
+
+        def moms(index):
+            u = UO.uniforms(seed, index.cpu().numpy().astype(np.uint64))
+            return UO.phase_space(u, ECM)[0]
+
+        ref = UW.observables(moms(idx_all))
+        for kind in ("plain", "two_stage"):
+            idx, wts = lines[kind]["_events"][k]
+            ev = UW.observables(moms(idx))
+            for obs in ref:
+                edges = UW.log_edges(ref[obs], 16)
+                c2, bins = UW.chi2_against(ref[obs], wa, ev[obs], wts.cpu().numpy(), edges)
+                chi.setdefault(kind, {}).setdefault(name, {})[obs] = round(c2 / max(1, bins), 3)
+    res["chi2_per_bin_vs_exact"] = chi
+    # the fused first stage alone: tensor throughput (algorithmic flops of the network per candidate)
+    flops = 2 * (64 * 256 + 3 * 256 * 256 + 256)
+    k0 = int(np.argmax(counts))
+    w_max, s_max, r_max = maxima[k0]
+    e0.record()
+    for _ in range(steps):
+        pl.counters.zero_()
+        S.lib()  # bound
+        UW._check(UW._lib().pacuda_uw_stage1(net.handle, pl.family_seed(k0), first, counts[k0], pl.sqrt_s,
+                                             UW.C.byref(pl.cuts), k0, mu, sigma, s_max, UW._ptr(pl.index),
+                                             UW._ptr(pl.kept_s), pl.capacity, UW._ptr(pl.counters), UW._stream()),
+                  "stage 1")
+    e1.record()
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    res["stage1_kernel"] = {"candidates": counts[k0], "ms": ms, "candidates_per_s": counts[k0] / (ms * 1e-3),
+                            "flops_per_candidate": flops, "tflops": counts[k0] * flops / (ms * 1e-3) / 1e12}
+    return res
+
+
 def oracle_parity(cases):
     """Bitwise parity of device outputs with the oracle: cases (label, template, point-major
     momenta, device outputs [point][helicity])."""
@@ -607,6 +749,8 @@ def main():
     ap.add_argument("--no-precision", action="store_true", help="skip the mixed-precision lines")
     ap.add_argument("--blocks-per-sm", type=int, default=0, help="1, 2, 3, 4, 5, 8 or 16 (with --no-tune or --lanes-per-point)")
     ap.add_argument("--no-reference-gpu", action="store_true", help="skip timing the reference's own GPU runner")
+    ap.add_argument("--no-surrogate", action="store_true", help="skip the surrogate and two-stage unweighting line")
+    ap.add_argument("--surrogate-only", action="store_true", help="only the surrogate line (development runs)")
     ap.add_argument("--reference-gpu-kind", default=None, help=argparse.SUPPRESS)  # the worker of reference_gpu()
     ap.add_argument("--keep", default=None, help=argparse.SUPPRESS)
     args = ap.parse_args()
@@ -651,6 +795,9 @@ def main():
     from pacuda_b200 import build
 
     build.build()
+    if args.surrogate_only:
+        print(json.dumps({"surrogate": surrogate_line(torch)}))
+        return
     if world > 1:
         import datetime
 
@@ -780,6 +927,8 @@ def main():
                                 for k in ("mixed", "mixed64", "df64")]
             res["precision_gg4g"] = six_gluon_line(torch, B)
             res["pp4j"] = pp4j_line(torch, B)
+        if not args.no_surrogate:
+            res["surrogate"] = surrogate_line(torch)
     if world > 1:
         import torch.distributed as dist
 

@@ -35,10 +35,16 @@ enum { PACUDA_B200_EXECUTOR_AUTO = 0, PACUDA_B200_EXECUTOR_ARENA = 1, PACUDA_B20
 typedef struct pacuda_b200_plan pacuda_b200_plan;
 typedef struct pacuda_b200_batch pacuda_b200_batch;
 
+/* A kernel kind of this API beside the reference's four (PACMAN_RECURRENCE_KERNEL_*): the f64
+ * arithmetic with each product and the sum it feeds fused into one multiply-add (one rounding
+ * instead of two). Not bit for bit the reference's f64 kernel; within about 1e-13 of it. */
+#define PACUDA_B200_KERNEL_F64_FMA 4
+
 /* Compiles the plan of `call` (its words, widths, plane counts, scales, factors and form terms;
  * its arrays and runs are not used) with the reduction (offsets[outputs + 1], planes, weights)
- * for the kernel kind `kernel` (PACMAN_RECURRENCE_KERNEL_*). NULL on error, with a message on
- * stderr. The plan may read no current plane before writing it (its inputs are its sources). */
+ * for the kernel kind `kernel` (PACMAN_RECURRENCE_KERNEL_* or PACUDA_B200_KERNEL_F64_FMA). NULL
+ * on error, with a message on stderr. The plan may read no current plane before writing it (its
+ * inputs are its sources). */
 pacuda_b200_plan *pacuda_b200_plan_create(const pacman_recurrence_call *call, const uint32_t *offsets,
                                           const uint32_t *planes, const double *weights, uint32_t outputs,
                                           uint32_t kernel);

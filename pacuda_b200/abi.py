@@ -16,6 +16,8 @@ OUTPUT_ZERO = 1
 OK, INVALID, DEVICE_ERROR = 0, 2, 3
 KERNEL_DF64, KERNEL_F64, KERNEL_MIXED, KERNEL_MIXED64 = 0, 1, 2, 3
 KERNELS = {"df64": KERNEL_DF64, "f64": KERNEL_F64, "mixed": KERNEL_MIXED, "mixed64": KERNEL_MIXED64}
+KERNEL_F64_FMA = 4  # the batched API's f64 kind with contracted multiply-adds (include/pacuda_b200.h)
+BATCH_KERNELS = dict(KERNELS, f64fma=KERNEL_F64_FMA)
 CAP_SOURCES, CAP_FORMS, CAP_SYMJIT = 1, 2, 4
 W_P, W_A, W_F, W_X, W_S, W_K = range(6)
 

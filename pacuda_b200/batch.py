@@ -49,7 +49,7 @@ class Plan:
 
     def __init__(self, template, kernel="f64"):
         self.template = template
-        k = abi.KERNELS[kernel] if isinstance(kernel, str) else int(kernel)
+        k = abi.BATCH_KERNELS[kernel] if isinstance(kernel, str) else int(kernel)
         args = template.call(np.zeros(4 * template.external_count), 1)
         self._keep = (np.ascontiguousarray(template.offsets, dtype=np.uint32),
                       np.ascontiguousarray(template.planes, dtype=np.uint32),

@@ -28,7 +28,7 @@ SG_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-shared", 
             "-Xptxas", "-warn-spills"] + ARCH
 
 RUNNER_DEPS = ["runner.cu", "batch.cu", "program.cpp", "program.h", "schedule.cpp", "schedule.h", "tiled_host.cu",
-               "tiled_host.h", "peak.cu", "arith.cuh", "executor.cuh", "tiled.cuh"]
+               "tiled_host.h", "peak.cu", "arith.cuh", "executor.cuh", "tiled.cuh", "tiled_fma.cu"]
 SG_DEPS = ["surrogate.cu", "umma.cuh"]
 
 
@@ -53,7 +53,12 @@ def _run(cmd, verbose):
 
 def build(force=False, verbose=False):
     if force or _stale(LIB, RUNNER_DEPS, ["pacman_recurrence.h", "pacuda_b200.h"]):
-        _run([NVCC] + FLAGS + ["-o", LIB] + [os.path.join(CSRC, s) for s in SOURCES], verbose)
+        # the f64 kind with contracted multiply-adds: the same executor compiled with -fmad=true
+        obj = os.path.join(CSRC, "..", "tiled_fma.o")
+        _run([NVCC] + [f if f != "-fmad=false" else "-fmad=true" for f in FLAGS if f not in ("-shared",)] +
+             ["-c", "-o", obj, os.path.join(CSRC, "tiled_fma.cu")], verbose)
+        _run([NVCC] + FLAGS + ["-o", LIB] + [os.path.join(CSRC, s) for s in SOURCES] + [obj], verbose)
+        os.unlink(obj)
     if force or _stale(SG_LIB, SG_DEPS, ["pacuda_surrogate.h"]):
         _run([NVCC] + SG_FLAGS + ["-o", SG_LIB] + [os.path.join(CSRC, s) for s in SG_SOURCES], verbose)
     return LIB

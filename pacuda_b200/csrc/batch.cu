@@ -246,7 +246,7 @@ extern "C" pacuda_b200_plan *pacuda_b200_plan_create(const pacman_recurrence_cal
                                                      const uint32_t *planes, const double *weights, uint32_t outputs,
                                                      uint32_t kernel) {
     if (!c || c->abi_version != PACMAN_RECURRENCE_ABI || c->struct_size != sizeof(pacman_recurrence_call) ||
-        !c->words || kernel > PACMAN_RECURRENCE_KERNEL_MIXED64 || !offsets || (offsets[outputs] && (!planes || !weights)) ||
+        !c->words || (kernel > PACMAN_RECURRENCE_KERNEL_MIXED64 && kernel != PACUDA_B200_KERNEL_F64_FMA) || !offsets || (offsets[outputs] && (!planes || !weights)) ||
         (c->scale_count && (!c->scale_re || !c->scale_im)) || (c->factor_count && (!c->factor_re || !c->factor_im)) ||
         !c->form_terms || (c->term_count && (!c->term_slots || !c->term_coefficients))) {
         fprintf(stderr, "%s: plan_create: an invalid call description\n", kTag);
@@ -303,7 +303,7 @@ extern "C" pacuda_b200_plan *pacuda_b200_plan_create(const pacman_recurrence_cal
     double *f = k.data() + 2 * c->scale_count;
     for (uint32_t i = 0; i < c->factor_count; i++) { f[i] = c->factor_re[i]; f[c->factor_count + i] = c->factor_im[i]; }
     for (size_t i = 0; i < nc; i++) {
-        if (kernel == PACMAN_RECURRENCE_KERNEL_F64) {
+        if (kernel == PACMAN_RECURRENCE_KERNEL_F64 || kernel == PACUDA_B200_KERNEL_F64_FMA) {
             k[nc + i] = k[i];
         } else {
             float hi = (float)k[i], lo = (float)(k[i] - (double)hi);

@@ -4,6 +4,7 @@
 #include <algorithm>
 
 #include "../../include/pacman_recurrence.h"
+#include "../../include/pacuda_b200.h"
 #include "tiled.cuh"
 #include "tiled_host.h"
 
@@ -16,6 +17,13 @@ template <class T> bool put(T **dst, const std::vector<T> &v, cudaStream_t s) {
     return v.empty() || cudaMemcpyAsync(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s) == cudaSuccess;
 }
 
+}  // namespace
+
+// the f64 kind with contracted multiply-adds (tiled_fma.cu, compiled with -fmad=true)
+const void *tiled_fma_kernel(bool abi);
+
+namespace {
+
 template <class K> const void *kernel_of(bool abi) {
     return abi ? (const void *)run_tiled<K, true> : (const void *)run_tiled<K, false>;
 }
@@ -23,6 +31,7 @@ template <class K> const void *kernel_of(bool abi) {
 const void *kernel_for(int kernel, bool abi = false) {
     switch (kernel) {
     case PACMAN_RECURRENCE_KERNEL_F64: return kernel_of<KindF64>(abi);
+    case PACUDA_B200_KERNEL_F64_FMA: return tiled_fma_kernel(abi);
     case PACMAN_RECURRENCE_KERNEL_MIXED: return kernel_of<KindMixed>(abi);
     case PACMAN_RECURRENCE_KERNEL_MIXED64: return kernel_of<KindMixed64>(abi);
     default: return kernel_of<KindDF64>(abi);

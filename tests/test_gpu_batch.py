@@ -190,3 +190,27 @@ def test_six_gluon_parts_match_oracle_bitwise(kind):
     b.run()
     torch.cuda.synchronize()
     check(out, want)
+
+
+@pytest.mark.gpu
+def test_fma_kind_within_1e13_of_the_oracle():
+    """The batched API's f64 kind with contracted multiply-adds: every point's |M|^2 (the sum of
+    its helicity outputs) within 1e-13 relative of the f64 oracle, each helicity output within
+    1e-13 of the point's largest; and not the same bits everywhere (the contraction happened)."""
+    from pacuda_b200 import batch as B
+    import torch
+
+    counts = [300, 200, 200, 100]
+    plans, ext, out, want = setup("f64", counts)
+    fma = [B.Plan(p.template, "f64fma") for p in plans]
+    b = B.Batch(fma, ext, out)
+    b.run()
+    torch.cuda.synchronize()
+    differ = 0
+    for o, w in zip(out, want):
+        got = o.cpu().numpy().reshape(w.shape)
+        tot_g, tot_w = got.sum(axis=1), w.sum(axis=1)
+        assert np.all(np.abs(tot_g - tot_w) <= 1e-13 * np.abs(tot_w))
+        assert np.all(np.abs(got - w) <= 1e-13 * np.abs(w).max(axis=1, keepdims=True))
+        differ += int((got.view(np.uint64) != w.view(np.uint64)).sum())
+    assert differ > 0
