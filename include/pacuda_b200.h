@@ -112,6 +112,25 @@ void pacuda_b200_batch_destroy(pacuda_b200_batch *batch);
 int pacuda_b200_run_static(pacuda_b200_plan *const *plans, uint32_t nplans, const double *const *external,
                            const uint32_t *count, double *const *output, void *stream);
 
+/* The rotated-momentum stability check's device steps (no counterpart in the reference).
+ * rotate: source-major momenta [(leg * 4 + k) * n + i] of n points with every leg's spatial part
+ * turned by the row-major 3x3 `rotation` (host array), energies kept, into `out`.
+ * compare: the helicity sums over `parts` output arrays a[k] and b[k] ([i][outputs[k]] each; the
+ * pointer arrays and `outputs` in device memory); a point whose sums differ by more than `tol`
+ * relative, or are not finite, is appended (in no particular order) to index[], *count (zeroed by
+ * the caller) counting them.
+ * gather: the momenta of points index[0 .. *count) into `out` (source-major with stride *count);
+ * scatter: their outputs src[j][outputs] back into dst[index[j]][outputs]; both launch for up to
+ * `capacity` points and read the count on the device. */
+int pacuda_b200_rotate(const double *external, uint32_t legs, uint32_t n, const double *rotation, double *out,
+                       void *stream);
+int pacuda_b200_compare(const double *const *a, const double *const *b, const uint32_t *outputs, uint32_t parts,
+                        uint32_t n, double tol, uint32_t *index, uint32_t *count, void *stream);
+int pacuda_b200_gather(const double *external, uint32_t legs, uint32_t n, const uint32_t *index, const uint32_t *count,
+                       uint32_t capacity, double *out, void *stream);
+int pacuda_b200_scatter(const double *src, uint32_t outputs, const uint32_t *index, const uint32_t *count,
+                        uint32_t capacity, double *dst, void *stream);
+
 /* Measurement: launches blocks x threads threads that each run 8 independent chains of
  * `iterations` f64 fused multiply-adds (2 flops each) on `stream`; the caller times it. `sink`
  * is a device array of at least *blocks doubles (never written in practice). */

@@ -19,7 +19,7 @@ INCLUDE = os.path.join(HERE, "..", "include")
 LIB = os.path.join(HERE, "librecurrence.so")
 SG_LIB = os.path.join(HERE, "libsurrogate.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
-SOURCES = ["runner.cu", "batch.cu", "program.cpp", "schedule.cpp", "tiled_host.cu", "peak.cu"]
+SOURCES = ["runner.cu", "batch.cu", "program.cpp", "schedule.cpp", "tiled_host.cu", "peak.cu", "stability.cu"]
 SG_SOURCES = ["surrogate.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-fmad=false", "-lineinfo", "-Xcompiler", "-fPIC", "-shared", "-cudart", "static",
@@ -28,7 +28,7 @@ SG_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-shared", 
             "-Xptxas", "-warn-spills"] + ARCH
 
 RUNNER_DEPS = ["runner.cu", "batch.cu", "program.cpp", "program.h", "schedule.cpp", "schedule.h", "tiled_host.cu",
-               "tiled_host.h", "peak.cu", "arith.cuh", "executor.cuh", "tiled.cuh", "tiled_fma.cu"]
+               "tiled_host.h", "peak.cu", "arith.cuh", "executor.cuh", "tiled.cuh", "tiled_fma.cu", "stability.cu"]
 SG_DEPS = ["surrogate.cu", "umma.cuh"]
 
 

@@ -75,3 +75,28 @@ def test_points_carry_mixed_or_f64_bits_as_their_check_decides(process, tol):
             assert np.array_equal(got.view(np.uint64), want.view(np.uint64)), repeat
     if tol == 0.0:
         assert m > n // 2  # two f32 evaluations rarely agree to the bit
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("tol", [1e-6, 1e-5])
+def test_kept_points_are_within_ten_tolerances_of_f64(tol):
+    """The points the check keeps in mixed precision: their |M|^2 within 10 tol of f64 (the check
+    estimates a point's error from two evaluations that round alike; it is not a bound, so the
+    margin is stated and tested), and a tolerance below the floor sends every point to f64."""
+    import torch
+
+    templates, p, ext = _setup([processes.template("gg>ggg")], 2000, 31)
+    f64 = _reference_outputs(templates, ext, 2000, "f64")[0].sum(axis=1)
+    s = stability.StableMixed(templates, 2000, tol)
+    outs, m = s.run(ext)
+    torch.cuda.synchronize()
+    got = outs[0].cpu().numpy().reshape(2000, -1).sum(axis=1)
+    kept = ~s.unstable.cpu().numpy()
+    rel = np.abs(got - f64) / np.abs(f64)
+    assert kept.sum() > 0
+    assert np.all(rel[kept] <= 10 * tol), (rel[kept].max(), tol)
+    low = stability.StableMixed(templates, 2000, stability.FLOOR / 10)
+    outs, m = low.run(ext)
+    torch.cuda.synchronize()
+    assert m == 2000
+    assert np.array_equal(outs[0].cpu().numpy().reshape(2000, -1).sum(axis=1), f64)
