@@ -42,6 +42,7 @@ POINTS = 1 << 20
 ECM = 13000.0
 SEED = 20261203
 TILE = 1 << 16
+OVERWEIGHT = 1e-3  # reduced unweighting maxima: at most this share of the total above them
 
 
 def split_points(total, seed):
@@ -270,7 +271,8 @@ def surrogate_line(torch, train_points=1 << 22, candidates=1 << 22, epochs=10, b
         n = d[0].shape[0]
         w = d[1] * d[2]
         sv = pl.surrogate_values(net, d[0], d[2], mu, sigma)
-        maxima.append((UW.maxima(w), UW.maxima(sv), UW.maxima(w / sv, 0.999)))
+        maxima.append((UW.maxima(w, overweight=OVERWEIGHT), UW.maxima(sv, overweight=OVERWEIGHT),
+                       UW.maxima(w / sv, sv, overweight=OVERWEIGHT)))
         start += n
     del data, x, me, jac, tx, ty
     # the two pipelines on the same candidates (stream from 0), timed per step
@@ -349,6 +351,45 @@ def surrogate_line(torch, train_points=1 << 22, candidates=1 << 22, epochs=10, b
     ms = e0.elapsed_time(e1) / steps
     res["stage1_kernel"] = {"candidates": counts[k0], "ms": ms, "candidates_per_s": counts[k0] / (ms * 1e-3),
                             "flops_per_candidate": flops, "tflops": counts[k0] * flops / (ms * 1e-3) / 1e12}
+    return res
+
+
+def surrogate_kernels(torch, count=1 << 21, steps=5):
+    """The surrogate's kernels alone on a random network (a small, self-contained case for
+    profiling): the fused inference kernel on `count` points of given inputs, and the fused first
+    stage on `count` candidates; time per launch and tensor throughput (algorithmic flops of the
+    network per point: 2 (64 x 256 + 3 x 256 x 256 + 256))."""
+    from pacuda_b200 import surrogate as S
+    from pacuda_b200 import unweight as UW
+
+    flops = 2 * (64 * 256 + 3 * 256 * 256 + 256)
+    net = S.Network(9, max_batch=1024, seed=3)
+    x = torch.rand(count, 9, device="cuda")
+    out = torch.empty(count, device="cuda")
+    pl = UW.Pipeline(families=FAMILIES, capacity=count)
+    res = {}
+    for what in ("forward", "stage1"):
+        def launch():
+            if what == "forward":
+                net.forward(x, out)
+            else:
+                pl.counters.zero_()
+                UW._check(UW._lib().pacuda_uw_stage1(net.handle, 11, 0, count, ECM, UW.C.byref(pl.cuts), 0, -3.0, 1.0,
+                                                     1e30, UW._ptr(pl.index), UW._ptr(pl.kept_s), pl.capacity,
+                                                     UW._ptr(pl.counters), UW._stream()), "stage 1")
+        for _ in range(2):
+            launch()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            launch()
+        e1.record()
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        res[what] = {"points": count, "ms": ms, "points_per_s": count / (ms * 1e-3),
+                     "tflops": count * flops / (ms * 1e-3) / 1e12}
+    if net.error():
+        raise RuntimeError(f"surrogate kernels reported error {net.error()}")
     return res
 
 
@@ -583,12 +624,12 @@ def e2e_abi(fams, steps, warmup, lib=None, kernel="f64", events=None):
             outp = r.lib.pacman_recurrence_v1_host_alloc(8 * m * t.outputs)
             out = np.ctypeslib.as_array((C.c_double * (m * t.outputs)).from_address(outp))
             red, keep = abi.reduce_resolved_args(t.planes, t.weights, t.offsets, out, m, 1, t.outputs, abi.OUTPUT_ZERO)
-            jobs.append((args, red, keep, out))
+            jobs.append((args, red, keep, out, name))
             h2d += ext.nbytes
             d2h += out.nbytes
 
     def step():
-        for args, red, keep, out in jobs:
+        for args, red, keep, out, _ in jobs:
             if r.run(args) != 0 or r.reduce_resolved(red) != 0:
                 raise RuntimeError("runner call failed")
 
@@ -610,7 +651,7 @@ def e2e_abi(fams, steps, warmup, lib=None, kernel="f64", events=None):
         ms = events[0].elapsed_time(events[1]) / steps
         res["device_value"] = total / (ms * 1e-3)
         res["device_ms_per_step"] = ms
-    return res, [j[3] for j in jobs]
+    return res, [(j[4], j[3]) for j in jobs]  # (family, outputs) per tile, the families' tiles in order
 
 
 REF_LIB = os.path.join(ROOT, "oracle", "_ref", "librecurrence.so")
@@ -633,8 +674,10 @@ def reference_gpu_worker(kind, steps, warmup, keep_path):
     line["kernel"] = kind
     if keep_path:
         first = {}
-        for (name, t, p), o in zip(fams, outs):
+        tmpl = {name: (t, p) for name, t, p in fams}
+        for name, o in outs:  # a family's first tile holds its first points
             if name not in first:
+                t, p = tmpl[name]
                 first[name] = np.array(o[: min(2048, p.shape[0]) * t.outputs]).reshape(-1, t.outputs)
         np.savez(keep_path, **first)
     print(json.dumps(line))
@@ -751,6 +794,8 @@ def main():
     ap.add_argument("--no-reference-gpu", action="store_true", help="skip timing the reference's own GPU runner")
     ap.add_argument("--no-surrogate", action="store_true", help="skip the surrogate and two-stage unweighting line")
     ap.add_argument("--surrogate-only", action="store_true", help="only the surrogate line (development runs)")
+    ap.add_argument("--surrogate-kernels", action="store_true", help="only the surrogate kernels on a random network "
+                                                                      "(the profiling case)")
     ap.add_argument("--reference-gpu-kind", default=None, help=argparse.SUPPRESS)  # the worker of reference_gpu()
     ap.add_argument("--keep", default=None, help=argparse.SUPPRESS)
     args = ap.parse_args()
@@ -795,6 +840,9 @@ def main():
     from pacuda_b200 import build
 
     build.build()
+    if args.surrogate_kernels:
+        print(json.dumps({"surrogate_kernels": surrogate_kernels(torch)}))
+        return
     if args.surrogate_only:
         print(json.dumps({"surrogate": surrogate_line(torch)}))
         return

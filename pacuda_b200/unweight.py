@@ -228,13 +228,28 @@ def train(net, x, y, epochs, batch=16384, lr=2e-3, lr_end=2e-5, seed=0):
     return history
 
 
-def maxima(w, quantile=None):
-    """The maximum used for unweighting: the largest value, or a quantile of the values (a reduced
-    maximum: the few larger ones become events of weight above 1)."""
-    w = w[w > 0]
-    if quantile is None:
-        return float(w.max())
-    return float(np.quantile(w.double().cpu().numpy(), quantile))
+def maxima(values, weights=None, overweight=1e-3):
+    """A reduced maximum for unweighting: the smallest threshold t such that the part of the
+    total above it, sum(weights * max(0, values - t)), is at most `overweight` of
+    sum(weights * values) (weights default to 1). Values above t become events of weight above 1
+    (kept, not clipped), so the choice sets the efficiency, not the result; overweight=0 gives the
+    largest value."""
+    v = values.double().cpu().numpy() if hasattr(values, "cpu") else np.asarray(values, dtype=np.float64)
+    w = np.ones_like(v) if weights is None else (
+        weights.double().cpu().numpy() if hasattr(weights, "cpu") else np.asarray(weights, dtype=np.float64))
+    keep = v > 0
+    v, w = v[keep], w[keep]
+    if v.size == 0:
+        return 0.0
+    order = np.argsort(-v)
+    v, w = v[order], w[order]
+    total = float((v * w).sum())
+    # excess above v[i]: sum_{j < i} w_j (v_j - v_i) = (prefix of w v) - v_i (prefix of w)
+    cwv = np.concatenate([[0.0], np.cumsum(w * v)[:-1]])
+    cw = np.concatenate([[0.0], np.cumsum(w)[:-1]])
+    excess = cwv - v * cw
+    ok = np.nonzero(excess <= overweight * total)[0]
+    return float(v[ok[-1]])
 
 
 def chi2_against(weighted_values, weights, event_values, event_weights, edges):

@@ -133,7 +133,8 @@ def test_stage1_matches_oracle():
 
 def test_two_stage_is_unbiased_and_gains_on_ggggg():
     """g g -> g g g at 13 TeV: a surrogate trained for a few seconds on 2^17 labelled points;
-    two-stage and plain unweighting of the same 2^20 candidates. Both samples' histograms of the
+    two-stage and plain unweighting of the same 2^20 candidates, both with reduced maxima (0.1 % of
+    the total above them). Both samples' histograms of the
     leading parton's pT, its pseudorapidity and m23 agree with the exact weighted histogram
     (chi^2 per bin below 2.5), and the two-stage events per exact evaluation exceed plain's."""
     import torch
@@ -151,9 +152,10 @@ def test_two_stage_is_unbiased_and_gains_on_ggggg():
     assert net.error() == 0
     w = me * jac
     s = pl.surrogate_values(net, x, jac, mu, sigma)
-    w_max = unweight.maxima(w)
-    s_max = unweight.maxima(s)
-    r_max = unweight.maxima(w / s, 0.999)
+    # reduced maxima: at most 0.1 % of the total above each (those events keep weights above 1)
+    w_max = unweight.maxima(w, overweight=1e-3)
+    s_max = unweight.maxima(s, overweight=1e-3)
+    r_max = unweight.maxima(w / s, s, overweight=1e-3)
     n_cand = 1 << 20
     idx_all = pl.passing(0, 0, n_cand)
     xa, ma, ja, _ = pl.labelled(0, 0, n_cand)
@@ -161,7 +163,8 @@ def test_two_stage_is_unbiased_and_gains_on_ggggg():
     ip, wp, exact_p = pl.plain(0, 0, n_cand, w_max)
     i2, w2, exact_2 = pl.two_stage(0, net, 0, n_cand, mu, sigma, s_max, r_max)
     assert exact_p == idx_all.numel()
-    assert len(ip) > 50 and len(i2) > 50
+    print(f"plain: {len(ip)} events from {exact_p} exact evaluations; two-stage: {len(i2)} from {exact_2}")
+    assert len(ip) > 50 and len(i2) > 50, (len(ip), len(i2), exact_p, exact_2)
     seed = pl.family_seed(0)
 
     def moms(index):

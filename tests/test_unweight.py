@@ -95,3 +95,19 @@ def test_two_stage_toy_detects_a_biased_rule():
     edges = np.linspace(0, 1, 21)
     chi2_bad, bins = unweight.chi2_against(x[:, 0], f, x[keep, 0], np.ones(keep.sum()), edges)
     assert chi2_bad > 10 * bins
+
+
+def test_reduced_maximum():
+    """The reduced maximum leaves at most the asked share of the total above it, and is the
+    largest value for a share of 0."""
+    rng = np.random.default_rng(9)
+    v = rng.pareto(3.0, 100000) + 1e-3
+    for eps in (0.0, 1e-4, 1e-3, 1e-2):
+        t = unweight.maxima(v, overweight=eps)
+        assert np.maximum(0, v - t).sum() <= eps * v.sum() * (1 + 1e-9)
+        if eps == 0.0:
+            assert t == v.max()
+    assert unweight.maxima(v, overweight=1e-2) < unweight.maxima(v, overweight=1e-4)
+    w = rng.uniform(0, 2, v.size)
+    t = unweight.maxima(v, w, 1e-3)
+    assert (w * np.maximum(0, v - t)).sum() <= 1e-3 * (w * v).sum() * (1 + 1e-9)
