@@ -338,19 +338,19 @@ def surrogate_line(torch, train_points=1 << 22, candidates=1 << 22, epochs=10, b
     flops = 2 * (64 * 256 + 3 * 256 * 256 + 256)
     k0 = int(np.argmax(counts))
     w_max, s_max, r_max = maxima[k0]
+    cand = pl.passing(k0, first, counts[k0]).clone()
     e0.record()
     for _ in range(steps):
         pl.counters.zero_()
-        S.lib()  # bound
-        UW._check(UW._lib().pacuda_uw_stage1(net.handle, pl.family_seed(k0), first, counts[k0], pl.sqrt_s,
-                                             UW.C.byref(pl.cuts), k0, mu, sigma, s_max, UW._ptr(pl.index),
-                                             UW._ptr(pl.kept_s), pl.capacity, UW._ptr(pl.counters), UW._stream()),
-                  "stage 1")
+        UW._check(UW._lib().pacuda_uw_stage1(net.handle, pl.family_seed(k0), UW._ptr(cand), cand.numel(), pl.sqrt_s,
+                                             k0, mu, sigma, s_max, UW._ptr(pl.kept), UW._ptr(pl.kept_s), pl.capacity,
+                                             UW._ptr(pl.counters), UW._stream()), "stage 1")
     e1.record()
     e1.synchronize()
     ms = e0.elapsed_time(e1) / steps
-    res["stage1_kernel"] = {"candidates": counts[k0], "ms": ms, "candidates_per_s": counts[k0] / (ms * 1e-3),
-                            "flops_per_candidate": flops, "tflops": counts[k0] * flops / (ms * 1e-3) / 1e12}
+    res["stage1_kernel"] = {"candidates_inside_cuts": int(cand.numel()), "ms": ms,
+                            "candidates_per_s": cand.numel() / (ms * 1e-3), "flops_per_candidate": flops,
+                            "tflops": cand.numel() * flops / (ms * 1e-3) / 1e12}
     return res
 
 
@@ -367,6 +367,7 @@ def surrogate_kernels(torch, count=1 << 21, steps=5):
     x = torch.rand(count, 9, device="cuda")
     out = torch.empty(count, device="cuda")
     pl = UW.Pipeline(families=FAMILIES, capacity=count)
+    cand = torch.arange(count, dtype=torch.int64, device="cuda")  # a candidate list (the weights do not matter)
     res = {}
     for what in ("forward", "stage1"):
         def launch():
@@ -374,8 +375,8 @@ def surrogate_kernels(torch, count=1 << 21, steps=5):
                 net.forward(x, out)
             else:
                 pl.counters.zero_()
-                UW._check(UW._lib().pacuda_uw_stage1(net.handle, 11, 0, count, ECM, UW.C.byref(pl.cuts), 0, -3.0, 1.0,
-                                                     1e30, UW._ptr(pl.index), UW._ptr(pl.kept_s), pl.capacity,
+                UW._check(UW._lib().pacuda_uw_stage1(net.handle, 11, UW._ptr(cand), count, ECM, 0, -3.0, 1.0, 1e30,
+                                                     UW._ptr(pl.kept), UW._ptr(pl.kept_s), pl.capacity,
                                                      UW._ptr(pl.counters), UW._stream()), "stage 1")
         for _ in range(2):
             launch()
@@ -422,19 +423,24 @@ def six_gluon_line(torch, B, points=1 << 20, steps=3, warmup=2, check=256):
         plans = [B.Plan(t, kind) for t in parts]
         outs = [torch.empty(points * t.outputs, dtype=torch.float64, device="cuda") for t in parts]
         batch = B.Batch(plans, [ext] * len(parts), outs)
+        stream = torch.cuda.Stream()
+        with torch.cuda.stream(stream):
+            batch.tune(stream)
+            batch.capture(stream)
         for _ in range(warmup):
-            batch.run()
+            batch.run(stream)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
+        e0.record(stream)
         for _ in range(steps):
-            batch.run()
-        e1.record()
+            batch.run(stream)
+        e1.record(stream)
         e1.synchronize()
         ms = e0.elapsed_time(e1) / steps
         flops = sum(pl.flops for pl in plans) * points
         res[kind] = {"value": points / (ms * 1e-3), "unit": "points/s", "ms_per_step": ms,
-                     "tflops": flops / (ms * 1e-3) / 1e12,
-                     "lanes_per_point": [batch.lanes_per_point(k) for k in range(len(plans))]}
+                     "tflops": flops / (ms * 1e-3) / 1e12, "launches_per_step": batch.launches,
+                     "lanes_per_point": [batch.lanes_per_point(k) for k in range(len(plans))],
+                     "blocks_per_sm": [batch.plan_blocks_per_sm(k) for k in range(len(plans))]}
         totals[kind] = sum(o.view(points, t.outputs).sum(dim=1) for o, t in zip(outs, parts))
         if kind == "f64":
             res["parity"] = oracle_parity([(f"gg>gggg part {k}", t, p[:check], o.view(points, t.outputs)[:check])
@@ -507,19 +513,23 @@ def pp4j_line(torch, B, points=1 << 22, steps=3, warmup=2, check=256):
         plans = [B.Plan(t, kind) for _, t, _, _ in fams]
         outs = [torch.empty(n * t.outputs, dtype=torch.float64, device="cuda") for _, t, n, _ in fams]
         batch = B.Batch(plans, [e for *_, e in fams], outs)
-        batch.blocks_per_sm = 1
+        stream = torch.cuda.Stream()
+        with torch.cuda.stream(stream):
+            batch.tune(stream)
+            batch.capture(stream)
         for _ in range(warmup):
-            batch.run()
+            batch.run(stream)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
+        e0.record(stream)
         for _ in range(steps):
-            batch.run()
-        e1.record()
+            batch.run(stream)
+        e1.record(stream)
         e1.synchronize()
         ms = e0.elapsed_time(e1) / steps
         flops = sum(pl.flops * n for pl, (_, _, n, _) in zip(plans, fams))
         res[kind] = {"value": points / (ms * 1e-3), "unit": "points/s", "ms_per_step": ms,
-                     "tflops": flops / (ms * 1e-3) / 1e12}
+                     "tflops": flops / (ms * 1e-3) / 1e12, "launches_per_step": batch.launches,
+                     "blocks_per_sm": [batch.plan_blocks_per_sm(k) for k in range(len(plans))]}
         per_family = {}
         for (name, t, n, _), o in zip(fams, outs):
             x = o.view(n, t.outputs).sum(dim=1)
@@ -904,6 +914,7 @@ def main():
     value = points / (ms * 1e-3)
     peak = fp64_peak(torch, B.lib())
     achieved = flops / (ms * 1e-3) / 1e12  # this rank's launch: its flops over its device time
+    alg_bytes = sum(p.shape[0] * (32 * t.external_count + 8 * t.outputs) for _, t, p in fams)
     per_point = dram_bytes_per_point() if not args.family else None
     traffic = per_point * sum(p.shape[0] for _, _, p in fams) if per_point else None
     res = {"metric": metric, "value": value, "unit": "points/s", "n_gpus": world, "steps": args.steps,
@@ -918,6 +929,10 @@ def main():
                         "traffic_source": "dram read+write bytes per point from one ncu capture of the same mix "
                                           "(profiles/launches_pp3j_bench.md), times this launch's points",
                         "hbm": {"achieved_gbs": traffic / (ms * 1e-3) / 1e9 if traffic else None,
+                                "algorithmic_bytes": alg_bytes,
+                                "algorithmic_gbs": alg_bytes / (ms * 1e-3) / 1e9,
+                                "algorithmic_bytes_note": "momenta in (legs x 4 x 8 B) and every helicity output out "
+                                                          "(8 B each) per point",
                                 "peak_gbs": hbm_peak(), "peak_source": "MEASURED_PEAKS.json hbm_gbs"},
                         "flops_per_point": {n: pl.flops for (n, _, _), pl in zip(fams, plans)}},
            "points_per_family": {n: p.shape[0] for n, _, p in fams},
@@ -972,7 +987,7 @@ def main():
                                  "and the reference runner's f64 kernel, bit for bit")
         if not args.no_precision:
             res["precision"] = [precision_line(torch, B, fams, ext, out, args.steps, args.warmup, k)
-                                for k in ("mixed", "mixed64", "df64")]
+                                for k in ("f64fma", "mixed", "mixed64", "df64")]
             res["precision_gg4g"] = six_gluon_line(torch, B)
             res["pp4j"] = pp4j_line(torch, B)
         if not args.no_surrogate:

@@ -70,11 +70,13 @@ int pacuda_sg_error(const pacuda_sg_net *net);
  *
  * Candidate i of a stream with seed S has seven uniforms from a xorshift64 stream started at
  * splitmix64(S ^ (i * 0xD1B54A32D192ED03)) | 1: five phase-space numbers x, then u5 and u6 for the
- * two accept/reject steps. Its point: s23 = s x1; leg 2 (p1) in the centre-of-mass frame with
- * |p1| = (s - s23) / (2 sqrt(s)), cos(theta) = 2 x2 - 1, phi = 2 pi x3; legs 3 and 4 back to back in
- * the rest frame of P - p1, cos(theta) = 2 x4 - 1, phi = 2 pi x5, boosted; legs 0 and 1 the beams.
- * Its phase-space weight J = s (1 - x1) / (128 pi^3). The network's inputs: x1..x5, then a one-hot
- * of the subprocess (`family`), zeros after. */
+ * two accept/reject steps. Its point (sequential two-body decays, importance-sampled): s23 =
+ * s sigma(16 (2 x1 - 1)) with sigma the logistic function; leg 2 (p1) in the centre-of-mass frame
+ * with |p1| = (s - s23) / (2 sqrt(s)), cos(theta) = tanh(5.5 (2 x2 - 1)), phi = 2 pi x3; legs 3 and 4
+ * back to back in the rest frame of P - p1, cos(theta) = tanh(7 (2 x4 - 1)), phi = 2 pi x5,
+ * boosted; legs 0 and 1 the beams. Its phase-space weight (the density of the unit cube)
+ * J = s (1 - sigma) / (128 pi^3) x 32 sigma (1 - sigma) x 5.5 (1 - cos^2 theta1) x 7 (1 - cos^2 theta2).
+ * The network's inputs: x1..x5, then a one-hot of the subprocess (`family`), zeros after. */
 typedef struct pacuda_uw_cuts {
     double pt_min, eta_max, dr_min; /* pT > pt_min, |eta| < eta_max, pairwise Delta R > dr_min (legs 2-4) */
 } pacuda_uw_cuts;
@@ -90,15 +92,14 @@ int pacuda_uw_candidates(uint64_t seed, uint64_t first, uint32_t count, double s
 int pacuda_uw_points(uint64_t seed, const uint64_t *index, uint32_t n, double sqrt_s, double *momenta, float *inputs,
                      uint32_t input_count, uint32_t family, double *jac, void *stream);
 
-/* Stage 1 in one launch of the fused inference kernel: for candidates first .. first + count - 1
- * of subprocess `family`, the point, the cuts and the surrogate s = exp(mu + sigma out) J (0
- * outside the cuts); a candidate is kept when u5 s_max < s. Kept candidates' indices and s are
- * appended in no particular order (at most `capacity`); counters[0] counts the kept ones, also
- * beyond the capacity, counters[1] those inside the cuts (the caller zeroes both). */
-int pacuda_uw_stage1(const pacuda_sg_net *net, uint64_t seed, uint64_t first, uint32_t count, double sqrt_s,
-                     const pacuda_uw_cuts *cuts, uint32_t family, double mu, double sigma, double s_max,
-                     uint64_t *kept_index, double *kept_s, uint32_t capacity, unsigned long long *counters,
-                     void *stream);
+/* Stage 1 in one launch of the fused inference kernel: for the candidates index[0 .. count) of
+ * subprocess `family` (inside the cuts, as pacuda_uw_candidates lists them), the network's inputs,
+ * the map's weight J and the surrogate s = exp(mu + sigma out) J; a candidate is kept when
+ * u5 s_max < s. Kept candidates' indices and s are appended in no particular order (at most
+ * `capacity`); *counter (zeroed by the caller) counts the kept ones, also beyond the capacity. */
+int pacuda_uw_stage1(const pacuda_sg_net *net, uint64_t seed, const uint64_t *index, uint32_t count, double sqrt_s,
+                     uint32_t family, double mu, double sigma, double s_max, uint64_t *kept_index, double *kept_s,
+                     uint32_t capacity, unsigned long long *counter, void *stream);
 
 /* The decision on points whose exact |M|^2 the runner evaluated (outputs [i][helicities], summed):
  * w = |M|^2 J. Plain unweighting (s == NULL): kept when u5 w_max < w, weight max(1, w / w_max).

@@ -454,18 +454,21 @@ __global__ void adam_kernel(float *params, float *m1, float *m2, const float *gr
 // ---- fused inference ------------------------------------------------------------------------------
 //
 // One block per 128 points at a time (persistent, two blocks per SM so that one block's products
-// run while the other's epilogue does): warps 0-3 build the inputs and run the epilogues (thread r
-// owns point r and tensor-memory lane r), warp 4 streams the weight images through a ring of two
-// 16 KB stages (tiles of 128 rows x 64 values: chunk (k tile, half) of each layer), warp 5 issues
-// the products (M = 128, N = 128 per half) into 256 FP32 columns of tensor memory. The activations
-// stay in one 64 KB A tile set, overwritten in place by each epilogue once the layer's products
-// have completed.
+// run while the other's epilogue does): warps 0-7 build the inputs and run the epilogues (thread
+// (w, lane) owns point r = 32 (w % 4) + lane, tensor-memory lane r, and the column half w / 4),
+// warp 8 streams the weight images through a ring of two 16 KB stages (tiles of 128 rows x 64
+// values: chunk (k tile, half) of each layer), warp 9 issues the products (M = 128, N = 128 per
+// half) into 256 FP32 columns of tensor memory. The activations stay in one 64 KB A tile set,
+// overwritten in place by each epilogue once the layer's products have completed. The biases and
+// the output layer's weights sit in shared memory.
 
-constexpr int FWD_THREADS = 192;
+constexpr int FWD_EPI_THREADS = 256;
+constexpr int FWD_THREADS = FWD_EPI_THREADS + 64;
 constexpr uint32_t FWD_CHUNK = 128 * 128;  // 16 KB
 constexpr int FWD_STAGES = 2;
 constexpr uint32_t FWD_SMEM = 4 * TILE_A + FWD_STAGES * FWD_CHUNK + 1024;
 constexpr int FWD_CHUNKS = 2 + 3 * 8;  // per tile: layer 1 (1 k tile x 2 halves), layers 2-4 (4 x 2)
+constexpr int FWD_PARAMS = 5 * WIDTH + 1;  // b1..b4, w5, b5
 
 struct ForwardArgs {
     const uint8_t *wimg;
@@ -474,16 +477,15 @@ struct ForwardArgs {
     uint32_t inputs, count, tiles;
     float *out;
     int *error;
-    // candidates (stage 1 of two-stage unweighting): candidate first + m of stream `seed`
-    uint64_t seed, first;
+    // candidates (stage 1 of two-stage unweighting): candidate index[m] of stream `seed`
+    const uint64_t *index;
+    uint64_t seed;
     double sqrt_s, mu, sigma, s_max;  // s = exp(mu + sigma out) J; kept when u5 s_max < s
-    pacuda::phase::Cuts cuts;
-    uint32_t family, families;
+    uint32_t family;
     uint64_t *kept_index;  // the kept candidates (unordered), at most `capacity`
     double *kept_s;
     uint32_t capacity;
     unsigned long long *kept_count;  // counts every kept candidate, also beyond the capacity
-    unsigned long long *passed_count;  // candidates that pass the cuts
 };
 
 enum { FWD_FROM_X = 0, FWD_CANDIDATES = 1 };
@@ -504,9 +506,11 @@ __device__ __forceinline__ void fwd_chunk(int c, int &layer, int &kt, int &half)
 template <int MODE>
 __global__ void __launch_bounds__(FWD_THREADS, 2) forward_kernel(ForwardArgs g) {
     extern __shared__ uint8_t smem_raw[];
-    __shared__ uint64_t full[FWD_STAGES], empty[FWD_STAGES], act_ready, acc_ready;
+    __shared__ uint64_t full[FWD_STAGES], empty[FWD_STAGES], act_ready, acc_ready, dot_ready;
     __shared__ uint32_t tmem_base;
     __shared__ volatile int abort_flag;
+    __shared__ float prm[FWD_PARAMS];
+    __shared__ float dot_hi[128];
     const uint32_t pad = (1024u - (smem_u32(smem_raw) & 1023u)) & 1023u;
     uint8_t *act = smem_raw + pad;         // 4 A tiles: the activations (K = 256)
     uint8_t *ring = act + 4 * TILE_A;      // weight chunks
@@ -518,18 +522,22 @@ __global__ void __launch_bounds__(FWD_THREADS, 2) forward_kernel(ForwardArgs g) 
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], 1);
         }
-        mbar_init(&act_ready, 128);
+        mbar_init(&act_ready, FWD_EPI_THREADS);
         mbar_init(&acc_ready, 1);
+        mbar_init(&dot_ready, FWD_EPI_THREADS / 2);
         abort_flag = 0;
         fence_mbar_init();
     }
+    // b1..b4, then w5 and b5 (P_W5, P_B5 follow each other)
+    for (int i = threadIdx.x; i < FWD_PARAMS; i += FWD_THREADS)
+        prm[i] = i < 4 * WIDTH ? g.params[bias_at(i / WIDTH) + i % WIDTH] : g.params[P_W5 + (i - 4 * WIDTH)];
     if (warp == 0) tmem_alloc(&tmem_base, 256);
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = tmem_base;
 
-    if (warp == 4) {
+    if (warp == 8) {
         if (lane == 0) {
             const uint32_t total = my_tiles * FWD_CHUNKS;
             uint32_t issued = 0;
@@ -550,7 +558,7 @@ __global__ void __launch_bounds__(FWD_THREADS, 2) forward_kernel(ForwardArgs g) 
                 if (!mbar_wait(&full[i % FWD_STAGES], (i / FWD_STAGES) & 1, WAIT_CYCLES))
                     flag_error(g.error, 202, &abort_flag);
         }
-    } else if (warp == 5) {
+    } else if (warp == 9) {
         if (lane == 0) {
             constexpr uint32_t idesc = idesc_bf16(128, 128);
             uint32_t chunk = 0, acts = 0;
@@ -584,46 +592,54 @@ __global__ void __launch_bounds__(FWD_THREADS, 2) forward_kernel(ForwardArgs g) 
             }
         }
     } else {
-        // warps 0-3: inputs, epilogues, outputs
-        const uint32_t r = threadIdx.x;  // 0..127
-        const uint32_t lane_addr = tmem + ((uint32_t)(32 * warp) << 16);
-        uint32_t accs = 0;
+        // warps 0-7: inputs, epilogues, outputs; this thread: row r, columns [128 h, 128 h + 128)
+        const uint32_t r = 32 * (warp & 3) + lane, h = warp >> 2;
+        const uint32_t lane_addr = tmem + ((uint32_t)(32 * (warp & 3)) << 16);
+        uint32_t accs = 0, dots = 0;
         for (uint32_t t = 0; t < my_tiles && !__any_sync(0xffffffffu, abort_flag != 0); t++) {
             const uint32_t tile = blockIdx.x + t * gridDim.x, m = tile * 128 + r;
-            // the inputs: row r of A tile 0 (K = 64)
-            uint32_t p[32];
-            bool pass = false;
+            // the inputs: features [32 h, 32 h + 32) of row r of A tile 0 (K = 64)
+            uint32_t p[16];
             double jac = 0.0, u_keep = 1.0;
+            uint64_t cand = 0;
             if (MODE == FWD_FROM_X) {
 #pragma unroll
-                for (int e = 0; e < 32; e++) {
-                    const uint32_t k = 2 * e;
+                for (int e = 0; e < 16; e++) {
+                    const uint32_t k = 32 * h + 2 * e;
                     const float lo = (m < g.count && k < g.inputs) ? g.x[(size_t)m * g.inputs + k] : 0.0f;
                     const float hi = (m < g.count && k + 1 < g.inputs) ? g.x[(size_t)m * g.inputs + k + 1] : 0.0f;
                     p[e] = pack_bf16(lo, hi);
                 }
             } else {
-                // the candidate's phase-space point, cuts and weight; inputs = its five numbers and
-                // the subprocess one-hot
-                double u[pacuda::phase::UNIFORMS], mom[5][4];
-                pacuda::phase::uniforms(g.seed, g.first + m, u);
-                jac = pacuda::phase::map(u, g.sqrt_s, mom);
-                pass = m < g.count && pacuda::phase::passes(mom, g.cuts);
-                u_keep = u[5];
-                float f[6] = {(float)u[0], (float)u[1], (float)u[2], (float)u[3], (float)u[4], 0.0f};
-#pragma unroll
-                for (int e = 0; e < 32; e++) {
-                    float lo = 0.0f, hi = 0.0f;
-                    if (2 * e < 6) lo = f[2 * e];
-                    if (2 * e + 1 < 6) hi = f[2 * e + 1];
-                    if ((uint32_t)(2 * e) == 5 + g.family) lo = 1.0f;
-                    if ((uint32_t)(2 * e + 1) == 5 + g.family) hi = 1.0f;
-                    p[e] = pack_bf16(lo, hi);
+                // the candidate's five numbers and the subprocess one-hot; its weight J (the
+                // listed candidates are inside the cuts)
+                double u[pacuda::phase::UNIFORMS];
+                if (m < g.count) {
+                    cand = g.index[m];
+                    pacuda::phase::uniforms(g.seed, cand, u);
+                    if (h == 0) jac = pacuda::phase::weight(u, g.sqrt_s);
+                } else {
+                    for (int k = 0; k < pacuda::phase::UNIFORMS; k++) u[k] = 0.0;
                 }
+                u_keep = u[5];
+                const bool real = m < g.count;
+                float f[32];  // this half's 32 features (constant indices only)
+#pragma unroll
+                for (int k = 0; k < 32; k++) f[k] = 0.0f;
+                if (h == 0 && real) {
+#pragma unroll
+                    for (int k = 0; k < 5; k++) f[k] = (float)u[k];
+                }
+#pragma unroll
+                for (int k = 0; k < 32; k++)
+                    if (real && 32 * h + k == 5 + g.family) f[k] = 1.0f;
+#pragma unroll
+                for (int e = 0; e < 16; e++) p[e] = pack_bf16(f[2 * e], f[2 * e + 1]);
             }
 #pragma unroll
-            for (int q = 0; q < 8; q++)
-                *reinterpret_cast<uint4 *>(act + sw128_offset(r, 8 * q)) = make_uint4(p[4 * q], p[4 * q + 1], p[4 * q + 2], p[4 * q + 3]);
+            for (int q = 0; q < 4; q++)
+                *reinterpret_cast<uint4 *>(act + sw128_offset(r, 32 * h + 8 * q)) =
+                    make_uint4(p[4 * q], p[4 * q + 1], p[4 * q + 2], p[4 * q + 3]);
             fence_async_shared();
             tc_fence_before();
             mbar_arrive(&act_ready);
@@ -638,8 +654,8 @@ __global__ void __launch_bounds__(FWD_THREADS, 2) forward_kernel(ForwardArgs g) 
                 }
                 accs++;
                 tc_fence_after();
-                const float *bias = g.params + bias_at(layer);
-                for (int c = 0; c < WIDTH / 32; c++) {
+                const float *bias = prm + layer * WIDTH;
+                for (int c = 4 * h; c < 4 * h + 4; c++) {
                     float v[32];
                     tmem_load32(lane_addr + 32 * c, v);
                     if (layer < 3) {
@@ -652,7 +668,7 @@ __global__ void __launch_bounds__(FWD_THREADS, 2) forward_kernel(ForwardArgs g) 
                             *reinterpret_cast<uint4 *>(act + (c / 2) * TILE_A + sw128_offset(r, (32 * c) % 64 + 8 * q)) =
                                 make_uint4(ph[4 * q], ph[4 * q + 1], ph[4 * q + 2], ph[4 * q + 3]);
                     } else {
-                        const float *w5 = g.params + P_W5;
+                        const float *w5 = prm + 4 * WIDTH;
 #pragma unroll
                         for (int j = 0; j < 32; j++) out += bf16_round(silu(v[j] + bias[32 * c + j])) * w5[32 * c + j];
                     }
@@ -663,24 +679,38 @@ __global__ void __launch_bounds__(FWD_THREADS, 2) forward_kernel(ForwardArgs g) 
                     mbar_arrive(&act_ready);
                 }
             }
+            // the two column halves' dot products meet in shared memory: the upper half's threads
+            // write theirs and arrive; the lower half's wait (bounded) and finish the point. The
+            // next write of dot_hi comes after this tile's reads: it needs the next tile's inputs,
+            // which the lower half writes after them.
+            if (h == 1) {
+                dot_hi[r] = out;
+                mbar_arrive(&dot_ready);
+                continue;
+            }
+            const bool have = __all_sync(0xffffffffu, mbar_wait(&dot_ready, dots & 1, WAIT_CYCLES));
+            dots++;
+            if (!have) {
+                flag_error(g.error, 206, &abort_flag);
+                continue;
+            }
+            if (!done) continue;
+            out += dot_hi[r] + prm[5 * WIDTH];
             if (MODE == FWD_FROM_X) {
-                if (done && m < g.count) g.out[m] = out + g.params[P_B5];
-            } else if (done) {
-                // stage 1: s = exp(mu + sigma out) J for a candidate inside the cuts; kept when
-                // u5 s_max < s (warp-aggregated appends)
-                const double sv = pass ? exp(g.mu + g.sigma * (double)(out + g.params[P_B5])) * jac : 0.0;
-                const bool keep = pass && u_keep * g.s_max < sv;
-                const unsigned ballot = __ballot_sync(0xffffffffu, keep), passed = __ballot_sync(0xffffffffu, pass);
+                if (m < g.count) g.out[m] = out;
+            } else {
+                // stage 1: s = exp(mu + sigma out) J; kept when u5 s_max < s (warp-aggregated appends)
+                const bool real = m < g.count;
+                const double sv = real ? exp(g.mu + g.sigma * (double)out) * jac : 0.0;
+                const bool keep = real && u_keep * g.s_max < sv;
+                const unsigned ballot = __ballot_sync(0xffffffffu, keep);
                 unsigned long long base = 0;
-                if (lane == 0) {
-                    if (ballot) base = atomicAdd(g.kept_count, (unsigned long long)__popc(ballot));
-                    if (passed) atomicAdd(g.passed_count, (unsigned long long)__popc(passed));
-                }
+                if (lane == 0 && ballot) base = atomicAdd(g.kept_count, (unsigned long long)__popc(ballot));
                 base = __shfl_sync(0xffffffffu, base, 0);
                 if (keep) {
                     const unsigned long long slot = base + __popc(ballot & ((1u << lane) - 1u));
                     if (slot < g.capacity) {
-                        g.kept_index[slot] = g.first + m;
+                        g.kept_index[slot] = cand;
                         g.kept_s[slot] = sv;
                     }
                 }
@@ -1115,13 +1145,14 @@ extern "C" int pacuda_uw_decide(uint64_t seed, const uint64_t *index, uint32_t n
     return failed(cudaGetLastError(), "decide") ? ST_DEVICE : ST_OK;
 }
 
-extern "C" int pacuda_uw_stage1(const pacuda_sg_net *n, uint64_t seed, uint64_t first, uint32_t count, double sqrt_s,
-                                const pacuda_uw_cuts *cuts, uint32_t family, double mu, double sigma, double s_max,
-                                uint64_t *kept_index, double *kept_s, uint32_t capacity,
-                                unsigned long long *counters, void *stream) {
+extern "C" int pacuda_uw_stage1(const pacuda_sg_net *n, uint64_t seed, const uint64_t *index, uint32_t count,
+                                double sqrt_s, uint32_t family, double mu, double sigma, double s_max,
+                                uint64_t *kept_index, double *kept_s, uint32_t capacity, unsigned long long *counter,
+                                void *stream) {
     g_last_launches = 0;
-    if (!n || !cuts || !kept_index || !kept_s || !counters || count == 0 || !(sqrt_s > 0) || 5 + family >= n->inputs)
+    if (!n || !index || !kept_index || !kept_s || !counter || !(sqrt_s > 0) || 5 + family >= n->inputs)
         return ST_INVALID;
+    if (count == 0) return ST_OK;
     ForwardArgs g;
     memset(&g, 0, sizeof g);
     g.wimg = n->wimg;
@@ -1130,18 +1161,16 @@ extern "C" int pacuda_uw_stage1(const pacuda_sg_net *n, uint64_t seed, uint64_t 
     g.count = count;
     g.tiles = (count + 127) / 128;
     g.error = n->error;
+    g.index = index;
     g.seed = seed;
-    g.first = first;
     g.sqrt_s = sqrt_s;
     g.mu = mu;
     g.sigma = sigma;
     g.s_max = s_max;
-    g.cuts = Cuts{cuts->pt_min, cuts->eta_max, cuts->dr_min};
     g.family = family;
     g.kept_index = kept_index;
     g.kept_s = kept_s;
     g.capacity = capacity;
-    g.kept_count = counters;
-    g.passed_count = counters + 1;
+    g.kept_count = counter;
     return launch_forward<FWD_CANDIDATES>(g, (cudaStream_t)stream) ? ST_OK : ST_DEVICE;
 }

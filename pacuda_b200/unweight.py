@@ -7,9 +7,10 @@ Per subprocess ("family"), candidates are seeded points of the unit cube mapped 
 
 * plain: every candidate inside the cuts is evaluated exactly, w = |M|^2 J, and kept when
   u5 w_max < w, with weight max(1, w / w_max);
-* two-stage: the surrogate s = exp(mu + sigma net(x)) J is evaluated on every candidate (one fused
-  launch: point, cuts, network, decision); the kept ones (u5 s_max < s) are evaluated exactly and
-  kept when u6 r_max < r, r = w / s, with weight max(1, s / s_max) max(1, r / r_max).
+* two-stage: the surrogate s = exp(mu + sigma net(x)) J is evaluated on every candidate inside the
+  cuts (one fused launch: inputs, network, weight, decision); the kept ones (u5 s_max < s) are
+  evaluated exactly and kept when u6 r_max < r, r = w / s, with weight
+  max(1, s / s_max) max(1, r / r_max).
 
 With those weights both samples are unbiased estimates of the distribution of w: a kept event's
 expected weight is w / (w_max) (plain) or w / (s_max r_max) (two-stage) for every candidate,
@@ -49,9 +50,9 @@ def _lib():
         L.pacuda_uw_decide.argtypes = [C.c_uint64, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p,
                                        C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_void_p, C.c_void_p,
                                        C.c_void_p, C.c_void_p]
-        L.pacuda_uw_stage1.argtypes = [C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint32, C.c_double, C.c_void_p,
-                                       C.c_uint32, C.c_double, C.c_double, C.c_double, C.c_void_p, C.c_void_p,
-                                       C.c_uint32, C.c_void_p, C.c_void_p]
+        L.pacuda_uw_stage1.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint32, C.c_double, C.c_uint32,
+                                       C.c_double, C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_uint32,
+                                       C.c_void_p, C.c_void_p]
         L._uw_bound = True
     return L
 
@@ -114,6 +115,7 @@ class Pipeline:
         self.inputs = 5 + len(self.names)
         self.fams = [Family(n, k, capacity) for k, n in enumerate(self.names)]
         self.index = torch.empty(capacity, dtype=torch.int64, device="cuda")
+        self.kept = torch.empty(capacity, dtype=torch.int64, device="cuda")
         self.kept_s = torch.empty(capacity, dtype=torch.float64, device="cuda")
         self.counters = torch.zeros(2, dtype=torch.int64, device="cuda")
         self.jac = torch.empty(capacity, dtype=torch.float64, device="cuda")
@@ -127,8 +129,9 @@ class Pipeline:
 
     # ---- candidates inside the cuts and their exact weights ------------------------------------
 
-    def passing(self, k, first, count):
-        """Indices of the candidates first .. first + count - 1 of family k inside the cuts (sorted)."""
+    def passing(self, k, first, count, sort=True):
+        """Indices of the candidates first .. first + count - 1 of family k inside the cuts (sorted,
+        a new tensor; or in no particular order, a view of this pipeline's index buffer)."""
         import torch
 
         self.counters.zero_()
@@ -138,7 +141,7 @@ class Pipeline:
         n = int(self.counters[0].item())
         if n > self.capacity:
             raise S.SurrogateError(f"{n} passing candidates exceed the capacity {self.capacity}")
-        return torch.sort(self.index[:n])[0]
+        return torch.sort(self.index[:n])[0] if sort else self.index[:n]
 
     def labelled(self, k, first, count):
         """(inputs [n][inputs] fp32, |M|^2 [n] f64, J [n] f64, index [n]) of the passing candidates."""
@@ -161,7 +164,7 @@ class Pipeline:
         """Plain unweighting of candidates first .. first + count - 1 of family k: (kept index,
         weights, exact evaluations)."""
         fam = self.fams[k]
-        idx = self.passing(k, first, count)
+        idx = self.passing(k, first, count, sort=False)
         n = idx.numel()
         jac = self.jac[:n]
         _check(_lib().pacuda_uw_points(self.family_seed(k), _ptr(idx), n, self.sqrt_s, None, None, 0, 0, _ptr(jac),
@@ -177,9 +180,10 @@ class Pipeline:
         import torch
 
         fam = self.fams[k]
+        cand = self.passing(k, first, count, sort=False)
         self.counters.zero_()
-        _check(_lib().pacuda_uw_stage1(net.handle, self.family_seed(k), first, count, self.sqrt_s, C.byref(self.cuts),
-                                       k, mu, sigma, s_max, _ptr(self.index), _ptr(self.kept_s), self.capacity,
+        _check(_lib().pacuda_uw_stage1(net.handle, self.family_seed(k), _ptr(cand), cand.numel(), self.sqrt_s, k, mu,
+                                       sigma, s_max, _ptr(self.kept), _ptr(self.kept_s), self.capacity,
                                        _ptr(self.counters), _stream()), "stage 1")
         n = int(self.counters[0].item())
         if n > self.capacity:
@@ -187,7 +191,7 @@ class Pipeline:
         if n == 0:
             empty = torch.empty(0, dtype=torch.int64, device="cuda")
             return empty, torch.empty(0, dtype=torch.float64, device="cuda"), 0
-        idx, s = self.index[:n], self.kept_s[:n]
+        idx, s = self.kept[:n], self.kept_s[:n]
         jac = self.jac[:n]
         _check(_lib().pacuda_uw_points(self.family_seed(k), _ptr(idx), n, self.sqrt_s, None, None, 0, 0, _ptr(jac),
                                        _stream()), "points")

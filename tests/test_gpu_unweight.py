@@ -91,9 +91,9 @@ def test_decisions_match_oracle():
 
 
 def test_stage1_matches_oracle():
-    """The fused first stage (point, cuts, network, decision in one launch) keeps the candidates
-    the restatement keeps with the CPU network's values, except where u s_max lies within 2 % of
-    s (the device network rounds differently)."""
+    """The fused first stage (inputs, network, weight, decision in one launch) over a list of
+    candidates keeps those the restatement keeps with the CPU network's values, except where
+    u s_max lies within 2 % of s (the device network rounds differently)."""
     import torch
 
     from oracle import surrogate_oracle as SO
@@ -106,29 +106,30 @@ def test_stage1_matches_oracle():
     mu, sigma = -2.0, 1.5
     n, first = 40000, 123
     seed = pl.family_seed(0)
-    u = U.uniforms(seed, np.arange(first, first + n, dtype=np.uint64))
-    mom, jac = U.phase_space(u, SQRT_S)
-    ok = U.passes(mom)
+    cand = pl.passing(0, first, n)  # sorted indices inside the cuts
+    idx = cand.cpu().numpy().astype(np.uint64)
+    u = U.uniforms(seed, idx)
+    jac = U.weight(u, SQRT_S)
     out = SO.forward(p, U.features(u, 0, 1)).astype(np.float64)
-    sv = np.where(ok, np.exp(mu + sigma * out) * jac, 0.0)
-    s_max = float(np.quantile(sv[ok], 0.99))
+    sv = np.exp(mu + sigma * out) * jac
+    s_max = float(np.quantile(sv, 0.99))
     pl.counters.zero_()
     L = unweight._lib()
-    assert L.pacuda_uw_stage1(net.handle, seed, first, n, SQRT_S, C.byref(pl.cuts), 0, mu, sigma, s_max,
-                              C.c_void_p(pl.index.data_ptr()), C.c_void_p(pl.kept_s.data_ptr()), pl.capacity,
+    assert L.pacuda_uw_stage1(net.handle, seed, C.c_void_p(cand.data_ptr()), cand.numel(), SQRT_S, 0, mu, sigma, s_max,
+                              C.c_void_p(pl.kept.data_ptr()), C.c_void_p(pl.kept_s.data_ptr()), pl.capacity,
                               C.c_void_p(pl.counters.data_ptr()), None) == 0
     torch.cuda.synchronize()
     assert net.error() == 0
-    kept, passed = int(pl.counters[0]), int(pl.counters[1])
-    assert passed == int(ok.sum())
-    got = pl.index[:kept].cpu().numpy()
+    kept = int(pl.counters[0])
+    got = pl.kept[:kept].cpu().numpy().astype(np.uint64)
+    pos = {int(c): i for i, c in enumerate(idx)}
     want_keep = u[:, 5] * s_max < sv
     borderline = np.abs(u[:, 5] * s_max - sv) <= 0.02 * np.maximum(sv, 1e-300)
-    got_mask = np.zeros(n, dtype=bool)
-    got_mask[got - first] = True
+    got_mask = np.zeros(len(idx), dtype=bool)
+    got_mask[[pos[int(c)] for c in got]] = True
     assert np.array_equal(got_mask[~borderline], want_keep[~borderline])
     ks = pl.kept_s[:kept].cpu().numpy()
-    assert np.allclose(ks, sv[got - first], rtol=0.05)
+    assert np.allclose(ks, sv[[pos[int(c)] for c in got]], rtol=0.05)
 
 
 def test_two_stage_is_unbiased_and_gains_on_ggggg():
