@@ -211,13 +211,14 @@ def precision_line(torch, B, fams, ext, ref_out, steps, warmup, kind="mixed"):
             "blocks_per_sm": {nm: batch.plan_blocks_per_sm(k) for k, (nm, _, _) in enumerate(fams)}}
 
 
-def surrogate_line(torch, train_points=1 << 22, candidates=1 << 22, epochs=10, batch=16384, steps=3, check=2048):
-    """The learned part: a surrogate of log |M|^2 per p p -> 3 jets subprocess (one network, the
-    five unit-cube numbers and a subprocess one-hot as inputs, 4 x 256 SiLU, BF16 tensor-core
-    products), trained by this library's kernels on `train_points` points labelled by the f64
-    recurrence, then two-stage unweighting of `candidates` seeded candidates (split over the
-    families as the benchmark's points are) against plain unweighting of the same candidates
-    with the f64 runner alone. Reports the training, the surrogate's relative errors on held-out
+def surrogate_line(torch, train_points=1 << 22, candidates=1 << 22, epochs=60, batch=16384, steps=3):
+    """The learned part: a surrogate of the weight w = |M|^2 J of p p -> 3 jets candidates (one
+    network, the five unit-cube numbers and a subprocess one-hot as inputs, 4 x 256 SiLU, BF16
+    tensor-core products, trained on the standardized log w), trained by this library's kernels
+    on `train_points` points inside the cuts labelled by the f64 recurrence (a training stream of
+    candidates), then two-stage unweighting of `candidates` seeded candidates (split over the
+    families as the benchmark's points are) against plain unweighting of the same candidates with
+    the f64 runner alone. Reports the training, the surrogate's relative errors on held-out
     points, both pipelines' efficiencies and unweighted events/s (device time, CUDA events around
     each step, the host's reads of the kept counts inside), the events' agreement with the exact
     weighted distribution (chi^2 per bin of three observables), and the fused first-stage
@@ -227,12 +228,13 @@ def surrogate_line(torch, train_points=1 << 22, candidates=1 << 22, epochs=10, b
 
     fams = list(FAMILIES)
     counts = split_points(candidates, SEED)
-    train_counts = split_points(train_points, SEED + 1)
-    pl = UW.Pipeline(families=fams, capacity=max(max(counts), max(train_counts)) + 1024)
+    # a training stream of 4 x train_points candidates: about 28 % pass the cuts
+    train_counts = split_points(4 * train_points, SEED + 1)
+    pl = UW.Pipeline(families=fams, capacity=int(0.4 * max(max(counts), max(train_counts))) + 4096)
     res = {"workload": f"pp>3j LC: {', '.join(fams)}; 13 TeV, pT>20 GeV, |eta|<5, dR>0.4; network 4 x 256 SiLU, "
-                       f"inputs 5 + {len(fams)} one-hot; {train_points} labelled candidates, {candidates} unweighted",
-           "candidates_per_family": dict(zip(fams, counts))}
-    # labels: the f64 recurrence on the passing candidates of a training stream (candidates from 2^40 on)
+                       f"inputs 5 + {len(fams)} one-hot; {train_points} labelled points, {candidates} candidates "
+                       f"unweighted", "candidates_per_family": dict(zip(fams, counts))}
+    # labels: the f64 recurrence on the candidates of a training stream (from 2^40 on) inside the cuts
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     data = [pl.labelled(k, 1 << 40, c) for k, c in enumerate(train_counts)]
@@ -240,41 +242,43 @@ def surrogate_line(torch, train_points=1 << 22, candidates=1 << 22, epochs=10, b
     e1.synchronize()
     label_ms = e0.elapsed_time(e1)
     x = torch.cat([d[0] for d in data])
-    me = torch.cat([d[1] for d in data])
-    jac = torch.cat([d[2] for d in data])
-    logm = me.log()
-    mu, sigma = float(logm.mean()), float(logm.std())
-    y = ((logm - mu) / sigma).float()
-    held = torch.randperm(x.shape[0], device="cuda", generator=torch.Generator(device="cuda").manual_seed(5))
+    w = torch.cat([d[1] * d[2] for d in data])
+    fam_of = torch.cat([torch.full((d[0].shape[0],), k, dtype=torch.int64, device="cuda") for k, d in enumerate(data)])
+    labelled = int(x.shape[0])
+    pick = torch.randperm(labelled, device="cuda", generator=torch.Generator(device="cuda").manual_seed(5))
     n_hold = 1 << 16
-    hx, hy, hme, hjac = x[held[:n_hold]], y[held[:n_hold]], me[held[:n_hold]], jac[held[:n_hold]]
-    tx, ty = x[held[n_hold:]].contiguous(), y[held[n_hold:]].contiguous()
+    hold, train = pick[:n_hold], pick[n_hold:n_hold + train_points]
+    logw = w.log()
+    mu, sigma = float(logw[train].mean()), float(logw[train].std())
+    y = ((logw - mu) / sigma).float()
+    tx, ty = x[train].contiguous(), y[train].contiguous()
     net = S.Network(pl.inputs, max_batch=batch, seed=7)
     e0.record()
-    hist = UW.train(net, tx, ty, epochs=epochs, batch=batch, lr=2e-3, lr_end=2e-5)
+    hist = UW.train(net, tx, ty, epochs=epochs, batch=batch, lr=2e-3, lr_end=1e-5)
     e1.record()
     e1.synchronize()
     train_ms = e0.elapsed_time(e1)
     if net.error():
         raise RuntimeError(f"surrogate kernels reported error {net.error()}")
-    pred = net.forward(hx)
-    rel = ((mu + sigma * pred.double()).exp() / hme - 1.0).abs().cpu().numpy()
-    res["training"] = {"points": int(tx.shape[0]), "epochs": epochs, "batch": batch, "loss_per_epoch": hist,
-                       "label_ms": label_ms, "train_ms": train_ms,
-                       "train_steps": epochs * (tx.shape[0] // batch),
-                       "held_out_points": n_hold,
-                       "surrogate_rel_error": {q: float(np.quantile(rel, float(q))) for q in ("0.5", "0.9", "0.99")}}
-    # maxima from the labelled sample, per family
+    sv_hold = pl.surrogate_values(net, x[hold], mu, sigma)
+    rel = (sv_hold / w[hold] - 1.0).abs().cpu().numpy()
+    res["training"] = {"labelled_points": labelled, "train_points": int(tx.shape[0]), "epochs": epochs,
+                       "batch": batch, "loss_per_epoch": [round(v, 6) for v in hist], "label_ms": label_ms,
+                       "train_ms": train_ms, "train_steps": epochs * (tx.shape[0] // batch),
+                       "sigma_log_w": sigma, "held_out_points": n_hold,
+                       "surrogate_rel_error": {q: float(np.quantile(rel, float(q))) for q in ("0.5", "0.9", "0.99")},
+                       "log_error_rms": float((sv_hold.log() - w[hold].log()).pow(2).mean().sqrt())}
+    # maxima per family from its labelled points (reduced: at most OVERWEIGHT of the total above)
     maxima = []
-    start = 0
-    for k, d in enumerate(data):
-        n = d[0].shape[0]
-        w = d[1] * d[2]
-        sv = pl.surrogate_values(net, d[0], d[2], mu, sigma)
-        maxima.append((UW.maxima(w, overweight=OVERWEIGHT), UW.maxima(sv, overweight=OVERWEIGHT),
-                       UW.maxima(w / sv, sv, overweight=OVERWEIGHT)))
-        start += n
-    del data, x, me, jac, tx, ty
+    sv_all = pl.surrogate_values(net, x, mu, sigma)
+    for k in range(len(fams)):
+        sel = fam_of == k
+        wk, sk = w[sel], sv_all[sel]
+        maxima.append((UW.maxima(wk, overweight=OVERWEIGHT), UW.maxima(sk, overweight=OVERWEIGHT),
+                       UW.maxima(wk / sk, sk, overweight=OVERWEIGHT)))
+    res["maxima"] = {"overweight_share": OVERWEIGHT, "per_family": {nm: {"w_max": m[0], "s_max": m[1], "r_max": m[2]}
+                                                                    for nm, m in zip(fams, maxima)}}
+    del data, x, w, tx, ty, sv_all, fam_of
     # the two pipelines on the same candidates (stream from 0), timed per step
     first = 0
 
@@ -314,12 +318,21 @@ def surrogate_line(torch, train_points=1 << 22, candidates=1 << 22, epochs=10, b
     # unbiasedness: each sample's histograms against the exact weighted distribution of all candidates
     from oracle import unweight_oracle as UO
 
-    chi = {}
+    chi, xsec = {}, {}
     for k, name in enumerate(fams):
         seed = pl.family_seed(k)
         idx_all = pl.passing(k, first, counts[k])
         _, ma, ja, _ = pl.labelled(k, first, counts[k])
         wa = (ma * ja).cpu().numpy()
+        # the total each sample estimates: sum of weights x its maxima, against the exact sum of w
+        w_max, s_max, r_max = maxima[k]
+        exact = float(wa.sum())
+        for kind, scale in (("plain", w_max), ("two_stage", s_max * r_max)):
+            wts = lines[kind]["_events"][k][1].double().cpu().numpy()
+            est = float(wts.sum()) * scale
+            err = float(np.sqrt((wts ** 2).sum())) * scale
+            xsec.setdefault(kind, {})[name] = {"ratio_to_exact": est / exact, "stat_error": err / exact,
+                                               "events": int(len(wts))}
 
         def moms(index):
             u = UO.uniforms(seed, index.cpu().numpy().astype(np.uint64))
@@ -334,6 +347,7 @@ def surrogate_line(torch, train_points=1 << 22, candidates=1 << 22, epochs=10, b
                 c2, bins = UW.chi2_against(ref[obs], wa, ev[obs], wts.cpu().numpy(), edges)
                 chi.setdefault(kind, {}).setdefault(name, {})[obs] = round(c2 / max(1, bins), 3)
     res["chi2_per_bin_vs_exact"] = chi
+    res["total_vs_exact"] = xsec
     # the fused first stage alone: tensor throughput (algorithmic flops of the network per candidate)
     flops = 2 * (64 * 256 + 3 * 256 * 256 + 256)
     k0 = int(np.argmax(counts))
@@ -342,8 +356,8 @@ def surrogate_line(torch, train_points=1 << 22, candidates=1 << 22, epochs=10, b
     e0.record()
     for _ in range(steps):
         pl.counters.zero_()
-        UW._check(UW._lib().pacuda_uw_stage1(net.handle, pl.family_seed(k0), UW._ptr(cand), cand.numel(), pl.sqrt_s,
-                                             k0, mu, sigma, s_max, UW._ptr(pl.kept), UW._ptr(pl.kept_s), pl.capacity,
+        UW._check(UW._lib().pacuda_uw_stage1(net.handle, pl.family_seed(k0), UW._ptr(cand), cand.numel(), k0, mu,
+                                             sigma, s_max, UW._ptr(pl.kept), UW._ptr(pl.kept_s), pl.capacity,
                                              UW._ptr(pl.counters), UW._stream()), "stage 1")
     e1.record()
     e1.synchronize()
@@ -375,7 +389,7 @@ def surrogate_kernels(torch, count=1 << 21, steps=5):
                 net.forward(x, out)
             else:
                 pl.counters.zero_()
-                UW._check(UW._lib().pacuda_uw_stage1(net.handle, 11, UW._ptr(cand), count, ECM, 0, -3.0, 1.0, 1e30,
+                UW._check(UW._lib().pacuda_uw_stage1(net.handle, 11, UW._ptr(cand), count, 0, -3.0, 1.0, 1e30,
                                                      UW._ptr(pl.kept), UW._ptr(pl.kept_s), pl.capacity,
                                                      UW._ptr(pl.counters), UW._stream()), "stage 1")
         for _ in range(2):

@@ -93,13 +93,14 @@ int pacuda_uw_points(uint64_t seed, const uint64_t *index, uint32_t n, double sq
                      uint32_t input_count, uint32_t family, double *jac, void *stream);
 
 /* Stage 1 in one launch of the fused inference kernel: for the candidates index[0 .. count) of
- * subprocess `family` (inside the cuts, as pacuda_uw_candidates lists them), the network's inputs,
- * the map's weight J and the surrogate s = exp(mu + sigma out) J; a candidate is kept when
- * u5 s_max < s. Kept candidates' indices and s are appended in no particular order (at most
- * `capacity`); *counter (zeroed by the caller) counts the kept ones, also beyond the capacity. */
-int pacuda_uw_stage1(const pacuda_sg_net *net, uint64_t seed, const uint64_t *index, uint32_t count, double sqrt_s,
-                     uint32_t family, double mu, double sigma, double s_max, uint64_t *kept_index, double *kept_s,
-                     uint32_t capacity, unsigned long long *counter, void *stream);
+ * subprocess `family` (inside the cuts, as pacuda_uw_candidates lists them), the network's inputs
+ * and the surrogate s = exp(mu + sigma out), the network's estimate of the candidate's weight
+ * w = |M|^2 J; a candidate is kept when u5 s_max < s. Kept candidates' indices and s are appended
+ * in no particular order (at most `capacity`); *counter (zeroed by the caller) counts the kept
+ * ones, also beyond the capacity. */
+int pacuda_uw_stage1(const pacuda_sg_net *net, uint64_t seed, const uint64_t *index, uint32_t count, uint32_t family,
+                     double mu, double sigma, double s_max, uint64_t *kept_index, double *kept_s, uint32_t capacity,
+                     unsigned long long *counter, void *stream);
 
 /* The decision on points whose exact |M|^2 the runner evaluated (outputs [i][helicities], summed):
  * w = |M|^2 J. Plain unweighting (s == NULL): kept when u5 w_max < w, weight max(1, w / w_max).

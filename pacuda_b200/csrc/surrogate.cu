@@ -480,7 +480,7 @@ struct ForwardArgs {
     // candidates (stage 1 of two-stage unweighting): candidate index[m] of stream `seed`
     const uint64_t *index;
     uint64_t seed;
-    double sqrt_s, mu, sigma, s_max;  // s = exp(mu + sigma out) J; kept when u5 s_max < s
+    double mu, sigma, s_max;  // s = exp(mu + sigma out); kept when u5 s_max < s
     uint32_t family;
     uint64_t *kept_index;  // the kept candidates (unordered), at most `capacity`
     double *kept_s;
@@ -600,7 +600,7 @@ __global__ void __launch_bounds__(FWD_THREADS, 2) forward_kernel(ForwardArgs g) 
             const uint32_t tile = blockIdx.x + t * gridDim.x, m = tile * 128 + r;
             // the inputs: features [32 h, 32 h + 32) of row r of A tile 0 (K = 64)
             uint32_t p[16];
-            double jac = 0.0, u_keep = 1.0;
+            double u_keep = 1.0;
             uint64_t cand = 0;
             if (MODE == FWD_FROM_X) {
 #pragma unroll
@@ -611,13 +611,12 @@ __global__ void __launch_bounds__(FWD_THREADS, 2) forward_kernel(ForwardArgs g) 
                     p[e] = pack_bf16(lo, hi);
                 }
             } else {
-                // the candidate's five numbers and the subprocess one-hot; its weight J (the
-                // listed candidates are inside the cuts)
+                // the candidate's five numbers and the subprocess one-hot (the listed candidates
+                // are inside the cuts)
                 double u[pacuda::phase::UNIFORMS];
                 if (m < g.count) {
                     cand = g.index[m];
                     pacuda::phase::uniforms(g.seed, cand, u);
-                    if (h == 0) jac = pacuda::phase::weight(u, g.sqrt_s);
                 } else {
                     for (int k = 0; k < pacuda::phase::UNIFORMS; k++) u[k] = 0.0;
                 }
@@ -699,9 +698,10 @@ __global__ void __launch_bounds__(FWD_THREADS, 2) forward_kernel(ForwardArgs g) 
             if (MODE == FWD_FROM_X) {
                 if (m < g.count) g.out[m] = out;
             } else {
-                // stage 1: s = exp(mu + sigma out) J; kept when u5 s_max < s (warp-aggregated appends)
+                // stage 1: s = exp(mu + sigma out), the network's estimate of the weight w = |M|^2 J;
+                // kept when u5 s_max < s (warp-aggregated appends)
                 const bool real = m < g.count;
-                const double sv = real ? exp(g.mu + g.sigma * (double)out) * jac : 0.0;
+                const double sv = real ? exp(g.mu + g.sigma * (double)out) : 0.0;
                 const bool keep = real && u_keep * g.s_max < sv;
                 const unsigned ballot = __ballot_sync(0xffffffffu, keep);
                 unsigned long long base = 0;
@@ -1146,12 +1146,11 @@ extern "C" int pacuda_uw_decide(uint64_t seed, const uint64_t *index, uint32_t n
 }
 
 extern "C" int pacuda_uw_stage1(const pacuda_sg_net *n, uint64_t seed, const uint64_t *index, uint32_t count,
-                                double sqrt_s, uint32_t family, double mu, double sigma, double s_max,
+                                uint32_t family, double mu, double sigma, double s_max,
                                 uint64_t *kept_index, double *kept_s, uint32_t capacity, unsigned long long *counter,
                                 void *stream) {
     g_last_launches = 0;
-    if (!n || !index || !kept_index || !kept_s || !counter || !(sqrt_s > 0) || 5 + family >= n->inputs)
-        return ST_INVALID;
+    if (!n || !index || !kept_index || !kept_s || !counter || 5 + family >= n->inputs) return ST_INVALID;
     if (count == 0) return ST_OK;
     ForwardArgs g;
     memset(&g, 0, sizeof g);
@@ -1163,7 +1162,6 @@ extern "C" int pacuda_uw_stage1(const pacuda_sg_net *n, uint64_t seed, const uin
     g.error = n->error;
     g.index = index;
     g.seed = seed;
-    g.sqrt_s = sqrt_s;
     g.mu = mu;
     g.sigma = sigma;
     g.s_max = s_max;

@@ -7,10 +7,10 @@ Per subprocess ("family"), candidates are seeded points of the unit cube mapped 
 
 * plain: every candidate inside the cuts is evaluated exactly, w = |M|^2 J, and kept when
   u5 w_max < w, with weight max(1, w / w_max);
-* two-stage: the surrogate s = exp(mu + sigma net(x)) J is evaluated on every candidate inside the
-  cuts (one fused launch: inputs, network, weight, decision); the kept ones (u5 s_max < s) are
-  evaluated exactly and kept when u6 r_max < r, r = w / s, with weight
-  max(1, s / s_max) max(1, r / r_max).
+* two-stage: the surrogate s = exp(mu + sigma net(x)), trained on the standardized log of the
+  weight w = |M|^2 J, is evaluated on every candidate inside the cuts (one fused launch: inputs,
+  network, decision); the kept ones (u5 s_max < s) are evaluated exactly and kept when
+  u6 r_max < r, r = w / s, with weight max(1, s / s_max) max(1, r / r_max).
 
 With those weights both samples are unbiased estimates of the distribution of w: a kept event's
 expected weight is w / (w_max) (plain) or w / (s_max r_max) (two-stage) for every candidate,
@@ -50,9 +50,9 @@ def _lib():
         L.pacuda_uw_decide.argtypes = [C.c_uint64, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p,
                                        C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_void_p, C.c_void_p,
                                        C.c_void_p, C.c_void_p]
-        L.pacuda_uw_stage1.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint32, C.c_double, C.c_uint32,
-                                       C.c_double, C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_uint32,
-                                       C.c_void_p, C.c_void_p]
+        L.pacuda_uw_stage1.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint32, C.c_uint32, C.c_double,
+                                       C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p,
+                                       C.c_void_p]
         L._uw_bound = True
     return L
 
@@ -182,9 +182,9 @@ class Pipeline:
         fam = self.fams[k]
         cand = self.passing(k, first, count, sort=False)
         self.counters.zero_()
-        _check(_lib().pacuda_uw_stage1(net.handle, self.family_seed(k), _ptr(cand), cand.numel(), self.sqrt_s, k, mu,
-                                       sigma, s_max, _ptr(self.kept), _ptr(self.kept_s), self.capacity,
-                                       _ptr(self.counters), _stream()), "stage 1")
+        _check(_lib().pacuda_uw_stage1(net.handle, self.family_seed(k), _ptr(cand), cand.numel(), k, mu, sigma, s_max,
+                                       _ptr(self.kept), _ptr(self.kept_s), self.capacity, _ptr(self.counters),
+                                       _stream()), "stage 1")
         n = int(self.counters[0].item())
         if n > self.capacity:
             raise S.SurrogateError(f"{n} first-stage events exceed the capacity {self.capacity}")
@@ -202,10 +202,11 @@ class Pipeline:
         keep = self.keep[:n].bool()
         return idx[keep].clone(), self.weight[:n][keep].clone(), n
 
-    def surrogate_values(self, net, x, jac, mu, sigma):
-        """s = exp(mu + sigma net(x)) J for points of known inputs (the fused inference kernel)."""
+    def surrogate_values(self, net, x, mu, sigma):
+        """s = exp(mu + sigma net(x)), the network's estimate of w = |M|^2 J, for points of known
+        inputs (the fused inference kernel)."""
         out = net.forward(x)
-        return (mu + sigma * out.double()).exp() * jac
+        return (mu + sigma * out.double()).exp()
 
 
 def train(net, x, y, epochs, batch=16384, lr=2e-3, lr_end=2e-5, seed=0):
@@ -256,19 +257,40 @@ def maxima(values, weights=None, overweight=1e-3):
     return float(v[ok[-1]])
 
 
-def chi2_against(weighted_values, weights, event_values, event_weights, edges):
+def chi2_against(weighted_values, weights, event_values, event_weights, edges, min_expected=5.0):
     """chi^2 and the number of bins between the normalised histogram of unweighted events (with
-    their weights) and that of the weighted sample it estimates (the exact weights of every
-    candidate), with the events' Poisson variance."""
+    their weights) and the exact weighted distribution it estimates (`weights` of every
+    candidate). Each bin's variance is the one expected from the reference: the events' share
+    p_b times sum(event_weights^2) / sum(event_weights)^2, plus the reference's own; neighbouring
+    bins are merged until each expects at least `min_expected` events."""
     ref, _ = np.histogram(weighted_values, bins=edges, weights=weights)
     ref_var, _ = np.histogram(weighted_values, bins=edges, weights=weights ** 2)
     ev, _ = np.histogram(event_values, bins=edges, weights=event_weights)
-    ev_var, _ = np.histogram(event_values, bins=edges, weights=event_weights ** 2)
-    rt, et = ref.sum(), ev.sum()
-    var = ev_var / et ** 2 + ref_var / rt ** 2
-    mask = var > 0
-    chi2 = float(((ev / et - ref / rt)[mask] ** 2 / var[mask]).sum())
-    return chi2, int(mask.sum())
+    rt, et = ref.sum(), event_weights.sum()
+    n_events = len(event_weights)
+    if rt <= 0 or et <= 0:
+        return float("nan"), 0
+    # merge bins (in order) until each expects min_expected events
+    groups, cur = [], []
+    for b in range(len(ref)):
+        cur.append(b)
+        if ref[cur].sum() / rt * n_events >= min_expected:
+            groups.append(cur)
+            cur = []
+    if cur:
+        if groups:
+            groups[-1] += cur
+        else:
+            groups.append(cur)
+    w2 = float((event_weights ** 2).sum()) / et ** 2
+    chi2 = 0.0
+    for g in groups:
+        p = ref[g].sum() / rt
+        h = ev[g].sum() / et
+        var = p * w2 + ref_var[g].sum() / rt ** 2
+        if var > 0:
+            chi2 += (h - p) ** 2 / var
+    return float(chi2), len(groups)
 
 
 def observables(p):

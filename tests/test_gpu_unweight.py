@@ -45,8 +45,9 @@ def test_candidates_and_points_match_oracle():
     torch.cuda.synchronize()
     keep = U.passes(p)
     got = mom.cpu().numpy().reshape(5, 4, m).transpose(2, 0, 1)
-    assert np.allclose(got, p[keep], rtol=1e-12, atol=1e-9)
-    assert np.allclose(j.cpu().numpy(), jac[keep], rtol=1e-14, atol=0)
+    # exp, tanh and the boost's cancellations round differently on the device: 1e-9 relative
+    assert np.allclose(got, p[keep], rtol=1e-9, atol=1e-7)
+    assert np.allclose(j.cpu().numpy(), jac[keep], rtol=1e-12, atol=0)
     assert np.array_equal(x.cpu().numpy(), U.features(u[keep], 0, 1))
 
 
@@ -91,7 +92,7 @@ def test_decisions_match_oracle():
 
 
 def test_stage1_matches_oracle():
-    """The fused first stage (inputs, network, weight, decision in one launch) over a list of
+    """The fused first stage (inputs, network, decision in one launch) over a list of
     candidates keeps those the restatement keeps with the CPU network's values, except where
     u s_max lies within 2 % of s (the device network rounds differently)."""
     import torch
@@ -109,13 +110,12 @@ def test_stage1_matches_oracle():
     cand = pl.passing(0, first, n)  # sorted indices inside the cuts
     idx = cand.cpu().numpy().astype(np.uint64)
     u = U.uniforms(seed, idx)
-    jac = U.weight(u, SQRT_S)
     out = SO.forward(p, U.features(u, 0, 1)).astype(np.float64)
-    sv = np.exp(mu + sigma * out) * jac
+    sv = np.exp(mu + sigma * out)
     s_max = float(np.quantile(sv, 0.99))
     pl.counters.zero_()
     L = unweight._lib()
-    assert L.pacuda_uw_stage1(net.handle, seed, C.c_void_p(cand.data_ptr()), cand.numel(), SQRT_S, 0, mu, sigma, s_max,
+    assert L.pacuda_uw_stage1(net.handle, seed, C.c_void_p(cand.data_ptr()), cand.numel(), 0, mu, sigma, s_max,
                               C.c_void_p(pl.kept.data_ptr()), C.c_void_p(pl.kept_s.data_ptr()), pl.capacity,
                               C.c_void_p(pl.counters.data_ptr()), None) == 0
     torch.cuda.synchronize()
@@ -133,7 +133,8 @@ def test_stage1_matches_oracle():
 
 
 def test_two_stage_is_unbiased_and_gains_on_ggggg():
-    """g g -> g g g at 13 TeV: a surrogate trained for a few seconds on 2^17 labelled points;
+    """g g -> g g g at 13 TeV: a surrogate of log w trained for a few seconds on the labelled points
+    of 2^19 candidates;
     two-stage and plain unweighting of the same 2^20 candidates, both with reduced maxima (0.1 % of
     the total above them). Both samples' histograms of the
     leading parton's pT, its pseudorapidity and m23 agree with the exact weighted histogram
@@ -144,15 +145,15 @@ def test_two_stage_is_unbiased_and_gains_on_ggggg():
     from pacuda_b200 import unweight
 
     pl = _pipeline(capacity=1 << 20)
-    x, me, jac, _ = pl.labelled(0, 1 << 30, 1 << 18)
-    logm = me.log()
-    mu, sigma = float(logm.mean()), float(logm.std())
-    y = ((logm - mu) / sigma).float()
-    net = S.Network(6, max_batch=8192, seed=3)
-    unweight.train(net, x, y, epochs=12, batch=8192, lr=2e-3, lr_end=1e-4)
-    assert net.error() == 0
+    x, me, jac, _ = pl.labelled(0, 1 << 30, 1 << 19)
     w = me * jac
-    s = pl.surrogate_values(net, x, jac, mu, sigma)
+    logw = w.log()
+    mu, sigma = float(logw.mean()), float(logw.std())
+    y = ((logw - mu) / sigma).float()
+    net = S.Network(6, max_batch=8192, seed=3)
+    unweight.train(net, x, y, epochs=30, batch=8192, lr=2e-3, lr_end=1e-5)
+    assert net.error() == 0
+    s = pl.surrogate_values(net, x, mu, sigma)
     # reduced maxima: at most 0.1 % of the total above each (those events keep weights above 1)
     w_max = unweight.maxima(w, overweight=1e-3)
     s_max = unweight.maxima(s, overweight=1e-3)
@@ -178,7 +179,7 @@ def test_two_stage_is_unbiased_and_gains_on_ggggg():
         edges = unweight.log_edges(ref[name], 12)
         for ev, ww in ((ev_p, wp), (ev_2, w2)):
             chi2, bins = unweight.chi2_against(ref[name], wa, ev[name], ww.cpu().numpy(), edges)
-            assert chi2 / bins < 2.5, (name, chi2, bins)
+            assert chi2 / max(1, bins) < 2.5, (name, chi2, bins)
     eff_plain = len(ip) / exact_p
     eff_two = len(i2) / max(1, exact_2)
     assert eff_two > 3 * eff_plain, (eff_two, eff_plain)
