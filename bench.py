@@ -211,7 +211,8 @@ def precision_line(torch, B, fams, ext, ref_out, steps, warmup, kind="mixed"):
             "blocks_per_sm": {nm: batch.plan_blocks_per_sm(k) for k, (nm, _, _) in enumerate(fams)}}
 
 
-def surrogate_line(torch, train_points=1 << 22, candidates=1 << 22, epochs=60, batch=16384, steps=3):
+def surrogate_line(torch, train_points=1 << 22, candidates=1 << 22, epochs=60, batch=16384, steps=3, alpha=0.5,
+                   lr=2e-3, overweight=None):
     """The learned part: a surrogate of the weight w = |M|^2 J of p p -> 3 jets candidates (one
     network, the five unit-cube numbers and a subprocess one-hot as inputs, 4 x 256 SiLU, BF16
     tensor-core products, trained on the standardized log w), trained by this library's kernels
@@ -241,6 +242,10 @@ def surrogate_line(torch, train_points=1 << 22, candidates=1 << 22, epochs=60, b
     e1.record()
     e1.synchronize()
     label_ms = e0.elapsed_time(e1)
+    # the runner's launch choices timed on every family's points (the plain pipeline's load)
+    listed = pl.candidates(1 << 40, train_counts)
+    pl.exact([f.cand for f in pl.fams], [min(a, max(1, int(0.28 * c))) for a, c in zip(listed, counts)])
+    pl.tune()
     x = torch.cat([d[0] for d in data])
     w = torch.cat([d[1] * d[2] for d in data])
     fam_of = torch.cat([torch.full((d[0].shape[0],), k, dtype=torch.int64, device="cuda") for k, d in enumerate(data)])
@@ -254,7 +259,9 @@ def surrogate_line(torch, train_points=1 << 22, candidates=1 << 22, epochs=60, b
     tx, ty = x[train].contiguous(), y[train].contiguous()
     net = S.Network(pl.inputs, max_batch=batch, seed=7)
     e0.record()
-    hist = UW.train(net, tx, ty, epochs=epochs, batch=batch, lr=2e-3, lr_end=1e-5)
+    # training points drawn in proportion to w^alpha: the accuracy goes where the events come from
+    imp = (logw[train] - logw[train].max()).mul(alpha).exp().float() if alpha else None
+    hist = UW.train(net, tx, ty, epochs=epochs, batch=batch, lr=lr, lr_end=1e-5, importance=imp)
     e1.record()
     e1.synchronize()
     train_ms = e0.elapsed_time(e1)
@@ -263,53 +270,54 @@ def surrogate_line(torch, train_points=1 << 22, candidates=1 << 22, epochs=60, b
     sv_hold = pl.surrogate_values(net, x[hold], mu, sigma)
     rel = (sv_hold / w[hold] - 1.0).abs().cpu().numpy()
     res["training"] = {"labelled_points": labelled, "train_points": int(tx.shape[0]), "epochs": epochs,
+                       "importance": f"points drawn in proportion to w^{alpha}" if alpha else "uniform", "lr": lr,
                        "batch": batch, "loss_per_epoch": [round(v, 6) for v in hist], "label_ms": label_ms,
                        "train_ms": train_ms, "train_steps": epochs * (tx.shape[0] // batch),
                        "sigma_log_w": sigma, "held_out_points": n_hold,
                        "surrogate_rel_error": {q: float(np.quantile(rel, float(q))) for q in ("0.5", "0.9", "0.99")},
                        "log_error_rms": float((sv_hold.log() - w[hold].log()).pow(2).mean().sqrt())}
-    # maxima per family from its labelled points (reduced: at most OVERWEIGHT of the total above)
+    # maxima per family from its labelled points (reduced: at most `overweight` of the total above)
+    overweight = OVERWEIGHT if overweight is None else overweight
     maxima = []
     sv_all = pl.surrogate_values(net, x, mu, sigma)
     for k in range(len(fams)):
         sel = fam_of == k
         wk, sk = w[sel], sv_all[sel]
-        maxima.append((UW.maxima(wk, overweight=OVERWEIGHT), UW.maxima(sk, overweight=OVERWEIGHT),
-                       UW.maxima(wk / sk, sk, overweight=OVERWEIGHT)))
-    res["maxima"] = {"overweight_share": OVERWEIGHT, "per_family": {nm: {"w_max": m[0], "s_max": m[1], "r_max": m[2]}
+        maxima.append((UW.maxima(wk, overweight=overweight), UW.maxima(sk, overweight=overweight),
+                       UW.maxima(wk / sk, sk, overweight=overweight)))
+    res["maxima"] = {"overweight_share": overweight, "per_family": {nm: {"w_max": m[0], "s_max": m[1], "r_max": m[2]}
                                                                     for nm, m in zip(fams, maxima)}}
     del data, x, w, tx, ty, sv_all, fam_of
     # the two pipelines on the same candidates (stream from 0), timed per step
     first = 0
 
+    w_maxes = [m[0] for m in maxima]
+    s_maxes = [m[1] for m in maxima]
+    r_maxes = [m[2] for m in maxima]
+
     def run(kind):
-        kept, exact, events_w = 0, 0, []
-        out = []
-        for k, c in enumerate(counts):
-            w_max, s_max, r_max = maxima[k]
-            if kind == "plain":
-                idx, wts, ne = pl.plain(k, first, c, w_max)
-            else:
-                idx, wts, ne = pl.two_stage(k, net, first, c, mu, sigma, s_max, r_max)
-            kept += idx.numel()
-            exact += ne
-            out.append((idx, wts))
-        return kept, exact, out
+        if kind == "plain":
+            events, exact = pl.plain(first, counts, w_maxes)
+        else:
+            events, exact = pl.two_stage(net, first, counts, mu, sigma, s_maxes, r_maxes)
+        return events, exact
 
     lines = {}
     for kind in ("plain", "two_stage"):
         run(kind)  # warm-up (and the batch plans' first launches)
         e0.record()
         for _ in range(steps):
-            kept, exact, out = run(kind)
+            events, exact = run(kind)
         e1.record()
         e1.synchronize()
         ms = e0.elapsed_time(e1) / steps
+        kept = sum(int(e.index.numel()) for e in events)
         lines[kind] = {"ms_per_step": ms, "events": kept, "exact_evaluations": exact,
                        "events_per_s": kept / (ms * 1e-3), "candidates_per_s": candidates / (ms * 1e-3),
                        "efficiency_per_exact": kept / max(1, exact), "efficiency_per_candidate": kept / candidates,
-                       "overweight_events": int(sum(int((w > 1).sum()) for _, w in out))}
-        lines[kind]["_events"] = out
+                       "overweight_events": int(sum(int((e.weight > 1).sum()) for e in events)),
+                       "events_per_family": {nm: int(e.index.numel()) for nm, e in zip(fams, events)}}
+        lines[kind]["_events"] = [(e.index.clone(), e.weight.clone()) for e in events]
     res["plain"] = {k: v for k, v in lines["plain"].items() if not k.startswith("_")}
     res["two_stage"] = {k: v for k, v in lines["two_stage"].items() if not k.startswith("_")}
     res["events_per_s_ratio"] = lines["two_stage"]["events_per_s"] / lines["plain"]["events_per_s"]
@@ -353,11 +361,12 @@ def surrogate_line(torch, train_points=1 << 22, candidates=1 << 22, epochs=60, b
     k0 = int(np.argmax(counts))
     w_max, s_max, r_max = maxima[k0]
     cand = pl.passing(k0, first, counts[k0]).clone()
+    f0 = pl.fams[k0]
     e0.record()
     for _ in range(steps):
         pl.counters.zero_()
         UW._check(UW._lib().pacuda_uw_stage1(net.handle, pl.family_seed(k0), UW._ptr(cand), cand.numel(), k0, mu,
-                                             sigma, s_max, UW._ptr(pl.kept), UW._ptr(pl.kept_s), pl.capacity,
+                                             sigma, s_max, UW._ptr(f0.kept), UW._ptr(f0.kept_s), pl.capacity,
                                              UW._ptr(pl.counters), UW._stream()), "stage 1")
     e1.record()
     e1.synchronize()
@@ -380,7 +389,7 @@ def surrogate_kernels(torch, count=1 << 21, steps=5):
     net = S.Network(9, max_batch=1024, seed=3)
     x = torch.rand(count, 9, device="cuda")
     out = torch.empty(count, device="cuda")
-    pl = UW.Pipeline(families=FAMILIES, capacity=count)
+    pl = UW.Pipeline(families=FAMILIES[:1], capacity=count)
     cand = torch.arange(count, dtype=torch.int64, device="cuda")  # a candidate list (the weights do not matter)
     res = {}
     for what in ("forward", "stage1"):
@@ -390,8 +399,8 @@ def surrogate_kernels(torch, count=1 << 21, steps=5):
             else:
                 pl.counters.zero_()
                 UW._check(UW._lib().pacuda_uw_stage1(net.handle, 11, UW._ptr(cand), count, 0, -3.0, 1.0, 1e30,
-                                                     UW._ptr(pl.kept), UW._ptr(pl.kept_s), pl.capacity,
-                                                     UW._ptr(pl.counters), UW._stream()), "stage 1")
+                                                     UW._ptr(pl.fams[0].kept), UW._ptr(pl.fams[0].kept_s),
+                                                     pl.capacity, UW._ptr(pl.counters), UW._stream()), "stage 1")
         for _ in range(2):
             launch()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -818,6 +827,7 @@ def main():
     ap.add_argument("--no-reference-gpu", action="store_true", help="skip timing the reference's own GPU runner")
     ap.add_argument("--no-surrogate", action="store_true", help="skip the surrogate and two-stage unweighting line")
     ap.add_argument("--surrogate-only", action="store_true", help="only the surrogate line (development runs)")
+    ap.add_argument("--surrogate-args", default="", help="key=value,... for the surrogate line (development runs)")
     ap.add_argument("--surrogate-kernels", action="store_true", help="only the surrogate kernels on a random network "
                                                                       "(the profiling case)")
     ap.add_argument("--reference-gpu-kind", default=None, help=argparse.SUPPRESS)  # the worker of reference_gpu()
@@ -868,7 +878,11 @@ def main():
         print(json.dumps({"surrogate_kernels": surrogate_kernels(torch)}))
         return
     if args.surrogate_only:
-        print(json.dumps({"surrogate": surrogate_line(torch)}))
+        kw = {}
+        for item in args.surrogate_args.split(",") if args.surrogate_args else []:
+            key, val = item.split("=")
+            kw[key] = float(val) if "." in val or "e" in val else int(val)
+        print(json.dumps({"surrogate": surrogate_line(torch, **kw)}))
         return
     if world > 1:
         import datetime

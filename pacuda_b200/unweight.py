@@ -73,7 +73,8 @@ def _stream():
 
 
 class Family:
-    """One subprocess: its plan for the runner (f64) and the buffers of its exact evaluations."""
+    """One subprocess: its plan for the runner (f64) and its buffers (candidates inside the cuts,
+    first-stage survivors, momenta and outputs of the exact evaluations, decisions)."""
 
     def __init__(self, name, index, capacity):
         import torch
@@ -84,26 +85,27 @@ class Family:
         self.plan = B.Plan(self.template, "f64")
         self.capacity = capacity
         dev = "cuda"
-        self.momenta = torch.empty(5 * 4 * capacity, dtype=torch.float64, device=dev)
+        self.cand = torch.empty(capacity, dtype=torch.int64, device=dev)
+        self.kept = torch.empty(capacity, dtype=torch.int64, device=dev)
+        self.kept_s = torch.empty(capacity, dtype=torch.float64, device=dev)
+        self.jac = torch.empty(capacity, dtype=torch.float64, device=dev)
+        self.keep = torch.empty(capacity, dtype=torch.uint8, device=dev)
+        self.weight = torch.empty(capacity, dtype=torch.float64, device=dev)
+        self.momenta = torch.zeros(5 * 4 * capacity, dtype=torch.float64, device=dev)
         self.outputs = torch.empty(capacity * self.helicities, dtype=torch.float64, device=dev)
-        self.batch = B.Batch([self.plan], [self.momenta[: 5 * 4 * 1024]], [self.outputs[: 1024 * self.helicities]])
 
-    def exact(self, seed, index, n, sqrt_s):
-        """|M|^2 outputs [n][helicities] of candidates index[:n] (f64 runner, one launch)."""
-        import torch
 
-        if n > self.capacity:
-            raise S.SurrogateError(f"{self.name}: {n} points exceed the capacity {self.capacity}")
-        mom = self.momenta[: 20 * n]
-        _check(_lib().pacuda_uw_points(seed, _ptr(index), n, sqrt_s, _ptr(mom), None, 0, 0, None, _stream()), "points")
-        out = self.outputs[: n * self.helicities]
-        self.batch.update([mom], [n], [out])
-        self.batch.run(torch.cuda.current_stream())
-        return out
+class Events:
+    """One family's kept events of a run: candidate indices and weights (device tensors)."""
+
+    def __init__(self, index, weight):
+        self.index, self.weight = index, weight
 
 
 class Pipeline:
-    """Plain and two-stage unweighting over `families` at sqrt(s) with jet cuts."""
+    """Plain and two-stage unweighting over `families` at sqrt(s) with jet cuts. Every step works
+    on all families at once: the candidates of every family listed (one read of the counts), the
+    exact evaluations of every family in one batched launch of the runner."""
 
     def __init__(self, families=None, sqrt_s=ECM, cuts=(20.0, 5.0, 0.4), seed=20261204, capacity=1 << 20):
         import torch
@@ -113,94 +115,130 @@ class Pipeline:
         self.cuts = Cuts(*cuts)
         self.seed = int(seed)
         self.inputs = 5 + len(self.names)
-        self.fams = [Family(n, k, capacity) for k, n in enumerate(self.names)]
-        self.index = torch.empty(capacity, dtype=torch.int64, device="cuda")
-        self.kept = torch.empty(capacity, dtype=torch.int64, device="cuda")
-        self.kept_s = torch.empty(capacity, dtype=torch.float64, device="cuda")
-        self.counters = torch.zeros(2, dtype=torch.int64, device="cuda")
-        self.jac = torch.empty(capacity, dtype=torch.float64, device="cuda")
-        self.keep = torch.empty(capacity, dtype=torch.uint8, device="cuda")
-        self.weight = torch.empty(capacity, dtype=torch.float64, device="cuda")
-        self.me = torch.empty(capacity, dtype=torch.float64, device="cuda")
         self.capacity = capacity
+        self.fams = [Family(n, k, capacity) for k, n in enumerate(self.names)]
+        nf = len(self.fams)
+        self.counters = torch.zeros(2 * nf, dtype=torch.int64, device="cuda")
+        self.batch = B.Batch([f.plan for f in self.fams], [f.momenta[: 20 * 1024] for f in self.fams],
+                             [f.outputs[: 1024 * f.helicities] for f in self.fams])
 
     def family_seed(self, k):
         return (self.seed * 1000003 + 7919 * (k + 1)) & ((1 << 64) - 1)
 
-    # ---- candidates inside the cuts and their exact weights ------------------------------------
+    # ---- steps on every family ----------------------------------------------------------------
+
+    def candidates(self, first, counts):
+        """Lists the candidates first .. first + counts[k] - 1 of every family k inside the cuts
+        into the families' `cand` buffers (in no particular order); their numbers."""
+        nf = len(self.fams)
+        self.counters[:nf].zero_()
+        for k, (fam, c) in enumerate(zip(self.fams, counts)):
+            if c:
+                _check(_lib().pacuda_uw_candidates(self.family_seed(k), first, c, self.sqrt_s, C.byref(self.cuts),
+                                                   _ptr(fam.cand), self.capacity, _ptr(self.counters[k:k + 1]),
+                                                   _stream()), "candidates")
+        n = [int(v) for v in self.counters[:nf].tolist()]
+        if max(n) > self.capacity:
+            raise S.SurrogateError(f"{max(n)} passing candidates exceed the capacity {self.capacity}")
+        return n
+
+    def exact(self, index, n, jac=True, inputs=None):
+        """The f64 runner's outputs for candidates index[k][:n[k]] of every family (one batched
+        launch; a family without points runs one stale point whose output is not used), with J into
+        the families' `jac` buffers and, optionally, the network's inputs into inputs[k]."""
+        import torch
+
+        moms, outs, counts = [], [], []
+        for k, (fam, idx, m) in enumerate(zip(self.fams, index, n)):
+            if m:
+                x = inputs[k] if inputs else None
+                _check(_lib().pacuda_uw_points(self.family_seed(k), _ptr(idx), m, self.sqrt_s, _ptr(fam.momenta),
+                                               _ptr(x) if x is not None else None, self.inputs if x is not None else 0,
+                                               k, _ptr(fam.jac) if jac else None, _stream()), "points")
+            mm = max(1, m)
+            moms.append(fam.momenta[: 20 * mm])
+            outs.append(fam.outputs[: mm * fam.helicities])
+            counts.append(mm)
+        self.batch.update(moms, counts, outs)
+        self.batch.run(torch.cuda.current_stream())
+        return [o.view(-1, f.helicities)[:m] for o, f, m in zip(outs, self.fams, n)]
+
+    def tune(self):
+        """Times the runner's launch choices on the points of the last exact evaluation (batch_tune)."""
+        self.batch.tune()
+
+    # ---- labelled points ------------------------------------------------------------------------
 
     def passing(self, k, first, count, sort=True):
         """Indices of the candidates first .. first + count - 1 of family k inside the cuts (sorted,
-        a new tensor; or in no particular order, a view of this pipeline's index buffer)."""
+        a new tensor; or in no particular order, a view of the family's buffer)."""
         import torch
 
-        self.counters.zero_()
-        _check(_lib().pacuda_uw_candidates(self.family_seed(k), first, count, self.sqrt_s, C.byref(self.cuts),
-                                           _ptr(self.index), self.capacity, _ptr(self.counters), _stream()),
-               "candidates")
-        n = int(self.counters[0].item())
-        if n > self.capacity:
-            raise S.SurrogateError(f"{n} passing candidates exceed the capacity {self.capacity}")
-        return torch.sort(self.index[:n])[0] if sort else self.index[:n]
+        counts = [0] * len(self.fams)
+        counts[k] = count
+        n = self.candidates(first, counts)[k]
+        idx = self.fams[k].cand[:n]
+        return torch.sort(idx)[0] if sort else idx
 
     def labelled(self, k, first, count):
-        """(inputs [n][inputs] fp32, |M|^2 [n] f64, J [n] f64, index [n]) of the passing candidates."""
+        """(inputs [n][inputs] fp32, |M|^2 [n] f64, J [n] f64, index [n]) of the candidates of
+        family k inside the cuts, in index order."""
         import torch
 
-        fam = self.fams[k]
         idx = self.passing(k, first, count)
         n = idx.numel()
         x = torch.empty(n, self.inputs, dtype=torch.float32, device="cuda")
-        jac = torch.empty(n, dtype=torch.float64, device="cuda")
-        _check(_lib().pacuda_uw_points(self.family_seed(k), _ptr(idx), n, self.sqrt_s, None, _ptr(x), self.inputs, k,
-                                       _ptr(jac), _stream()), "points")
-        out = fam.exact(self.family_seed(k), idx, n, self.sqrt_s)
-        me = out.view(n, fam.helicities).sum(dim=1)
-        return x, me, jac, idx
+        index = [self.fams[j].cand[:0] for j in range(len(self.fams))]
+        index[k] = idx
+        counts = [0] * len(self.fams)
+        counts[k] = n
+        inputs = [None] * len(self.fams)
+        inputs[k] = x
+        out = self.exact(index, counts, jac=True, inputs=inputs)[k]
+        return x, out.sum(dim=1), self.fams[k].jac[:n].clone(), idx
 
     # ---- the two pipelines -------------------------------------------------------------------
 
-    def plain(self, k, first, count, w_max):
-        """Plain unweighting of candidates first .. first + count - 1 of family k: (kept index,
-        weights, exact evaluations)."""
-        fam = self.fams[k]
-        idx = self.passing(k, first, count, sort=False)
-        n = idx.numel()
-        jac = self.jac[:n]
-        _check(_lib().pacuda_uw_points(self.family_seed(k), _ptr(idx), n, self.sqrt_s, None, None, 0, 0, _ptr(jac),
-                                       _stream()), "points")
-        out = fam.exact(self.family_seed(k), idx, n, self.sqrt_s)
-        _check(_lib().pacuda_uw_decide(self.family_seed(k), _ptr(idx), n, _ptr(out), fam.helicities, _ptr(jac), None,
-                                       w_max, 0.0, 0.0, _ptr(self.keep), _ptr(self.weight), None, _stream()), "decide")
-        keep = self.keep[:n].bool()
-        return idx[keep], self.weight[:n][keep], n
+    def plain(self, first, counts, w_max):
+        """Plain unweighting of candidates first .. first + counts[k] - 1 of every family k: the
+        kept events per family and the number of exact evaluations."""
+        n = self.candidates(first, counts)
+        cand = [f.cand for f in self.fams]
+        out = self.exact(cand, n)
+        events = []
+        for k, (fam, m) in enumerate(zip(self.fams, n)):
+            if m:
+                _check(_lib().pacuda_uw_decide(self.family_seed(k), _ptr(fam.cand), m, _ptr(out[k]), fam.helicities,
+                                               _ptr(fam.jac), None, w_max[k], 0.0, 0.0, _ptr(fam.keep),
+                                               _ptr(fam.weight), None, _stream()), "decide")
+            keep = fam.keep[:m].bool()
+            events.append(Events(fam.cand[:m][keep], fam.weight[:m][keep]))
+        return events, sum(n)
 
-    def two_stage(self, k, net, first, count, mu, sigma, s_max, r_max):
-        """Two-stage unweighting of the same candidates: (kept index, weights, exact evaluations)."""
-        import torch
-
-        fam = self.fams[k]
-        cand = self.passing(k, first, count, sort=False)
-        self.counters.zero_()
-        _check(_lib().pacuda_uw_stage1(net.handle, self.family_seed(k), _ptr(cand), cand.numel(), k, mu, sigma, s_max,
-                                       _ptr(self.kept), _ptr(self.kept_s), self.capacity, _ptr(self.counters),
-                                       _stream()), "stage 1")
-        n = int(self.counters[0].item())
-        if n > self.capacity:
-            raise S.SurrogateError(f"{n} first-stage events exceed the capacity {self.capacity}")
-        if n == 0:
-            empty = torch.empty(0, dtype=torch.int64, device="cuda")
-            return empty, torch.empty(0, dtype=torch.float64, device="cuda"), 0
-        idx, s = self.kept[:n], self.kept_s[:n]
-        jac = self.jac[:n]
-        _check(_lib().pacuda_uw_points(self.family_seed(k), _ptr(idx), n, self.sqrt_s, None, None, 0, 0, _ptr(jac),
-                                       _stream()), "points")
-        out = fam.exact(self.family_seed(k), idx, n, self.sqrt_s)
-        _check(_lib().pacuda_uw_decide(self.family_seed(k), _ptr(idx), n, _ptr(out), fam.helicities, _ptr(jac), _ptr(s),
-                                       0.0, s_max, r_max, _ptr(self.keep), _ptr(self.weight), None, _stream()),
-               "decide")
-        keep = self.keep[:n].bool()
-        return idx[keep].clone(), self.weight[:n][keep].clone(), n
+    def two_stage(self, net, first, counts, mu, sigma, s_max, r_max):
+        """Two-stage unweighting of the same candidates: the kept events per family and the number
+        of exact evaluations."""
+        nf = len(self.fams)
+        n = self.candidates(first, counts)
+        self.counters[nf:].zero_()
+        for k, (fam, m) in enumerate(zip(self.fams, n)):
+            if m:
+                _check(_lib().pacuda_uw_stage1(net.handle, self.family_seed(k), _ptr(fam.cand), m, k, mu, sigma,
+                                               s_max[k], _ptr(fam.kept), _ptr(fam.kept_s), self.capacity,
+                                               _ptr(self.counters[nf + k:nf + k + 1]), _stream()), "stage 1")
+        kept = [int(v) for v in self.counters[nf:].tolist()]
+        if max(kept) > self.capacity:
+            raise S.SurrogateError(f"{max(kept)} first-stage events exceed the capacity {self.capacity}")
+        out = self.exact([f.kept for f in self.fams], kept)
+        events = []
+        for k, (fam, m) in enumerate(zip(self.fams, kept)):
+            if m:
+                _check(_lib().pacuda_uw_decide(self.family_seed(k), _ptr(fam.kept), m, _ptr(out[k]), fam.helicities,
+                                               _ptr(fam.jac), _ptr(fam.kept_s), 0.0, s_max[k], r_max[k],
+                                               _ptr(fam.keep), _ptr(fam.weight), None, _stream()), "decide")
+            keep = fam.keep[:m].bool()
+            events.append(Events(fam.kept[:m][keep], fam.weight[:m][keep]))
+        return events, sum(kept)
 
     def surrogate_values(self, net, x, mu, sigma):
         """s = exp(mu + sigma net(x)), the network's estimate of w = |M|^2 J, for points of known
@@ -209,9 +247,12 @@ class Pipeline:
         return (mu + sigma * out.double()).exp()
 
 
-def train(net, x, y, epochs, batch=16384, lr=2e-3, lr_end=2e-5, seed=0):
-    """Adam on (x, y) for `epochs` passes in shuffled batches (whole batches only), the learning
-    rate falling geometrically from lr to lr_end; returns the mean loss of each epoch."""
+def train(net, x, y, epochs, batch=16384, lr=2e-3, lr_end=2e-5, seed=0, importance=None):
+    """Adam on (x, y) for `epochs` passes in batches (whole batches only), the learning rate
+    falling geometrically from lr to lr_end; each pass a random order of the points or, with
+    `importance` (non-negative per-point weights), as many points drawn with replacement in
+    proportion to it (the network then spends its accuracy where the drawn points are). Returns the
+    mean loss of each epoch."""
     import torch
 
     n = (x.shape[0] // batch) * batch
@@ -222,7 +263,10 @@ def train(net, x, y, epochs, batch=16384, lr=2e-3, lr_end=2e-5, seed=0):
     history = []
     step = 0
     for _ in range(epochs):
-        perm = torch.randperm(x.shape[0], device="cuda", generator=gen)[:n]
+        if importance is None:
+            perm = torch.randperm(x.shape[0], device="cuda", generator=gen)[:n]
+        else:
+            perm = torch.multinomial(importance, n, replacement=True, generator=gen)
         xs, ys = x[perm].contiguous(), y[perm].contiguous()
         loss.zero_()
         for b in range(n // batch):

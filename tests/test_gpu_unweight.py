@@ -47,7 +47,7 @@ def test_candidates_and_points_match_oracle():
     got = mom.cpu().numpy().reshape(5, 4, m).transpose(2, 0, 1)
     # exp, tanh and the boost's cancellations round differently on the device: 1e-9 relative
     assert np.allclose(got, p[keep], rtol=1e-9, atol=1e-7)
-    assert np.allclose(j.cpu().numpy(), jac[keep], rtol=1e-12, atol=0)
+    assert np.allclose(j.cpu().numpy(), jac[keep], rtol=1e-10, atol=0)
     assert np.array_equal(x.cpu().numpy(), U.features(u[keep], 0, 1))
 
 
@@ -115,20 +115,21 @@ def test_stage1_matches_oracle():
     s_max = float(np.quantile(sv, 0.99))
     pl.counters.zero_()
     L = unweight._lib()
+    f0 = pl.fams[0]
     assert L.pacuda_uw_stage1(net.handle, seed, C.c_void_p(cand.data_ptr()), cand.numel(), 0, mu, sigma, s_max,
-                              C.c_void_p(pl.kept.data_ptr()), C.c_void_p(pl.kept_s.data_ptr()), pl.capacity,
+                              C.c_void_p(f0.kept.data_ptr()), C.c_void_p(f0.kept_s.data_ptr()), pl.capacity,
                               C.c_void_p(pl.counters.data_ptr()), None) == 0
     torch.cuda.synchronize()
     assert net.error() == 0
     kept = int(pl.counters[0])
-    got = pl.kept[:kept].cpu().numpy().astype(np.uint64)
+    got = f0.kept[:kept].cpu().numpy().astype(np.uint64)
     pos = {int(c): i for i, c in enumerate(idx)}
     want_keep = u[:, 5] * s_max < sv
     borderline = np.abs(u[:, 5] * s_max - sv) <= 0.02 * np.maximum(sv, 1e-300)
     got_mask = np.zeros(len(idx), dtype=bool)
     got_mask[[pos[int(c)] for c in got]] = True
     assert np.array_equal(got_mask[~borderline], want_keep[~borderline])
-    ks = pl.kept_s[:kept].cpu().numpy()
+    ks = f0.kept_s[:kept].cpu().numpy()
     assert np.allclose(ks, sv[[pos[int(c)] for c in got]], rtol=0.05)
 
 
@@ -159,11 +160,12 @@ def test_two_stage_is_unbiased_and_gains_on_ggggg():
     s_max = unweight.maxima(s, overweight=1e-3)
     r_max = unweight.maxima(w / s, s, overweight=1e-3)
     n_cand = 1 << 20
-    idx_all = pl.passing(0, 0, n_cand)
-    xa, ma, ja, _ = pl.labelled(0, 0, n_cand)
+    xa, ma, ja, idx_all = pl.labelled(0, 0, n_cand)
     wa = (ma * ja).cpu().numpy()
-    ip, wp, exact_p = pl.plain(0, 0, n_cand, w_max)
-    i2, w2, exact_2 = pl.two_stage(0, net, 0, n_cand, mu, sigma, s_max, r_max)
+    ev, exact_p = pl.plain(0, [n_cand], [w_max])
+    ip, wp = ev[0].index, ev[0].weight
+    ev, exact_2 = pl.two_stage(net, 0, [n_cand], mu, sigma, [s_max], [r_max])
+    i2, w2 = ev[0].index, ev[0].weight
     assert exact_p == idx_all.numel()
     print(f"plain: {len(ip)} events from {exact_p} exact evaluations; two-stage: {len(i2)} from {exact_2}")
     assert len(ip) > 50 and len(i2) > 50, (len(ip), len(i2), exact_p, exact_2)
