@@ -77,6 +77,8 @@ int pacuda_sg_error(const pacuda_sg_net *net);
  * boosted; legs 0 and 1 the beams. Its phase-space weight (the density of the unit cube)
  * J = s (1 - sigma) / (128 pi^3) x 32 sigma (1 - sigma) x 5.5 (1 - cos^2 theta1) x 7 (1 - cos^2 theta2).
  * The network's inputs: x1..x5, then a one-hot of the subprocess (`family`), zeros after. */
+#define PACUDA_UW_MAX_SEGMENTS 8
+
 typedef struct pacuda_uw_cuts {
     double pt_min, eta_max, dr_min; /* pT > pt_min, |eta| < eta_max, pairwise Delta R > dr_min (legs 2-4) */
 } pacuda_uw_cuts;
@@ -86,6 +88,17 @@ typedef struct pacuda_uw_cuts {
  * all) */
 int pacuda_uw_candidates(uint64_t seed, uint64_t first, uint32_t count, double sqrt_s, const pacuda_uw_cuts *cuts,
                          uint64_t *index, uint32_t capacity, unsigned long long *counter, void *stream);
+
+/* Several subprocesses' candidate lists in one launch (each segment as pacuda_uw_candidates takes
+ * it; at most PACUDA_UW_MAX_SEGMENTS, every index array holding `capacity` entries). */
+typedef struct pacuda_uw_candidate_segment {
+    uint64_t seed, first;
+    uint32_t count;
+    uint64_t *index;
+    unsigned long long *counter;
+} pacuda_uw_candidate_segment;
+int pacuda_uw_candidates_segments(const pacuda_uw_candidate_segment *segments, uint32_t segment_count, double sqrt_s,
+                                  const pacuda_uw_cuts *cuts, uint32_t capacity, void *stream);
 
 /* the points of candidates index[0 .. n): momenta as the runner reads them (source-major,
  * [(leg * 4 + k) * n + i]), the network's inputs [i][input_count] and J (each output may be NULL) */
@@ -101,6 +114,22 @@ int pacuda_uw_points(uint64_t seed, const uint64_t *index, uint32_t n, double sq
 int pacuda_uw_stage1(const pacuda_sg_net *net, uint64_t seed, const uint64_t *index, uint32_t count, uint32_t family,
                      double mu, double sigma, double s_max, uint64_t *kept_index, double *kept_s, uint32_t capacity,
                      unsigned long long *counter, void *stream);
+
+/* Several subprocesses' first stages in one launch: segment k is stage 1 of its own candidates
+ * (seed, index[0 .. count), family, s_max) into its own outputs (kept_index, kept_s, *kept_count,
+ * which the caller zeroes); every output array holds `capacity` entries. At most
+ * PACUDA_UW_MAX_SEGMENTS segments. */
+typedef struct pacuda_uw_segment {
+    uint64_t seed;
+    const uint64_t *index;
+    uint32_t count, family;
+    double s_max;
+    uint64_t *kept_index;
+    double *kept_s;
+    unsigned long long *kept_count;
+} pacuda_uw_segment;
+int pacuda_uw_stage1_segments(const pacuda_sg_net *net, const pacuda_uw_segment *segments, uint32_t segment_count,
+                              double mu, double sigma, uint32_t capacity, void *stream);
 
 /* The decision on points whose exact |M|^2 the runner evaluated (outputs [i][helicities], summed):
  * w = |M|^2 J. Plain unweighting (s == NULL): kept when u5 w_max < w, weight max(1, w / w_max).

@@ -477,16 +477,21 @@ struct ForwardArgs {
     uint32_t inputs, count, tiles;
     float *out;
     int *error;
-    // candidates (stage 1 of two-stage unweighting): candidate index[m] of stream `seed`
-    const uint64_t *index;
-    uint64_t seed;
-    double mu, sigma, s_max;  // s = exp(mu + sigma out); kept when u5 s_max < s
-    uint32_t family;
-    uint64_t *kept_index;  // the kept candidates (unordered), at most `capacity`
-    double *kept_s;
+    // candidates (stage 1 of two-stage unweighting): segments of candidates, one per subprocess;
+    // tile t belongs to the segment whose tiles [tile_first, next tile_first) hold it
+    pacuda_uw_segment seg[PACUDA_UW_MAX_SEGMENTS];
+    uint32_t tile_first[PACUDA_UW_MAX_SEGMENTS + 1];
+    uint32_t segments;
+    double mu, sigma;  // s = exp(mu + sigma out); kept when u5 s_max < s
     uint32_t capacity;
-    unsigned long long *kept_count;  // counts every kept candidate, also beyond the capacity
 };
+
+// the segment of tile t (segments are few: a linear scan)
+__device__ __forceinline__ uint32_t segment_of(const ForwardArgs &g, uint32_t t) {
+    uint32_t k = 0;
+    while (k + 1 < g.segments && t >= g.tile_first[k + 1]) k++;
+    return k;
+}
 
 enum { FWD_FROM_X = 0, FWD_CANDIDATES = 1 };
 
@@ -597,7 +602,11 @@ __global__ void __launch_bounds__(FWD_THREADS, 2) forward_kernel(ForwardArgs g) 
         const uint32_t lane_addr = tmem + ((uint32_t)(32 * (warp & 3)) << 16);
         uint32_t accs = 0, dots = 0;
         for (uint32_t t = 0; t < my_tiles && !__any_sync(0xffffffffu, abort_flag != 0); t++) {
-            const uint32_t tile = blockIdx.x + t * gridDim.x, m = tile * 128 + r;
+            const uint32_t tile = blockIdx.x + t * gridDim.x;
+            // candidates: the tile's segment and the point's place in it
+            const uint32_t sg = MODE == FWD_CANDIDATES ? segment_of(g, tile) : 0;
+            const uint32_t m = MODE == FWD_CANDIDATES ? (tile - g.tile_first[sg]) * 128 + r : tile * 128 + r;
+            const uint32_t m_count = MODE == FWD_CANDIDATES ? g.seg[sg].count : g.count;
             // the inputs: features [32 h, 32 h + 32) of row r of A tile 0 (K = 64)
             uint32_t p[16];
             double u_keep = 1.0;
@@ -614,14 +623,15 @@ __global__ void __launch_bounds__(FWD_THREADS, 2) forward_kernel(ForwardArgs g) 
                 // the candidate's five numbers and the subprocess one-hot (the listed candidates
                 // are inside the cuts)
                 double u[pacuda::phase::UNIFORMS];
-                if (m < g.count) {
-                    cand = g.index[m];
-                    pacuda::phase::uniforms(g.seed, cand, u);
+                if (m < m_count) {
+                    cand = g.seg[sg].index[m];
+                    pacuda::phase::uniforms(g.seg[sg].seed, cand, u);
                 } else {
                     for (int k = 0; k < pacuda::phase::UNIFORMS; k++) u[k] = 0.0;
                 }
                 u_keep = u[5];
-                const bool real = m < g.count;
+                const bool real = m < m_count;
+                const uint32_t family = g.seg[sg].family;
                 float f[32];  // this half's 32 features (constant indices only)
 #pragma unroll
                 for (int k = 0; k < 32; k++) f[k] = 0.0f;
@@ -631,7 +641,7 @@ __global__ void __launch_bounds__(FWD_THREADS, 2) forward_kernel(ForwardArgs g) 
                 }
 #pragma unroll
                 for (int k = 0; k < 32; k++)
-                    if (real && 32 * h + k == 5 + g.family) f[k] = 1.0f;
+                    if (real && 32 * h + k == 5 + family) f[k] = 1.0f;
 #pragma unroll
                 for (int e = 0; e < 16; e++) p[e] = pack_bf16(f[2 * e], f[2 * e + 1]);
             }
@@ -700,18 +710,19 @@ __global__ void __launch_bounds__(FWD_THREADS, 2) forward_kernel(ForwardArgs g) 
             } else {
                 // stage 1: s = exp(mu + sigma out), the network's estimate of the weight w = |M|^2 J;
                 // kept when u5 s_max < s (warp-aggregated appends)
-                const bool real = m < g.count;
+                const pacuda_uw_segment &sgm = g.seg[sg];
+                const bool real = m < m_count;
                 const double sv = real ? exp(g.mu + g.sigma * (double)out) : 0.0;
-                const bool keep = real && u_keep * g.s_max < sv;
+                const bool keep = real && u_keep * sgm.s_max < sv;
                 const unsigned ballot = __ballot_sync(0xffffffffu, keep);
                 unsigned long long base = 0;
-                if (lane == 0 && ballot) base = atomicAdd(g.kept_count, (unsigned long long)__popc(ballot));
+                if (lane == 0 && ballot) base = atomicAdd(sgm.kept_count, (unsigned long long)__popc(ballot));
                 base = __shfl_sync(0xffffffffu, base, 0);
                 if (keep) {
                     const unsigned long long slot = base + __popc(ballot & ((1u << lane) - 1u));
                     if (slot < g.capacity) {
-                        g.kept_index[slot] = cand;
-                        g.kept_s[slot] = sv;
+                        sgm.kept_index[slot] = cand;
+                        sgm.kept_s[slot] = sv;
                     }
                 }
             }
@@ -1062,6 +1073,37 @@ __global__ void candidates_kernel(uint64_t seed, uint64_t first, uint32_t count,
     }
 }
 
+// several subprocesses' candidates in one launch: block b lists segment k's candidates when
+// block_first[k] <= b < block_first[k + 1]
+struct CandidateSegments {
+    pacuda_uw_candidate_segment seg[PACUDA_UW_MAX_SEGMENTS];
+    uint32_t block_first[PACUDA_UW_MAX_SEGMENTS + 1];
+    uint32_t segments;
+};
+
+__global__ void candidate_segments_kernel(CandidateSegments c, double sqrt_s, Cuts cuts, uint32_t capacity) {
+    uint32_t k = 0;
+    while (k + 1 < c.segments && blockIdx.x >= c.block_first[k + 1]) k++;
+    const pacuda_uw_candidate_segment &sg = c.seg[k];
+    const uint32_t i = (blockIdx.x - c.block_first[k]) * blockDim.x + threadIdx.x;
+    bool pass = false;
+    if (i < sg.count) {
+        double u[pacuda::phase::UNIFORMS], p[5][4];
+        pacuda::phase::uniforms(sg.seed, sg.first + i, u);
+        pacuda::phase::map(u, sqrt_s, p);
+        pass = pacuda::phase::passes(p, cuts);
+    }
+    const unsigned ballot = __ballot_sync(0xffffffffu, pass);
+    const int lane = threadIdx.x & 31;
+    unsigned long long base = 0;
+    if (lane == 0 && ballot) base = atomicAdd(sg.counter, (unsigned long long)__popc(ballot));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (pass) {
+        const unsigned long long slot = base + __popc(ballot & ((1u << lane) - 1u));
+        if (slot < capacity) sg.index[slot] = sg.first + i;
+    }
+}
+
 // the points of candidates index[0..n): source-major momenta [(leg * 4 + k) * n + i] for the
 // runner, the network's inputs [i][inputs] and the map's weight
 __global__ void points_kernel(uint64_t seed, const uint64_t *index, uint32_t n, double sqrt_s, double *momenta,
@@ -1122,6 +1164,28 @@ extern "C" int pacuda_uw_candidates(uint64_t seed, uint64_t first, uint32_t coun
     return failed(cudaGetLastError(), "candidates") ? ST_DEVICE : ST_OK;
 }
 
+extern "C" int pacuda_uw_candidates_segments(const pacuda_uw_candidate_segment *segs, uint32_t segments, double sqrt_s,
+                                             const pacuda_uw_cuts *cuts, uint32_t capacity, void *stream) {
+    g_last_launches = 0;
+    if (!segs || !cuts || segments == 0 || segments > PACUDA_UW_MAX_SEGMENTS || !(sqrt_s > 0)) return ST_INVALID;
+    CandidateSegments c;
+    memset(&c, 0, sizeof c);
+    uint32_t blocks = 0;
+    for (uint32_t k = 0; k < segments; k++) {
+        if ((segs[k].count && !segs[k].index) || !segs[k].counter) return ST_INVALID;
+        c.seg[k] = segs[k];
+        c.block_first[k] = blocks;
+        blocks += (segs[k].count + 255) / 256;
+    }
+    c.block_first[segments] = blocks;
+    c.segments = segments;
+    if (blocks == 0) return ST_OK;
+    candidate_segments_kernel<<<blocks, 256, 0, (cudaStream_t)stream>>>(c, sqrt_s, Cuts{cuts->pt_min, cuts->eta_max,
+                                                                                       cuts->dr_min}, capacity);
+    g_last_launches++;
+    return failed(cudaGetLastError(), "candidates") ? ST_DEVICE : ST_OK;
+}
+
 extern "C" int pacuda_uw_points(uint64_t seed, const uint64_t *index, uint32_t n, double sqrt_s, double *momenta,
                                 float *inputs, uint32_t input_count, uint32_t family, double *jac, void *stream) {
     g_last_launches = 0;
@@ -1145,30 +1209,52 @@ extern "C" int pacuda_uw_decide(uint64_t seed, const uint64_t *index, uint32_t n
     return failed(cudaGetLastError(), "decide") ? ST_DEVICE : ST_OK;
 }
 
-extern "C" int pacuda_uw_stage1(const pacuda_sg_net *n, uint64_t seed, const uint64_t *index, uint32_t count,
-                                uint32_t family, double mu, double sigma, double s_max,
-                                uint64_t *kept_index, double *kept_s, uint32_t capacity, unsigned long long *counter,
-                                void *stream) {
+extern "C" int pacuda_uw_stage1_segments(const pacuda_sg_net *n, const pacuda_uw_segment *segs, uint32_t segments,
+                                         double mu, double sigma, uint32_t capacity, void *stream) {
     g_last_launches = 0;
-    if (!n || !index || !kept_index || !kept_s || !counter || 5 + family >= n->inputs) return ST_INVALID;
-    if (count == 0) return ST_OK;
+    if (!n || !segs || segments == 0 || segments > PACUDA_UW_MAX_SEGMENTS) {
+        fprintf(stderr, "%s: stage 1: 1 to %d segments\n", kTag, PACUDA_UW_MAX_SEGMENTS);
+        return ST_INVALID;
+    }
     ForwardArgs g;
     memset(&g, 0, sizeof g);
+    uint32_t tiles = 0;
+    for (uint32_t k = 0; k < segments; k++) {
+        const pacuda_uw_segment &sg = segs[k];
+        if ((sg.count && !sg.index) || !sg.kept_index || !sg.kept_s || !sg.kept_count || 5 + sg.family >= n->inputs) {
+            fprintf(stderr, "%s: stage 1: segment %u: a missing array or a family beyond the inputs\n", kTag, k);
+            return ST_INVALID;
+        }
+        g.seg[k] = sg;
+        g.tile_first[k] = tiles;
+        tiles += (sg.count + 127) / 128;
+    }
+    g.tile_first[segments] = tiles;
+    if (tiles == 0) return ST_OK;
+    g.segments = segments;
     g.wimg = n->wimg;
     g.params = n->params;
     g.inputs = n->inputs;
-    g.count = count;
-    g.tiles = (count + 127) / 128;
+    g.tiles = tiles;
     g.error = n->error;
-    g.index = index;
-    g.seed = seed;
     g.mu = mu;
     g.sigma = sigma;
-    g.s_max = s_max;
-    g.family = family;
-    g.kept_index = kept_index;
-    g.kept_s = kept_s;
     g.capacity = capacity;
-    g.kept_count = counter;
     return launch_forward<FWD_CANDIDATES>(g, (cudaStream_t)stream) ? ST_OK : ST_DEVICE;
+}
+
+extern "C" int pacuda_uw_stage1(const pacuda_sg_net *n, uint64_t seed, const uint64_t *index, uint32_t count,
+                                uint32_t family, double mu, double sigma, double s_max, uint64_t *kept_index,
+                                double *kept_s, uint32_t capacity, unsigned long long *counter, void *stream) {
+    pacuda_uw_segment sg;
+    sg.seed = seed;
+    sg.index = index;
+    sg.count = count;
+    sg.family = family;
+    sg.s_max = s_max;
+    sg.kept_index = kept_index;
+    sg.kept_s = kept_s;
+    sg.kept_count = counter;
+    if (!index) return ST_INVALID;
+    return pacuda_uw_stage1_segments(n, &sg, 1, mu, sigma, capacity, stream);
 }

@@ -40,6 +40,16 @@ class Cuts(C.Structure):
     _fields_ = [("pt_min", C.c_double), ("eta_max", C.c_double), ("dr_min", C.c_double)]
 
 
+class CandidateSegment(C.Structure):  # pacuda_uw_candidate_segment
+    _fields_ = [("seed", C.c_uint64), ("first", C.c_uint64), ("count", C.c_uint32), ("index", C.c_void_p),
+                ("counter", C.c_void_p)]
+
+
+class Segment(C.Structure):  # pacuda_uw_segment
+    _fields_ = [("seed", C.c_uint64), ("index", C.c_void_p), ("count", C.c_uint32), ("family", C.c_uint32),
+                ("s_max", C.c_double), ("kept_index", C.c_void_p), ("kept_s", C.c_void_p), ("kept_count", C.c_void_p)]
+
+
 def _lib():
     L = S.lib()
     if not getattr(L, "_uw_bound", False):
@@ -53,6 +63,10 @@ def _lib():
         L.pacuda_uw_stage1.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint32, C.c_uint32, C.c_double,
                                        C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p,
                                        C.c_void_p]
+        L.pacuda_uw_candidates_segments.argtypes = [C.c_void_p, C.c_uint32, C.c_double, C.c_void_p, C.c_uint32,
+                                                    C.c_void_p]
+        L.pacuda_uw_stage1_segments.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_double, C.c_double, C.c_uint32,
+                                                C.c_void_p]
         L._uw_bound = True
     return L
 
@@ -132,11 +146,12 @@ class Pipeline:
         into the families' `cand` buffers (in no particular order); their numbers."""
         nf = len(self.fams)
         self.counters[:nf].zero_()
+        segs = (CandidateSegment * nf)()
         for k, (fam, c) in enumerate(zip(self.fams, counts)):
-            if c:
-                _check(_lib().pacuda_uw_candidates(self.family_seed(k), first, c, self.sqrt_s, C.byref(self.cuts),
-                                                   _ptr(fam.cand), self.capacity, _ptr(self.counters[k:k + 1]),
-                                                   _stream()), "candidates")
+            segs[k] = CandidateSegment(self.family_seed(k), first, int(c), fam.cand.data_ptr(),
+                                       self.counters[k:k + 1].data_ptr())
+        _check(_lib().pacuda_uw_candidates_segments(segs, nf, self.sqrt_s, C.byref(self.cuts), self.capacity,
+                                                    _stream()), "candidates")
         n = [int(v) for v in self.counters[:nf].tolist()]
         if max(n) > self.capacity:
             raise S.SurrogateError(f"{max(n)} passing candidates exceed the capacity {self.capacity}")
@@ -221,11 +236,11 @@ class Pipeline:
         nf = len(self.fams)
         n = self.candidates(first, counts)
         self.counters[nf:].zero_()
+        segs = (Segment * nf)()
         for k, (fam, m) in enumerate(zip(self.fams, n)):
-            if m:
-                _check(_lib().pacuda_uw_stage1(net.handle, self.family_seed(k), _ptr(fam.cand), m, k, mu, sigma,
-                                               s_max[k], _ptr(fam.kept), _ptr(fam.kept_s), self.capacity,
-                                               _ptr(self.counters[nf + k:nf + k + 1]), _stream()), "stage 1")
+            segs[k] = Segment(self.family_seed(k), fam.cand.data_ptr(), m, k, s_max[k], fam.kept.data_ptr(),
+                              fam.kept_s.data_ptr(), self.counters[nf + k:nf + k + 1].data_ptr())
+        _check(_lib().pacuda_uw_stage1_segments(net.handle, segs, nf, mu, sigma, self.capacity, _stream()), "stage 1")
         kept = [int(v) for v in self.counters[nf:].tolist()]
         if max(kept) > self.capacity:
             raise S.SurrogateError(f"{max(kept)} first-stage events exceed the capacity {self.capacity}")

@@ -135,8 +135,8 @@ def test_stage1_matches_oracle():
 
 def test_two_stage_is_unbiased_and_gains_on_ggggg():
     """g g -> g g g at 13 TeV: a surrogate of log w trained for a few seconds on the labelled points
-    of 2^19 candidates;
-    two-stage and plain unweighting of the same 2^20 candidates, both with reduced maxima (0.1 % of
+    of 2^20 candidates;
+    two-stage and plain unweighting of the same 2^20 candidates, both with reduced maxima (1 % of
     the total above them). Both samples' histograms of the
     leading parton's pT, its pseudorapidity and m23 agree with the exact weighted histogram
     (chi^2 per bin below 2.5), and the two-stage events per exact evaluation exceed plain's."""
@@ -146,19 +146,20 @@ def test_two_stage_is_unbiased_and_gains_on_ggggg():
     from pacuda_b200 import unweight
 
     pl = _pipeline(capacity=1 << 20)
-    x, me, jac, _ = pl.labelled(0, 1 << 30, 1 << 19)
+    x, me, jac, _ = pl.labelled(0, 1 << 30, 1 << 20)
     w = me * jac
     logw = w.log()
     mu, sigma = float(logw.mean()), float(logw.std())
     y = ((logw - mu) / sigma).float()
-    net = S.Network(6, max_batch=8192, seed=3)
-    unweight.train(net, x, y, epochs=30, batch=8192, lr=2e-3, lr_end=1e-5)
+    net = S.Network(6, max_batch=4096, seed=3)
+    imp = (0.5 * (logw - logw.max())).exp().float()  # training points drawn in proportion to w^0.5
+    unweight.train(net, x, y, epochs=80, batch=4096, lr=2e-3, lr_end=1e-5, importance=imp)
     assert net.error() == 0
     s = pl.surrogate_values(net, x, mu, sigma)
-    # reduced maxima: at most 0.1 % of the total above each (those events keep weights above 1)
-    w_max = unweight.maxima(w, overweight=1e-3)
-    s_max = unweight.maxima(s, overweight=1e-3)
-    r_max = unweight.maxima(w / s, s, overweight=1e-3)
+    # reduced maxima: at most 1 % of the total above each (those events keep weights above 1)
+    w_max = unweight.maxima(w, overweight=1e-2)
+    s_max = unweight.maxima(s, overweight=1e-2)
+    r_max = unweight.maxima(w / s, s, overweight=1e-2)
     n_cand = 1 << 20
     xa, ma, ja, idx_all = pl.labelled(0, 0, n_cand)
     wa = (ma * ja).cpu().numpy()

@@ -216,6 +216,21 @@ def test_library_loads_and_exports_every_declared_symbol():
         assert hasattr(lib, name), name
 
 
+def test_surrogate_library_exports_every_declared_symbol():
+    """libsurrogate.so loads without a GPU and exports every function include/pacuda_surrogate.h
+    declares (no compute calls)."""
+    from pacuda_b200 import build
+    build.build()
+    lib = C.CDLL(build.SG_LIB)
+    text = open(os.path.join(ROOT, "include", "pacuda_surrogate.h")).read()
+    names = set(re.findall(r"\b(pacuda_(?:sg|uw)_\w+)\s*\(", text))
+    assert {"pacuda_sg_create", "pacuda_sg_train_step", "pacuda_sg_forward", "pacuda_uw_stage1"} <= names
+    for name in sorted(names):
+        assert hasattr(lib, name), name
+    lib.pacuda_sg_param_count.restype = C.c_size_t
+    assert lib.pacuda_sg_param_count() == 256 * 64 + 3 * 256 * 256 + 5 * 256 + 1
+
+
 def test_abi_struct_layout_is_the_references():
     """The ctypes mirror has the reference's layout (runner/pacman_recurrence.h:18-138 on LP64, as
     gcc lays out both that header and include/pacman_recurrence.h)."""
