@@ -211,7 +211,7 @@ def precision_line(torch, B, fams, ext, ref_out, steps, warmup, kind="mixed"):
             "blocks_per_sm": {nm: batch.plan_blocks_per_sm(k) for k, (nm, _, _) in enumerate(fams)}}
 
 
-def surrogate_line(torch, train_points=1 << 22, candidates=1 << 22, epochs=150, batch=16384, steps=3, alpha=0.5,
+def surrogate_line(torch, train_points=1 << 22, candidates=1 << 22, epochs=300, batch=16384, steps=3, alpha=0.5,
                    lr=2e-3, overweight=None):
     """The learned part: a surrogate of the weight w = |M|^2 J of p p -> 3 jets candidates (one
     network, the five unit-cube numbers and a subprocess one-hot as inputs, 4 x 256 SiLU, BF16

@@ -514,7 +514,7 @@ __global__ void __launch_bounds__(FWD_THREADS, 2) forward_kernel(ForwardArgs g) 
     __shared__ uint64_t full[FWD_STAGES], empty[FWD_STAGES], act_ready, acc_ready, dot_ready;
     __shared__ uint32_t tmem_base;
     __shared__ volatile int abort_flag;
-    __shared__ float prm[FWD_PARAMS];
+    __shared__ __align__(16) float prm[FWD_PARAMS];
     __shared__ float dot_hi[128];
     const uint32_t pad = (1024u - (smem_u32(smem_raw) & 1023u)) & 1023u;
     uint8_t *act = smem_raw + pad;         // 4 A tiles: the activations (K = 256)
@@ -664,22 +664,40 @@ __global__ void __launch_bounds__(FWD_THREADS, 2) forward_kernel(ForwardArgs g) 
                 accs++;
                 tc_fence_after();
                 const float *bias = prm + layer * WIDTH;
-                for (int c = 4 * h; c < 4 * h + 4; c++) {
-                    float v[32];
-                    tmem_load32(lane_addr + 32 * c, v);
+                // this half's 128 columns in eight pieces of 16, each piece's tensor-memory load
+                // issued before the previous piece is computed (its latency hidden behind the math)
+                uint32_t buf[2][16];
+                tmem_load16_async(lane_addr + 128 * h, buf[0]);
+#pragma unroll
+                for (int piece = 0; piece < 8; piece++) {
+                    uint32_t(&cur)[16] = buf[piece & 1];
+                    tmem_wait16(cur);
+                    if (piece + 1 < 8) tmem_load16_async(lane_addr + 128 * h + 16 * (piece + 1), buf[(piece + 1) & 1]);
+                    const int col = 128 * h + 16 * piece;
+                    const float4 *b4 = reinterpret_cast<const float4 *>(bias + col);
+                    float bb[16];
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        const float4 t4 = b4[q];
+                        bb[4 * q] = t4.x;
+                        bb[4 * q + 1] = t4.y;
+                        bb[4 * q + 2] = t4.z;
+                        bb[4 * q + 3] = t4.w;
+                    }
                     if (layer < 3) {
-                        uint32_t ph[16];
+                        uint32_t ph[8];
 #pragma unroll
-                        for (int j = 0; j < 32; j += 2)
-                            ph[j / 2] = pack_bf16(silu(v[j] + bias[32 * c + j]), silu(v[j + 1] + bias[32 * c + j + 1]));
+                        for (int j = 0; j < 16; j += 2)
+                            ph[j / 2] = pack_bf16(silu(__uint_as_float(cur[j]) + bb[j]),
+                                                  silu(__uint_as_float(cur[j + 1]) + bb[j + 1]));
 #pragma unroll
-                        for (int q = 0; q < 4; q++)
-                            *reinterpret_cast<uint4 *>(act + (c / 2) * TILE_A + sw128_offset(r, (32 * c) % 64 + 8 * q)) =
+                        for (int q = 0; q < 2; q++)
+                            *reinterpret_cast<uint4 *>(act + (col / 64) * TILE_A + sw128_offset(r, col % 64 + 8 * q)) =
                                 make_uint4(ph[4 * q], ph[4 * q + 1], ph[4 * q + 2], ph[4 * q + 3]);
                     } else {
-                        const float *w5 = prm + 4 * WIDTH;
+                        const float *w5 = prm + 4 * WIDTH + col;
 #pragma unroll
-                        for (int j = 0; j < 32; j++) out += bf16_round(silu(v[j] + bias[32 * c + j])) * w5[32 * c + j];
+                        for (int j = 0; j < 16; j++) out += bf16_round(silu(__uint_as_float(cur[j]) + bb[j])) * w5[j];
                     }
                 }
                 if (layer < 3) {

@@ -98,6 +98,26 @@ __device__ __forceinline__ void tmem_load32(uint32_t taddr, float *v) {
     for (int k = 0; k < 32; k++) v[k] = __uint_as_float(r[k]);
 }
 
+// 32 lanes x 16 consecutive FP32 columns from `taddr`, not yet waited for: the registers may be
+// read only after tmem_wait16 on the same array (which ties their uses to the wait)
+__device__ __forceinline__ void tmem_load16_async(uint32_t taddr, uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+}
+// waits for every tensor-memory load this thread issued; `r` (the last load's registers) is
+// read and written here so that no use of it moves above the wait
+__device__ __forceinline__ void tmem_wait16(uint32_t (&r)[16]) {
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]),
+                   "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15])
+                 :
+                 : "memory");
+}
+
 // ---- descriptors and the MMA ---------------------------------------------------------------------
 
 // shared-memory matrix descriptor of a K-major, 128-byte-swizzled operand starting at `addr`
