@@ -308,16 +308,19 @@ def surrogate_line(torch, train_points=1 << 22, candidates=1 << 22, epochs=300, 
         e0.record()
         for _ in range(steps):
             events, exact = run(kind)
+            counts_dev = torch.stack([e.count() for e in events])  # the step's kept events, on the device
         e1.record()
         e1.synchronize()
         ms = e0.elapsed_time(e1) / steps
-        kept = sum(int(e.index.numel()) for e in events)
+        per_family = [int(v) for v in counts_dev.tolist()]
+        kept = sum(per_family)
+        compact = [e.compact() for e in events]
         lines[kind] = {"ms_per_step": ms, "events": kept, "exact_evaluations": exact,
                        "events_per_s": kept / (ms * 1e-3), "candidates_per_s": candidates / (ms * 1e-3),
                        "efficiency_per_exact": kept / max(1, exact), "efficiency_per_candidate": kept / candidates,
-                       "overweight_events": int(sum(int((e.weight > 1).sum()) for e in events)),
-                       "events_per_family": {nm: int(e.index.numel()) for nm, e in zip(fams, events)}}
-        lines[kind]["_events"] = [(e.index.clone(), e.weight.clone()) for e in events]
+                       "overweight_events": int(sum(int((w > 1).sum()) for _, w in compact)),
+                       "events_per_family": dict(zip(fams, per_family))}
+        lines[kind]["_events"] = compact
     res["plain"] = {k: v for k, v in lines["plain"].items() if not k.startswith("_")}
     res["two_stage"] = {k: v for k, v in lines["two_stage"].items() if not k.startswith("_")}
     res["events_per_s_ratio"] = lines["two_stage"]["events_per_s"] / lines["plain"]["events_per_s"]
@@ -392,9 +395,10 @@ def surrogate_kernels(torch, count=1 << 21, steps=5):
     pl = UW.Pipeline(families=FAMILIES[:1], capacity=count)
     cand = torch.arange(count, dtype=torch.int64, device="cuda")  # a candidate list (the weights do not matter)
     res = {}
-    for what in ("forward", "stage1"):
+    for what, blocks in (("forward", 2), ("stage1", 2), ("forward_1_block_per_sm", 1), ("stage1_1_block_per_sm", 1)):
+        S.set_inference_blocks(blocks)
         def launch():
-            if what == "forward":
+            if what.startswith("forward"):
                 net.forward(x, out)
             else:
                 pl.counters.zero_()
@@ -411,7 +415,8 @@ def surrogate_kernels(torch, count=1 << 21, steps=5):
         e1.synchronize()
         ms = e0.elapsed_time(e1) / steps
         res[what] = {"points": count, "ms": ms, "points_per_s": count / (ms * 1e-3),
-                     "tflops": count * flops / (ms * 1e-3) / 1e12}
+                     "tflops": count * flops / (ms * 1e-3) / 1e12, "blocks_per_sm": blocks}
+    S.set_inference_blocks(2)
     if net.error():
         raise RuntimeError(f"surrogate kernels reported error {net.error()}")
     return res

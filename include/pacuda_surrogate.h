@@ -139,6 +139,11 @@ int pacuda_uw_decide(uint64_t seed, const uint64_t *index, uint32_t n, const dou
                      const double *jac, const double *s, double w_max, double s_max, double r_max, uint8_t *keep,
                      double *weight, double *me, void *stream);
 
+/* Blocks per SM of the fused inference kernel (pacuda_sg_forward, the first stage): 2 (the
+ * default; two blocks whose products and epilogues overlap, a 2-stage weight ring each) or 1 (one
+ * block with a 9-stage weight ring); INVALID otherwise. Applies to later launches in the process. */
+int pacuda_sg_set_inference_blocks(uint32_t blocks);
+
 /* kernel launches made by the last call of each entry point (0 for none) */
 uint32_t pacuda_sg_last_launches(void);
 

@@ -465,8 +465,12 @@ __global__ void adam_kernel(float *params, float *m1, float *m2, const float *gr
 constexpr int FWD_EPI_THREADS = 256;
 constexpr int FWD_THREADS = FWD_EPI_THREADS + 64;
 constexpr uint32_t FWD_CHUNK = 128 * 128;  // 16 KB
-constexpr int FWD_STAGES = 2;
-constexpr uint32_t FWD_SMEM = 4 * TILE_A + FWD_STAGES * FWD_CHUNK + 1024;
+// the weight ring's stages for one or two blocks per SM (the shared memory left beside the 64 KB of
+// activations), and the dynamic shared memory of a block
+template <int CTAS> struct FwdShape {
+    static constexpr int STAGES = CTAS == 1 ? 9 : 2;
+    static constexpr uint32_t SMEM = 4 * TILE_A + STAGES * FWD_CHUNK + 1024;
+};
 constexpr int FWD_CHUNKS = 2 + 3 * 8;  // per tile: layer 1 (1 k tile x 2 halves), layers 2-4 (4 x 2)
 constexpr int FWD_PARAMS = 5 * WIDTH + 1;  // b1..b4, w5, b5
 
@@ -508,8 +512,9 @@ __device__ __forceinline__ void fwd_chunk(int c, int &layer, int &kt, int &half)
     }
 }
 
-template <int MODE>
-__global__ void __launch_bounds__(FWD_THREADS, 2) forward_kernel(ForwardArgs g) {
+template <int MODE, int CTAS>
+__global__ void __launch_bounds__(FWD_THREADS, CTAS) forward_kernel(ForwardArgs g) {
+    constexpr int FWD_STAGES = FwdShape<CTAS>::STAGES;
     extern __shared__ uint8_t smem_raw[];
     __shared__ uint64_t full[FWD_STAGES], empty[FWD_STAGES], act_ready, acc_ready, dot_ready;
     __shared__ uint32_t tmem_base;
@@ -778,11 +783,16 @@ bool launch_gemm(const GemmArgs &g, uint32_t m_tiles, uint32_t splits, cudaStrea
     return !failed(cudaGetLastError(), "product kernel launch");
 }
 
-template <int MODE>
-bool launch_forward(const ForwardArgs &g, cudaStream_t s) {
+// blocks per SM of the inference kernel: 2 (two blocks, a 2-stage weight ring each) or 1 (one
+// block, a 9-stage ring)
+int g_forward_blocks = 2;
+
+template <int MODE, int CTAS>
+bool launch_forward_shape(const ForwardArgs &g, cudaStream_t s) {
     static bool configured = false;
     if (!configured) {
-        if (failed(cudaFuncSetAttribute(forward_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, FWD_SMEM),
+        if (failed(cudaFuncSetAttribute(forward_kernel<MODE, CTAS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        FwdShape<CTAS>::SMEM),
                    "inference kernel attributes"))
             return false;
         configured = true;
@@ -790,10 +800,15 @@ bool launch_forward(const ForwardArgs &g, cudaStream_t s) {
     int dev = 0, sms = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const uint32_t grid = std::min<uint32_t>(g.tiles, 2u * (uint32_t)sms);
-    forward_kernel<MODE><<<grid, FWD_THREADS, FWD_SMEM, s>>>(g);
+    const uint32_t grid = std::min<uint32_t>(g.tiles, (uint32_t)CTAS * (uint32_t)sms);
+    forward_kernel<MODE, CTAS><<<grid, FWD_THREADS, FwdShape<CTAS>::SMEM, s>>>(g);
     g_last_launches++;
     return !failed(cudaGetLastError(), "inference launch");
+}
+
+template <int MODE>
+bool launch_forward(const ForwardArgs &g, cudaStream_t s) {
+    return g_forward_blocks == 1 ? launch_forward_shape<MODE, 1>(g, s) : launch_forward_shape<MODE, 2>(g, s);
 }
 
 }  // namespace
@@ -839,6 +854,12 @@ int refresh_images(pacuda_sg_net *n, cudaStream_t s) {
 extern "C" size_t pacuda_sg_param_count(void) { return P_COUNT; }
 
 extern "C" uint32_t pacuda_sg_last_launches(void) { return g_last_launches; }
+
+extern "C" int pacuda_sg_set_inference_blocks(uint32_t blocks) {
+    if (blocks != 1 && blocks != 2) return ST_INVALID;
+    g_forward_blocks = (int)blocks;
+    return ST_OK;
+}
 
 extern "C" void pacuda_sg_destroy(pacuda_sg_net *n) {
     if (!n) return;

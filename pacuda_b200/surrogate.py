@@ -37,6 +37,7 @@ def lib():
         L.pacuda_sg_forward.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]
         L.pacuda_sg_last_launches.restype = C.c_uint32
         L.pacuda_sg_error.argtypes = [C.c_void_p]
+        L.pacuda_sg_set_inference_blocks.argtypes = [C.c_uint32]
         _lib = L
     return _lib
 
@@ -106,6 +107,11 @@ class Network:
 
     def error(self):
         return lib().pacuda_sg_error(self.handle)
+
+
+def set_inference_blocks(blocks):
+    """Blocks per SM of the fused inference kernel (1 or 2)."""
+    _check(lib().pacuda_sg_set_inference_blocks(int(blocks)), "set_inference_blocks")
 
 
 def last_launches():

@@ -110,10 +110,20 @@ class Family:
 
 
 class Events:
-    """One family's kept events of a run: candidate indices and weights (device tensors)."""
+    """One family's decided points of a run: candidate indices, keep flags and weights (views of the
+    family's device buffers, valid until its next run); `compact()` gives the kept events alone."""
 
-    def __init__(self, index, weight):
-        self.index, self.weight = index, weight
+    def __init__(self, index, keep, weight):
+        self.points, self.keep_flags, self.all_weights = index, keep, weight
+
+    def count(self):
+        """The number of kept events, as a device tensor (no host synchronisation)."""
+        return self.keep_flags.sum(dtype=self.points.dtype) if self.points.numel() else self.points.new_zeros(())
+
+    def compact(self):
+        """(indices, weights) of the kept events (new tensors)."""
+        keep = self.keep_flags.bool()
+        return self.points[keep].clone(), self.all_weights[keep].clone()
 
 
 class Pipeline:
@@ -226,8 +236,7 @@ class Pipeline:
                 _check(_lib().pacuda_uw_decide(self.family_seed(k), _ptr(fam.cand), m, _ptr(out[k]), fam.helicities,
                                                _ptr(fam.jac), None, w_max[k], 0.0, 0.0, _ptr(fam.keep),
                                                _ptr(fam.weight), None, _stream()), "decide")
-            keep = fam.keep[:m].bool()
-            events.append(Events(fam.cand[:m][keep], fam.weight[:m][keep]))
+            events.append(Events(fam.cand[:m], fam.keep[:m], fam.weight[:m]))
         return events, sum(n)
 
     def two_stage(self, net, first, counts, mu, sigma, s_max, r_max):
@@ -251,8 +260,7 @@ class Pipeline:
                 _check(_lib().pacuda_uw_decide(self.family_seed(k), _ptr(fam.kept), m, _ptr(out[k]), fam.helicities,
                                                _ptr(fam.jac), _ptr(fam.kept_s), 0.0, s_max[k], r_max[k],
                                                _ptr(fam.keep), _ptr(fam.weight), None, _stream()), "decide")
-            keep = fam.keep[:m].bool()
-            events.append(Events(fam.kept[:m][keep], fam.weight[:m][keep]))
+            events.append(Events(fam.kept[:m], fam.keep[:m], fam.weight[:m]))
         return events, sum(kept)
 
     def surrogate_values(self, net, x, mu, sigma):

@@ -164,9 +164,10 @@ def test_two_stage_is_unbiased_and_gains_on_ggggg():
     xa, ma, ja, idx_all = pl.labelled(0, 0, n_cand)
     wa = (ma * ja).cpu().numpy()
     ev, exact_p = pl.plain(0, [n_cand], [w_max])
-    ip, wp = ev[0].index, ev[0].weight
+    ip, wp = ev[0].compact()
+    assert int(ev[0].count()) == len(ip)
     ev, exact_2 = pl.two_stage(net, 0, [n_cand], mu, sigma, [s_max], [r_max])
-    i2, w2 = ev[0].index, ev[0].weight
+    i2, w2 = ev[0].compact()
     assert exact_p == idx_all.numel()
     print(f"plain: {len(ip)} events from {exact_p} exact evaluations; two-stage: {len(i2)} from {exact_2}")
     assert len(ip) > 50 and len(i2) > 50, (len(ip), len(i2), exact_p, exact_2)
