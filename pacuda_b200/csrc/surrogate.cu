@@ -61,7 +61,9 @@ __device__ __forceinline__ float tanh_fast(float x) {
     asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
     return y;
 }
-__device__ __forceinline__ float silu(float z) { return 0.5f * z * (1.0f + tanh_fast(0.5f * z)); }
+// silu(z) = z (1 + tanh(z / 2)) / 2 = hz + hz tanh(hz) with hz = z / 2 (one MUFU, one FMA)
+__device__ __forceinline__ float silu_of_half(float hz) { return fmaf(hz, tanh_fast(hz), hz); }
+__device__ __forceinline__ float silu(float z) { return silu_of_half(0.5f * z); }
 __device__ __forceinline__ float silu_grad(float z) {
     const float s = 0.5f + 0.5f * tanh_fast(0.5f * z);
     return s * (1.0f + z * (1.0f - s));
@@ -71,6 +73,17 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
     return *reinterpret_cast<uint32_t *>(&v);
 }
 __device__ __forceinline__ float bf16_round(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
+// two FP32 values rounded to BF16 (nearest, ties to even) and packed, by integer arithmetic on the
+// ALU pipe (finite inputs): the same bits as pack_bf16
+__device__ __forceinline__ uint32_t pack_bf16_alu(float lo, float hi) {
+    const uint32_t a = __float_as_uint(lo), b = __float_as_uint(hi);
+    const uint32_t ra = (a + 0x7fffu + ((a >> 16) & 1u)) >> 16, rb = (b + 0x7fffu + ((b >> 16) & 1u)) & 0xffff0000u;
+    return ra | rb;
+}
+__device__ __forceinline__ float bf16_round_alu(float x) {
+    const uint32_t a = __float_as_uint(x);
+    return __uint_as_float((a + 0x7fffu + ((a >> 16) & 1u)) & 0xffff0000u);
+}
 
 // byte offset of element (r, k) in an A image whose row tiles hold `kt` tiles of 64 values of K
 __device__ __forceinline__ size_t a_img(uint32_t r, uint32_t k, uint32_t kt) {
@@ -538,9 +551,10 @@ __global__ void __launch_bounds__(FWD_THREADS, CTAS) forward_kernel(ForwardArgs 
         abort_flag = 0;
         fence_mbar_init();
     }
-    // b1..b4, then w5 and b5 (P_W5, P_B5 follow each other)
+    // b1..b4 halved (the epilogue computes z / 2 = acc / 2 + b / 2 in one FMA), then w5 and b5
+    // (P_W5, P_B5 follow each other)
     for (int i = threadIdx.x; i < FWD_PARAMS; i += FWD_THREADS)
-        prm[i] = i < 4 * WIDTH ? g.params[bias_at(i / WIDTH) + i % WIDTH] : g.params[P_W5 + (i - 4 * WIDTH)];
+        prm[i] = i < 4 * WIDTH ? 0.5f * g.params[bias_at(i / WIDTH) + i % WIDTH] : g.params[P_W5 + (i - 4 * WIDTH)];
     if (warp == 0) tmem_alloc(&tmem_base, 256);
     tc_fence_before();
     __syncthreads();
@@ -668,7 +682,7 @@ __global__ void __launch_bounds__(FWD_THREADS, CTAS) forward_kernel(ForwardArgs 
                 }
                 accs++;
                 tc_fence_after();
-                const float *bias = prm + layer * WIDTH;
+                const float *bias = prm + layer * WIDTH;  // halved biases (the epilogue works on z / 2)
                 // this half's 128 columns in eight pieces of 16, each piece's tensor-memory load
                 // issued before the previous piece is computed (its latency hidden behind the math)
                 uint32_t buf[2][16];
@@ -693,8 +707,8 @@ __global__ void __launch_bounds__(FWD_THREADS, CTAS) forward_kernel(ForwardArgs 
                         uint32_t ph[8];
 #pragma unroll
                         for (int j = 0; j < 16; j += 2)
-                            ph[j / 2] = pack_bf16(silu(__uint_as_float(cur[j]) + bb[j]),
-                                                  silu(__uint_as_float(cur[j + 1]) + bb[j + 1]));
+                            ph[j / 2] = pack_bf16_alu(silu_of_half(fmaf(__uint_as_float(cur[j]), 0.5f, bb[j])),
+                                                      silu_of_half(fmaf(__uint_as_float(cur[j + 1]), 0.5f, bb[j + 1])));
 #pragma unroll
                         for (int q = 0; q < 2; q++)
                             *reinterpret_cast<uint4 *>(act + (col / 64) * TILE_A + sw128_offset(r, col % 64 + 8 * q)) =
@@ -702,7 +716,8 @@ __global__ void __launch_bounds__(FWD_THREADS, CTAS) forward_kernel(ForwardArgs 
                     } else {
                         const float *w5 = prm + 4 * WIDTH + col;
 #pragma unroll
-                        for (int j = 0; j < 16; j++) out += bf16_round(silu(__uint_as_float(cur[j]) + bb[j])) * w5[j];
+                        for (int j = 0; j < 16; j++)
+                            out = fmaf(bf16_round_alu(silu_of_half(fmaf(__uint_as_float(cur[j]), 0.5f, bb[j]))), w5[j], out);
                     }
                 }
                 if (layer < 3) {
