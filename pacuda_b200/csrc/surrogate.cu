@@ -73,18 +73,6 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
     return *reinterpret_cast<uint32_t *>(&v);
 }
 __device__ __forceinline__ float bf16_round(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
-// two FP32 values rounded to BF16 (nearest, ties to even) and packed, by integer arithmetic on the
-// ALU pipe (finite inputs): the same bits as pack_bf16
-__device__ __forceinline__ uint32_t pack_bf16_alu(float lo, float hi) {
-    const uint32_t a = __float_as_uint(lo), b = __float_as_uint(hi);
-    const uint32_t ra = (a + 0x7fffu + ((a >> 16) & 1u)) >> 16, rb = (b + 0x7fffu + ((b >> 16) & 1u)) & 0xffff0000u;
-    return ra | rb;
-}
-__device__ __forceinline__ float bf16_round_alu(float x) {
-    const uint32_t a = __float_as_uint(x);
-    return __uint_as_float((a + 0x7fffu + ((a >> 16) & 1u)) & 0xffff0000u);
-}
-
 // byte offset of element (r, k) in an A image whose row tiles hold `kt` tiles of 64 values of K
 __device__ __forceinline__ size_t a_img(uint32_t r, uint32_t k, uint32_t kt) {
     return ((size_t)(r >> 7) * kt + (k >> 6)) * TILE_A + sw128_offset(r & 127u, k & 63u);
@@ -707,8 +695,8 @@ __global__ void __launch_bounds__(FWD_THREADS, CTAS) forward_kernel(ForwardArgs 
                         uint32_t ph[8];
 #pragma unroll
                         for (int j = 0; j < 16; j += 2)
-                            ph[j / 2] = pack_bf16_alu(silu_of_half(fmaf(__uint_as_float(cur[j]), 0.5f, bb[j])),
-                                                      silu_of_half(fmaf(__uint_as_float(cur[j + 1]), 0.5f, bb[j + 1])));
+                            ph[j / 2] = pack_bf16(silu_of_half(fmaf(__uint_as_float(cur[j]), 0.5f, bb[j])),
+                                                  silu_of_half(fmaf(__uint_as_float(cur[j + 1]), 0.5f, bb[j + 1])));
 #pragma unroll
                         for (int q = 0; q < 2; q++)
                             *reinterpret_cast<uint4 *>(act + (col / 64) * TILE_A + sw128_offset(r, col % 64 + 8 * q)) =
@@ -717,7 +705,7 @@ __global__ void __launch_bounds__(FWD_THREADS, CTAS) forward_kernel(ForwardArgs 
                         const float *w5 = prm + 4 * WIDTH + col;
 #pragma unroll
                         for (int j = 0; j < 16; j++)
-                            out = fmaf(bf16_round_alu(silu_of_half(fmaf(__uint_as_float(cur[j]), 0.5f, bb[j]))), w5[j], out);
+                            out = fmaf(bf16_round(silu_of_half(fmaf(__uint_as_float(cur[j]), 0.5f, bb[j]))), w5[j], out);
                     }
                 }
                 if (layer < 3) {
