@@ -103,14 +103,15 @@ def phase_space(u, sqrt_s):
 
 
 def passes(p, pt_min=20.0, eta_max=5.0, dr_min=0.4):
-    """The cuts on legs 2..4: pT > pt_min, |eta| < eta_max (eta = asinh(pz / pT)), pairwise
-    Delta R > dr_min."""
+    """The cuts on legs 2..4: pT^2 > pt_min^2, |pz| < pT sinh(eta_max) (|eta| < eta_max), pairwise
+    Delta R > dr_min with eta = asinh(pz / pT), phi = atan2(py, px)."""
     fin = p[:, 2:]
-    pt = np.hypot(fin[..., 1], fin[..., 2])
+    pt2 = fin[..., 1] ** 2 + fin[..., 2] ** 2
+    pt = np.sqrt(pt2)
+    ok = (pt2 > pt_min * pt_min).all(axis=1) & (np.abs(fin[..., 3]) < pt * math.sinh(eta_max)).all(axis=1)
     with np.errstate(divide="ignore", invalid="ignore"):
         eta = np.arcsinh(fin[..., 3] / pt)
     phi = np.arctan2(fin[..., 2], fin[..., 1])
-    ok = (pt > pt_min).all(axis=1) & (np.abs(eta) < eta_max).all(axis=1)
     for i in range(3):
         for j in range(i + 1, 3):
             d = np.abs(phi[:, i] - phi[:, j])

@@ -101,16 +101,23 @@ __device__ __forceinline__ double map(const double (&u)[UNIFORMS], double sqrt_s
            (MAP_E2 * (1.0 - c2 * c2));
 }
 
-// pT > pt_min, |eta| < eta_max (eta = asinh(pz / pT)) and pairwise Delta R > dr_min on legs 2..4
+// pT > pt_min, |eta| < eta_max and pairwise Delta R > dr_min on legs 2..4; the first two as
+// pT^2 > pt_min^2 and |pz| < pT sinh(eta_max) (no transcendental function for a point they reject),
+// eta = asinh(pz / pT) and phi = atan2(py, px) only for the Delta R of points that pass them
 __device__ __forceinline__ bool passes(const double (&p)[5][4], const Cuts &c) {
-    double eta[3], phi[3];
+    const double sh = sinh(c.eta_max);
+    double pt[3];
     for (int i = 0; i < 3; i++) {
         const double *q = p[2 + i];
-        const double pt = hypot(q[1], q[2]);
-        if (!(pt > c.pt_min)) return false;
-        eta[i] = asinh(q[3] / pt);
-        if (!(fabs(eta[i]) < c.eta_max)) return false;
-        phi[i] = atan2(q[2], q[1]);
+        const double pt2 = q[1] * q[1] + q[2] * q[2];
+        if (!(pt2 > c.pt_min * c.pt_min)) return false;
+        pt[i] = sqrt(pt2);
+        if (!(fabs(q[3]) < pt[i] * sh)) return false;
+    }
+    double eta[3], phi[3];
+    for (int i = 0; i < 3; i++) {
+        eta[i] = asinh(p[2 + i][3] / pt[i]);
+        phi[i] = atan2(p[2 + i][2], p[2 + i][1]);
     }
     const double pi = 3.141592653589793;
     for (int i = 0; i < 3; i++)
