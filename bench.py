@@ -1,4 +1,5 @@
-"""Benchmark: matrix-element points/s of p p -> 3 jets (leading colour, f64) on B200.
+"""Benchmark: matrix-element points/s of p p -> 3 jets (leading colour, f64) on B200, and the
+learned part's unweighted events/s against plain unweighting.
 
 Workload (one step): 2^20 seeded RAMBO points at sqrt(s) = 13 TeV with jet cuts (pT > 20 GeV,
 |eta| < 5, Delta R > 0.4), split over the subprocess families gg>ggg, qg>qgg, qq~>ggg and
@@ -12,12 +13,23 @@ colour orderings summed, in f64 (bit for bit the reference runner's f64 arithmet
   (pacuda_b200/umami), one call per step over all events from pinned host momenta to |M|^2 in
   host memory, the copies in the timed region; e2e_abi: the runner's own C ABI
   (pacman_recurrence_v1_run + _reduce_resolved per tile of 2^16 points) the same way;
+* reference_gpu: the reference's own runner (recurrence_runner.cu built from its sources for
+  sm_100a, unmodified) through its C ABI on the same points, per kernel kind (f64, df64, mixed),
+  each in its own process; vs_reference_gpu: this library's rates over its f64 rate;
+* parity: the timed outputs of the first 2048 points of every family bit for bit against the
+  oracle and the reference runner's f64 outputs (the 6-leg lines check 256 points per plan);
 * roofline: the dominant kernel's algorithmic flops (fixed per-op counts) per launch over its
-  CUDA-event time, against this GPU's f64 FMA throughput measured in the same run;
+  CUDA-event time, against this GPU's f64 FMA throughput measured in the same run; the
+  algorithmic bytes (momenta in, outputs out) beside the DRAM traffic of an ncu capture;
 * cpu_baseline: the CPU oracle (the runner's arithmetic restated in C++, OpenMP over all cores)
   on a bounded sample of the same families;
-* precision, precision_gg4g (with the stability check), pp4j: the other kinds and the 6-leg
-  configurations (--no-precision skips them).
+* precision (f64fma, mixed, mixed64, df64), precision_gg4g (with the stability check), pp4j:
+  the other kinds and the 6-leg configurations (--no-precision skips them);
+* surrogate: a network of log w (w = |M|^2 J) trained by this library's tensor-core kernels on
+  2^22 points labelled by the f64 runner, then two-stage unweighting (network first, f64 runner
+  second) against plain unweighting (f64 runner on every candidate) of the same 2^22 candidates:
+  events/s of each, their ratio, efficiencies, the events' agreement with the exact weighted
+  distribution (--no-surrogate skips it).
 --impl reference prints the reference arm's line: the CPU oracle on the same sample per step.
 
 usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]

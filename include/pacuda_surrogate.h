@@ -58,6 +58,11 @@ int pacuda_sg_gradients(pacuda_sg_net *net, const float *x, const float *y, uint
 int pacuda_sg_train_step(pacuda_sg_net *net, const float *x, const float *y, uint32_t batch, float lr, float *loss_sum,
                          void *stream);
 
+/* One Adam step (as pacuda_sg_train_step takes it) on a gradient the caller supplies (device,
+ * param order): data-parallel training averages pacuda_sg_gradients over the ranks' shards (one
+ * all-reduce of pacuda_sg_param_count floats) and applies the mean on every rank. */
+int pacuda_sg_apply_gradients(pacuda_sg_net *net, const float *grad, float lr, void *stream);
+
 /* out[i] for `count` points of x (device FP32 [count][inputs]) with the fused inference kernel
  * (all layers of a tile of 128 points in one block, weights streamed through shared memory). */
 int pacuda_sg_forward(const pacuda_sg_net *net, const float *x, uint32_t count, float *out, void *stream);

@@ -1048,19 +1048,34 @@ extern "C" int pacuda_sg_gradients(pacuda_sg_net *n, const float *x, const float
     return gradients(n, x, y, batch, grad, loss, nullptr, (cudaStream_t)stream);
 }
 
+namespace {
+
+// one Adam step on the gradient `grad` (param order, device) and the weight images
+int adam_step(pacuda_sg_net *n, const float *grad, float lr, cudaStream_t s) {
+    n->step++;
+    const float c1 = (float)(1.0 / (1.0 - std::pow(0.9, (double)n->step)));
+    const float c2 = (float)(1.0 / (1.0 - std::pow(0.999, (double)n->step)));
+    adam_kernel<<<(unsigned)((P_COUNT + 255) / 256), 256, 0, s>>>(n->params, n->m1, n->m2, grad, lr, c1, c2, n->inputs);
+    g_last_launches++;
+    if (failed(cudaGetLastError(), "adam")) return ST_DEVICE;
+    return refresh_images(n, s);
+}
+
+}  // namespace
+
+extern "C" int pacuda_sg_apply_gradients(pacuda_sg_net *n, const float *grad, float lr, void *stream) {
+    g_last_launches = 0;
+    if (!n || !grad) return ST_INVALID;
+    return adam_step(n, grad, lr, (cudaStream_t)stream);
+}
+
 extern "C" int pacuda_sg_train_step(pacuda_sg_net *n, const float *x, const float *y, uint32_t batch, float lr,
                                     float *loss_sum, void *stream) {
     g_last_launches = 0;
     cudaStream_t s = (cudaStream_t)stream;
     int st = gradients(n, x, y, batch, n ? n->grad : nullptr, nullptr, loss_sum, s);
     if (st != ST_OK) return st;
-    n->step++;
-    const float c1 = (float)(1.0 / (1.0 - std::pow(0.9, (double)n->step)));
-    const float c2 = (float)(1.0 / (1.0 - std::pow(0.999, (double)n->step)));
-    adam_kernel<<<(unsigned)((P_COUNT + 255) / 256), 256, 0, s>>>(n->params, n->m1, n->m2, n->grad, lr, c1, c2, n->inputs);
-    g_last_launches++;
-    if (failed(cudaGetLastError(), "adam")) return ST_DEVICE;
-    return refresh_images(n, s);
+    return adam_step(n, n->grad, lr, s);
 }
 
 extern "C" int pacuda_sg_forward(const pacuda_sg_net *n, const float *x, uint32_t count, float *out, void *stream) {

@@ -38,6 +38,7 @@ def lib():
         L.pacuda_sg_last_launches.restype = C.c_uint32
         L.pacuda_sg_error.argtypes = [C.c_void_p]
         L.pacuda_sg_set_inference_blocks.argtypes = [C.c_uint32]
+        L.pacuda_sg_apply_gradients.argtypes = [C.c_void_p, C.c_void_p, C.c_float, C.c_void_p]
         _lib = L
     return _lib
 
@@ -95,6 +96,11 @@ class Network:
         _check(lib().pacuda_sg_train_step(self.handle, x.data_ptr(), y.data_ptr(), x.shape[0], float(lr),
                                           loss_sum.data_ptr() if loss_sum is not None else None, _stream(stream)),
                "train_step")
+
+    def apply_gradients(self, grad, lr, stream=None):
+        """One Adam step on a supplied gradient (a float32 CUDA tensor in parameter order)."""
+        _check(lib().pacuda_sg_apply_gradients(self.handle, grad.data_ptr(), float(lr), _stream(stream)),
+               "apply_gradients")
 
     def forward(self, x, out=None, stream=None):
         import torch

@@ -302,6 +302,37 @@ def train(net, x, y, epochs, batch=16384, lr=2e-3, lr_end=2e-5, seed=0, importan
     return history
 
 
+def train_data_parallel(net, x, y, dist, epochs, batch=16384, lr=2e-3, lr_end=2e-5, seed=0):
+    """Data-parallel training over the ranks of `dist` (torch.distributed): each rank holds its own
+    shard (x, y) of the labelled points (equal sizes), computes the gradient of its batch of `batch`
+    points, the ranks average the gradients (one all-reduce of the parameter vector per step) and
+    every rank applies the same Adam step, so their networks stay identical. Returns the mean loss
+    of each epoch over all ranks."""
+    import torch
+
+    world = dist.get_world_size()
+    n = (x.shape[0] // batch) * batch
+    steps = epochs * (n // batch)
+    gen = torch.Generator(device=x.device)
+    gen.manual_seed(seed)
+    history, step = [], 0
+    for _ in range(epochs):
+        perm = torch.randperm(x.shape[0], device=x.device, generator=gen)[:n]
+        xs, ys = x[perm].contiguous(), y[perm].contiguous()
+        total = torch.zeros(1, dtype=torch.float64, device=x.device)
+        for b in range(n // batch):
+            rate = lr * (lr_end / lr) ** (step / max(1, steps - 1))
+            grad, loss = net.gradients(xs[b * batch:(b + 1) * batch], ys[b * batch:(b + 1) * batch])
+            dist.all_reduce(grad)
+            grad /= world
+            net.apply_gradients(grad, rate)
+            total += loss.double()
+            step += 1
+        dist.all_reduce(total)
+        history.append(float(total.item()) / (n * world))
+    return history
+
+
 def maxima(values, weights=None, overweight=1e-3):
     """A reduced maximum for unweighting: the smallest threshold t such that the part of the
     total above it, sum(weights * max(0, values - t)), is at most `overweight` of
