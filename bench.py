@@ -386,9 +386,12 @@ def surrogate_line(torch, train_points=1 << 22, candidates=1 << 22, epochs=300, 
     e1.record()
     e1.synchronize()
     ms = e0.elapsed_time(e1) / steps
+    peak, source = bf16_peak()
+    tf = cand.numel() * flops / (ms * 1e-3) / 1e12
     res["stage1_kernel"] = {"candidates_inside_cuts": int(cand.numel()), "ms": ms,
                             "candidates_per_s": cand.numel() / (ms * 1e-3), "flops_per_candidate": flops,
-                            "tflops": cand.numel() * flops / (ms * 1e-3) / 1e12}
+                            "tflops": tf, "roofline": {"bound": "tensor", "achieved": tf, "peak": peak,
+                                                       "unit": "TFLOP/s", "frac": tf / peak, "peak_source": source}}
     return res
 
 
@@ -603,6 +606,15 @@ def hbm_peak():
         return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]
     except (OSError, ValueError, KeyError):
         return 6650.0
+
+
+def bf16_peak():
+    """(dense BF16 TFLOP/s of this pool's B200s, its source): the burst figure of
+    MEASURED_PEAKS.json, else the earlier measurement on this pool (1590)."""
+    try:
+        return float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["bf16_tflops"]), "MEASURED_PEAKS.json"
+    except (OSError, ValueError, KeyError):
+        return 1590.0, "fallback (no MEASURED_PEAKS.json)"
 
 
 def cpu_baseline(fams, sample=2048, keep=None):
@@ -842,6 +854,8 @@ def main():
     ap.add_argument("--no-precision", action="store_true", help="skip the mixed-precision lines")
     ap.add_argument("--blocks-per-sm", type=int, default=0, help="1, 2, 3, 4, 5, 8 or 16 (with --no-tune or --lanes-per-point)")
     ap.add_argument("--no-reference-gpu", action="store_true", help="skip timing the reference's own GPU runner")
+    ap.add_argument("--no-graph", action="store_true", help="plain launches instead of a CUDA-graph replay "
+                                                             "(profiling cases: ncu does not replay the graph)")
     ap.add_argument("--no-surrogate", action="store_true", help="skip the surrogate and two-stage unweighting line")
     ap.add_argument("--surrogate-only", action="store_true", help="only the surrogate line (development runs)")
     ap.add_argument("--surrogate-args", default="", help="key=value,... for the surrogate line (development runs)")
@@ -926,8 +940,9 @@ def main():
     if args.blocks_per_sm:
         batch.blocks_per_sm = args.blocks_per_sm
     stream = torch.cuda.Stream()
-    with torch.cuda.stream(stream):
-        batch.capture(stream)
+    if not args.no_graph:
+        with torch.cuda.stream(stream):
+            batch.capture(stream)
     for _ in range(args.warmup):
         batch.run(stream)
     clocks = Clocks(int(os.environ.get("LOCAL_RANK", 0))) if rank == 0 else None
