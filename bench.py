@@ -432,8 +432,25 @@ def surrogate_kernels(torch, count=1 << 21, steps=5):
         res[what] = {"points": count, "ms": ms, "points_per_s": count / (ms * 1e-3),
                      "tflops": count * flops / (ms * 1e-3) / 1e12, "blocks_per_sm": blocks}
     S.set_inference_blocks(2)
-    if net.error():
-        raise RuntimeError(f"surrogate kernels reported error {net.error()}")
+    # training steps (forward, backward and weight-gradient products, gradient reduction, Adam):
+    # three products per layer per point, 3 x the inference flops
+    batch = 16384
+    tnet = S.Network(9, max_batch=batch, seed=5)
+    tx = torch.rand(batch, 9, device="cuda")
+    ty = torch.randn(batch, device="cuda")
+    for _ in range(3):
+        tnet.train_step(tx, ty, 1e-4)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(4 * steps):
+        tnet.train_step(tx, ty, 1e-4)
+    e1.record()
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / (4 * steps)
+    res["train_step"] = {"batch": batch, "ms": ms, "launches": S.last_launches(),
+                         "tflops": 3 * batch * flops / (ms * 1e-3) / 1e12}
+    if net.error() or tnet.error():
+        raise RuntimeError(f"surrogate kernels reported error {net.error() or tnet.error()}")
     return res
 
 
