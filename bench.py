@@ -1004,6 +1004,7 @@ def main():
                                        "reference's arithmetic has no FMA, so half of it is the ceiling",
                         "frac_of_no_fma_ceiling": achieved / (peak / 2),
                         "traffic_source": "dram read+write bytes per point from one ncu capture of the same mix "
+                                          "at its full 2^20 points in one launch "
                                           "(profiles/launches_pp3j_bench.md), times this launch's points",
                         "hbm": {"achieved_gbs": traffic / (ms * 1e-3) / 1e9 if traffic else None,
                                 "algorithmic_bytes": alg_bytes,
