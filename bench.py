@@ -223,10 +223,11 @@ def precision_line(torch, B, fams, ext, ref_out, steps, warmup, kind="mixed"):
             "blocks_per_sm": {nm: batch.plan_blocks_per_sm(k) for k, (nm, _, _) in enumerate(fams)}}
 
 
-def surrogate_line(torch, train_points=1 << 22, candidates=1 << 22, epochs=300, batch=16384, steps=3, alpha=0.5,
-                   lr=2e-3, overweight=None):
-    """The learned part: a surrogate of the weight w = |M|^2 J of p p -> 3 jets candidates (one
-    network, the five unit-cube numbers and a subprocess one-hot as inputs, 4 x 256 SiLU, BF16
+def surrogate_line(torch, families=None, train_points=1 << 22, candidates=1 << 22, epochs=300, batch=16384, steps=3,
+                   alpha=0.5, lr=2e-3, overweight=None):
+    """The learned part: a surrogate of the weight w = |M|^2 J of p p -> 3 jets candidates (or of
+    the p p -> 4 jets families with families=processes.PP4J: eight unit-cube numbers; one
+    network, the unit-cube numbers and a subprocess one-hot as inputs, 4 x 256 SiLU, BF16
     tensor-core products, trained on the standardized log w), trained by this library's kernels
     on `train_points` points inside the cuts labelled by the f64 recurrence (a training stream of
     candidates), then two-stage unweighting of `candidates` seeded candidates (split over the
@@ -239,14 +240,16 @@ def surrogate_line(torch, train_points=1 << 22, candidates=1 << 22, epochs=300, 
     from pacuda_b200 import surrogate as S
     from pacuda_b200 import unweight as UW
 
-    fams = list(FAMILIES)
+    fams = list(families or FAMILIES)
+    final_state = UW.final_state_of(fams[0])
     counts = split_points(candidates, SEED)
-    # a training stream of 4 x train_points candidates: about 28 % pass the cuts
-    train_counts = split_points(4 * train_points, SEED + 1)
-    pl = UW.Pipeline(families=fams, capacity=int(0.4 * max(max(counts), max(train_counts))) + 4096)
-    res = {"workload": f"pp>3j LC: {', '.join(fams)}; 13 TeV, pT>20 GeV, |eta|<5, dR>0.4; network 4 x 256 SiLU, "
-                       f"inputs 5 + {len(fams)} one-hot; {train_points} labelled points, {candidates} candidates "
-                       f"unweighted", "candidates_per_family": dict(zip(fams, counts))}
+    # a training stream of candidates: about 28 % of 2 -> 3 candidates pass the cuts, 5.6 % of 2 -> 4
+    stream, share = (4, 0.4) if final_state == 3 else (24, 0.1)
+    train_counts = split_points(stream * train_points, SEED + 1)
+    pl = UW.Pipeline(families=fams, capacity=int(share * max(max(counts), max(train_counts))) + 4096)
+    res = {"workload": f"pp>{final_state}j LC: {', '.join(fams)}; 13 TeV, pT>20 GeV, |eta|<5, dR>0.4; network "
+                       f"4 x 256 SiLU, inputs {pl.numbers} + {len(fams)} one-hot; {train_points} labelled points, "
+                       f"{candidates} candidates unweighted", "candidates_per_family": dict(zip(fams, counts))}
     # labels: the f64 recurrence on the candidates of a training stream (from 2^40 on) inside the cuts
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
@@ -358,8 +361,8 @@ def surrogate_line(torch, train_points=1 << 22, candidates=1 << 22, epochs=300, 
                                                "events": int(len(wts))}
 
         def moms(index):
-            u = UO.uniforms(seed, index.cpu().numpy().astype(np.uint64))
-            return UO.phase_space(u, ECM)[0]
+            u = UO.uniforms(seed, index.cpu().numpy().astype(np.uint64), final_state)
+            return UO.momenta(u, ECM, final_state)[0]
 
         ref = UW.observables(moms(idx_all))
         for kind in ("plain", "two_stage"):
@@ -380,9 +383,10 @@ def surrogate_line(torch, train_points=1 << 22, candidates=1 << 22, epochs=300, 
     e0.record()
     for _ in range(steps):
         pl.counters.zero_()
-        UW._check(UW._lib().pacuda_uw_stage1(net.handle, pl.family_seed(k0), UW._ptr(cand), cand.numel(), k0, mu,
-                                             sigma, s_max, UW._ptr(f0.kept), UW._ptr(f0.kept_s), pl.capacity,
-                                             UW._ptr(pl.counters), UW._stream()), "stage 1")
+        UW._check(UW._lib().pacuda_uw_stage1(net.handle, pl.family_seed(k0), UW._ptr(cand), cand.numel(),
+                                             pl.final_state, k0, mu, sigma, s_max, UW._ptr(f0.kept),
+                                             UW._ptr(f0.kept_s), pl.capacity, UW._ptr(pl.counters), UW._stream()),
+                  "stage 1")
     e1.record()
     e1.synchronize()
     ms = e0.elapsed_time(e1) / steps
@@ -417,7 +421,7 @@ def surrogate_kernels(torch, count=1 << 21, steps=5):
                 net.forward(x, out)
             else:
                 pl.counters.zero_()
-                UW._check(UW._lib().pacuda_uw_stage1(net.handle, 11, UW._ptr(cand), count, 0, -3.0, 1.0, 1e30,
+                UW._check(UW._lib().pacuda_uw_stage1(net.handle, 11, UW._ptr(cand), count, 3, 0, -3.0, 1.0, 1e30,
                                                      UW._ptr(pl.fams[0].kept), UW._ptr(pl.fams[0].kept_s),
                                                      pl.capacity, UW._ptr(pl.counters), UW._stream()), "stage 1")
         for _ in range(2):
@@ -596,12 +600,27 @@ def pp4j_line(torch, B, points=1 << 22, steps=3, warmup=2, check=256):
             per_family[name] = per_family[name] + x if name in per_family else x
         totals[kind] = torch.cat([per_family[nm] for nm in names])
         if kind == "f64":
-            res["parity"] = oracle_parity([(f"{name} plan {k}", t, moms[name][:check], o.view(n, t.outputs)[:check])
-                                           for k, ((name, t, n, _), o) in enumerate(zip(fams, outs))])
+            # the oracle on the first `check` points of every plan: the parity check, and timed, the
+            # CPU recurrence's rate (each family's plans on its sample, weighted by its share)
+            from oracle import oracle as O
+
+            pairs, secs = [], {}
+            for k, ((name, t, n, _), o) in enumerate(zip(fams, outs)):
+                t0 = time.perf_counter()
+                _, want = O.evaluate(t, moms[name][:check], kernel=1)
+                secs[name] = secs.get(name, 0.0) + time.perf_counter() - t0
+                pairs.append((f"{name} plan {k}", o.view(n, t.outputs)[:check].cpu().numpy(), want))
+            res["parity"] = parity(pairs)
+            total_s = sum(secs[nm] * int(c) / min(check, int(c)) for nm, c in zip(names, counts))
+            res["cpu_baseline"] = {"value": points / total_s, "unit": "points/s", "cores": os.cpu_count(),
+                                   "kind": "port",
+                                   "sample": f"first {check} points of each family through all its plans, OpenMP "
+                                             f"over all host cores, rates weighted by the families' shares"}
         del batch, outs
     rel = ((totals["mixed"] - totals["f64"]).abs() / totals["f64"].abs().clamp_min(1e-300)).cpu().numpy()
     res["mixed"]["rel_error_vs_f64"] = {"median": float(np.median(rel)), "q999": float(np.quantile(rel, 0.999)),
                                         "max": float(rel.max())}
+    res["f64_vs_cpu"] = res["f64"]["value"] / res["cpu_baseline"]["value"]
     return res
 
 
@@ -929,6 +948,11 @@ def main():
         kw = {}
         for item in args.surrogate_args.split(",") if args.surrogate_args else []:
             key, val = item.split("=")
+            if key == "families":
+                from pacuda_b200 import processes
+
+                kw[key] = processes.PP4J if val == "pp4j" else processes.PP3J
+                continue
             kw[key] = float(val) if "." in val or "e" in val else int(val)
         print(json.dumps({"surrogate": surrogate_line(torch, **kw)}))
         return
@@ -1069,7 +1093,12 @@ def main():
             res["precision_gg4g"] = six_gluon_line(torch, B)
             res["pp4j"] = pp4j_line(torch, B)
         if not args.no_surrogate:
+            from pacuda_b200 import processes
+
             res["surrogate"] = surrogate_line(torch)
+            if not args.no_precision:
+                # p p -> 4 jets: the combined configuration's learned part
+                res["surrogate_pp4j"] = surrogate_line(torch, families=processes.PP4J)
     if world > 1:
         import torch.distributed as dist
 

@@ -1,11 +1,13 @@
-// Candidates of the unweighting: counter-based uniforms, the five-number phase-space map of
-// massless 2 -> 3 at fixed sqrt(s) and the jet cuts, in f64 on the device.
+// Candidates of the unweighting: counter-based uniforms, the phase-space maps of massless 2 -> 3
+// (five numbers) and 2 -> 4 (eight numbers) at fixed sqrt(s) and the jet cuts, in f64 on the
+// device.
 //
 // Candidate i of a stream with seed S: a xorshift64 stream (shifts 13, 7, 17; uniform =
-// ((state >> 11) + 0.5) / 2^53) started at splitmix64(S ^ (i * 0xD1B54A32D192ED03)) | 1. Uniforms
-// 0-4 are the phase-space numbers, 5 the first accept/reject number, 6 the second.
+// ((state >> 11) + 0.5) / 2^53) started at splitmix64(S ^ (i * 0xD1B54A32D192ED03)) | 1. For N
+// final-state partons, uniforms 0 .. 3N - 5 are the phase-space numbers, 3N - 4 the first
+// accept/reject number and 3N - 3 the second.
 //
-// The map (sequential two-body decays, each variable importance-sampled where |M|^2 peaks):
+// The 2 -> 3 map (sequential two-body decays, each variable importance-sampled where |M|^2 peaks):
 //   s23 = s sigma(y), y = L (2 x1 - 1), sigma(y) = 1 / (1 + e^-y): logarithmic towards both the
 //     collinear 2 || 3 end (small s23) and the soft-p1 end (s23 near s);
 //   p1 in the centre-of-mass frame with |p1| = (s - s23) / (2 sqrt(s)), cos(theta1) =
@@ -18,13 +20,32 @@
 // reaches m23 down to 4.4 GeV at 13 TeV (the cuts need at least 8 GeV); E1 = 5.5 covers every p1
 // inside |eta| < 5; E2 = 7 leaves out a q-frame solid angle of 1.7e-6 around the z axis.
 // Legs: 0, 1 the beams (sqrt(s)/2)(1, 0, 0, +-1), 2 = p1, 3 = p2, 4 = p3.
+//
+// The 2 -> 4 map adds one decay: P -> p1 + Q, Q -> p2 + R, R -> p3 + p4 with
+//   s_Q = s sigma(L (2 x1 - 1)), s_R = s_Q sigma(L (2 x4 - 1));
+//   p1 as above (x2, x3), |p1| = (s - s_Q) / (2 sqrt(s));
+//   p2 in the rest frame of Q, |p2| = (s_Q - s_R) / (2 sqrt(s_Q)), cos(theta2) = tanh(E2 (2 x5 - 1)),
+//     phi2 = 2 pi x6, R opposite;
+//   p3, p4 back to back in the rest frame of R, |p| = sqrt(s_R) / 2, cos(theta3) = tanh(E2 (2 x7 - 1)),
+//     phi3 = 2 pi x8; boosted to Q's frame along R, then with p2 to the lab along Q;
+// from dPhi_4 = dPhi_2(P; p1, Q) ds_Q / 2 pi dPhi_2(Q; p2, R) ds_R / 2 pi dPhi_2(R; p3, p4) and
+// dPhi_2(K; k1 massless, k2 of mass^2 m) = (K^2 - m) / (32 pi^2 K^2) dOmega:
+//   J = s s_Q (1 - sigma1) (1 - sigma2) / (2048 pi^5) x 2 L sigma1 (1 - sigma1) x 2 L sigma2 (1 - sigma2)
+//       x E1 (1 - c1^2) x E2 (1 - c2^2) x E2 (1 - c3^2)
+// (flat variables integrate it to the massless four-body volume s^2 / (24576 pi^5)).
+// Legs: 0, 1 the beams, 2 = p1, 3 = p2, 4 = p3, 5 = p4.
 #pragma once
 #include <stdint.h>
 
 namespace pacuda {
 namespace phase {
 
-constexpr int UNIFORMS = 7;
+// N final-state partons: 3N - 2 uniforms, 3N - 4 of them phase-space numbers, N + 2 legs
+template <int N> struct Space {
+    static constexpr int UNIFORMS = 3 * N - 2, NUMBERS = 3 * N - 4, LEGS = N + 2;
+};
+constexpr int UNIFORMS = Space<3>::UNIFORMS;
+constexpr int MAX_UNIFORMS = Space<4>::UNIFORMS;
 
 struct Cuts {
     double pt_min, eta_max, dr_min;
@@ -37,10 +58,10 @@ __device__ __forceinline__ uint64_t splitmix64(uint64_t x) {
     return z ^ (z >> 31);
 }
 
-__device__ __forceinline__ void uniforms(uint64_t seed, uint64_t index, double (&u)[UNIFORMS]) {
+template <int U> __device__ __forceinline__ void uniforms(uint64_t seed, uint64_t index, double (&u)[U]) {
     uint64_t state = splitmix64(seed ^ (index * 0xD1B54A32D192ED03ull)) | 1ull;
 #pragma unroll
-    for (int k = 0; k < UNIFORMS; k++) {
+    for (int k = 0; k < U; k++) {
         state ^= state << 13;
         state ^= state >> 7;
         state ^= state << 17;
@@ -63,7 +84,7 @@ __device__ __forceinline__ void boost(const double (&p)[4], const double (&b)[3]
 
 constexpr double MAP_L = 16.0, MAP_E1 = 5.5, MAP_E2 = 7.0;
 
-// the map's weight J from uniforms u[0..4] alone (no momenta)
+// the 2 -> 3 map's weight J from uniforms u[0..4] alone (no momenta)
 __device__ __forceinline__ double weight(const double (&u)[UNIFORMS], double sqrt_s) {
     const double s = sqrt_s * sqrt_s, pi = 3.141592653589793;
     const double sg = 1.0 / (1.0 + exp(-MAP_L * (2.0 * u[0] - 1.0)));
@@ -101,27 +122,92 @@ __device__ __forceinline__ double map(const double (&u)[UNIFORMS], double sqrt_s
            (MAP_E2 * (1.0 - c2 * c2));
 }
 
-// pT > pt_min, |eta| < eta_max and pairwise Delta R > dr_min on legs 2..4; the first two as
+// the 2 -> 4 map: the six legs' momenta [leg][E, px, py, pz] and the weight J of uniforms u[0..7]
+__device__ __forceinline__ double map4(const double (&u)[Space<4>::UNIFORMS], double sqrt_s, double (&p)[6][4]) {
+    const double s = sqrt_s * sqrt_s, pi = 3.141592653589793;
+    const double sg1 = 1.0 / (1.0 + exp(-MAP_L * (2.0 * u[0] - 1.0)));
+    const double sq = s * sg1;
+    const double sg2 = 1.0 / (1.0 + exp(-MAP_L * (2.0 * u[3] - 1.0)));
+    const double sr = sq * sg2;
+    // p1 in the centre-of-mass frame
+    const double e1 = (s - sq) / (2.0 * sqrt_s);
+    const double c1 = tanh(MAP_E1 * (2.0 * u[1] - 1.0)), st1 = sqrt(fmax(0.0, 1.0 - c1 * c1)), f1 = 2.0 * pi * u[2];
+    double sf1, cf1;
+    sincos(f1, &sf1, &cf1);
+    p[0][0] = 0.5 * sqrt_s; p[0][1] = 0.0; p[0][2] = 0.0; p[0][3] = 0.5 * sqrt_s;
+    p[1][0] = 0.5 * sqrt_s; p[1][1] = 0.0; p[1][2] = 0.0; p[1][3] = -0.5 * sqrt_s;
+    p[2][0] = e1; p[2][1] = e1 * st1 * cf1; p[2][2] = e1 * st1 * sf1; p[2][3] = e1 * c1;
+    // p2 and R in the rest frame of Q
+    const double mq = sqrt(sq);
+    const double k2 = (sq - sr) / (2.0 * mq);
+    const double c2 = tanh(MAP_E2 * (2.0 * u[4] - 1.0)), st2 = sqrt(fmax(0.0, 1.0 - c2 * c2)), f2 = 2.0 * pi * u[5];
+    double sf2, cf2;
+    sincos(f2, &sf2, &cf2);
+    const double q2[4] = {k2, k2 * st2 * cf2, k2 * st2 * sf2, k2 * c2};
+    const double er = (sq + sr) / (2.0 * mq);
+    // p3 and p4 back to back in the rest frame of R, then into Q's frame along R (velocity -q2 / er)
+    const double k3 = 0.5 * sqrt(sr);
+    const double c3 = tanh(MAP_E2 * (2.0 * u[6] - 1.0)), st3 = sqrt(fmax(0.0, 1.0 - c3 * c3)), f3 = 2.0 * pi * u[7];
+    double sf3, cf3;
+    sincos(f3, &sf3, &cf3);
+    const double r3[4] = {k3, k3 * st3 * cf3, k3 * st3 * sf3, k3 * c3};
+    const double r4[4] = {k3, -r3[1], -r3[2], -r3[3]};
+    const double br[3] = {-q2[1] / er, -q2[2] / er, -q2[3] / er};
+    double q3[4], q4[4];
+    boost(r3, br, q3);
+    boost(r4, br, q4);
+    // everything in Q's frame to the lab along Q (velocity -p1 / (sqrt(s) - e1))
+    const double eq = sqrt_s - e1;
+    const double bq[3] = {-p[2][1] / eq, -p[2][2] / eq, -p[2][3] / eq};
+    double o[4];
+    boost(q2, bq, o);
+    for (int c = 0; c < 4; c++) p[3][c] = o[c];
+    boost(q3, bq, o);
+    for (int c = 0; c < 4; c++) p[4][c] = o[c];
+    boost(q4, bq, o);
+    for (int c = 0; c < 4; c++) p[5][c] = o[c];
+    return s * sq * (1.0 - sg1) * (1.0 - sg2) / (2048.0 * pi * pi * pi * pi * pi) * (2.0 * MAP_L * sg1 * (1.0 - sg1)) *
+           (2.0 * MAP_L * sg2 * (1.0 - sg2)) * (MAP_E1 * (1.0 - c1 * c1)) * (MAP_E2 * (1.0 - c2 * c2)) *
+           (MAP_E2 * (1.0 - c3 * c3));
+}
+
+// the map of N final-state partons (3 or 4)
+template <int N> struct Map;
+template <> struct Map<3> {
+    __device__ __forceinline__ static double momenta(const double (&u)[Space<3>::UNIFORMS], double sqrt_s,
+                                                     double (&p)[5][4]) {
+        return map(u, sqrt_s, p);
+    }
+};
+template <> struct Map<4> {
+    __device__ __forceinline__ static double momenta(const double (&u)[Space<4>::UNIFORMS], double sqrt_s,
+                                                     double (&p)[6][4]) {
+        return map4(u, sqrt_s, p);
+    }
+};
+
+// pT > pt_min, |eta| < eta_max and pairwise Delta R > dr_min on legs 2 .. L - 1; the first two as
 // pT^2 > pt_min^2 and |pz| < pT sinh(eta_max) (no transcendental function for a point they reject),
 // eta = asinh(pz / pT) and phi = atan2(py, px) only for the Delta R of points that pass them
-__device__ __forceinline__ bool passes(const double (&p)[5][4], const Cuts &c) {
+template <int L> __device__ __forceinline__ bool passes(const double (&p)[L][4], const Cuts &c) {
+    constexpr int F = L - 2;
     const double sh = sinh(c.eta_max);
-    double pt[3];
-    for (int i = 0; i < 3; i++) {
+    double pt[F];
+    for (int i = 0; i < F; i++) {
         const double *q = p[2 + i];
         const double pt2 = q[1] * q[1] + q[2] * q[2];
         if (!(pt2 > c.pt_min * c.pt_min)) return false;
         pt[i] = sqrt(pt2);
         if (!(fabs(q[3]) < pt[i] * sh)) return false;
     }
-    double eta[3], phi[3];
-    for (int i = 0; i < 3; i++) {
+    double eta[F], phi[F];
+    for (int i = 0; i < F; i++) {
         eta[i] = asinh(p[2 + i][3] / pt[i]);
         phi[i] = atan2(p[2 + i][2], p[2 + i][1]);
     }
     const double pi = 3.141592653589793;
-    for (int i = 0; i < 3; i++)
-        for (int j = i + 1; j < 3; j++) {
+    for (int i = 0; i < F; i++)
+        for (int j = i + 1; j < F; j++) {
             double d = fabs(phi[i] - phi[j]);
             if (d > pi) d = 2.0 * pi - d;
             const double de = eta[i] - eta[j];

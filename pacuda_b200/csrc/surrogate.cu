@@ -487,8 +487,9 @@ struct ForwardArgs {
     pacuda_uw_segment seg[PACUDA_UW_MAX_SEGMENTS];
     uint32_t tile_first[PACUDA_UW_MAX_SEGMENTS + 1];
     uint32_t segments;
-    double mu, sigma;  // s = exp(mu + sigma out); kept when u5 s_max < s
+    double mu, sigma;  // s = exp(mu + sigma out); kept when (first decision uniform) s_max < s
     uint32_t capacity;
+    uint32_t numbers;  // the candidates' phase-space numbers: 5 (2 -> 3) or 8 (2 -> 4)
 };
 
 // the segment of tile t (segments are few: a linear scan)
@@ -627,16 +628,25 @@ __global__ void __launch_bounds__(FWD_THREADS, CTAS) forward_kernel(ForwardArgs 
                     p[e] = pack_bf16(lo, hi);
                 }
             } else {
-                // the candidate's five numbers and the subprocess one-hot (the listed candidates
+                // the candidate's phase-space numbers and the subprocess one-hot (the listed candidates
                 // are inside the cuts)
-                double u[pacuda::phase::UNIFORMS];
+                constexpr int MAXU = pacuda::phase::MAX_UNIFORMS;
+                double u[MAXU];
+#pragma unroll
+                for (int k = 0; k < MAXU; k++) u[k] = 0.0;
+                const uint32_t nx = g.numbers;
                 if (m < m_count) {
                     cand = g.seg[sg].index[m];
-                    pacuda::phase::uniforms(g.seg[sg].seed, cand, u);
-                } else {
-                    for (int k = 0; k < pacuda::phase::UNIFORMS; k++) u[k] = 0.0;
+                    if (nx == 8) {
+                        pacuda::phase::uniforms(g.seg[sg].seed, cand, u);
+                    } else {
+                        double v[pacuda::phase::Space<3>::UNIFORMS];
+                        pacuda::phase::uniforms(g.seg[sg].seed, cand, v);
+#pragma unroll
+                        for (int k = 0; k < pacuda::phase::Space<3>::UNIFORMS; k++) u[k] = v[k];
+                    }
                 }
-                u_keep = u[5];
+                u_keep = nx == 8 ? u[8] : u[5];
                 const bool real = m < m_count;
                 const uint32_t family = g.seg[sg].family;
                 float f[32];  // this half's 32 features (constant indices only)
@@ -644,11 +654,12 @@ __global__ void __launch_bounds__(FWD_THREADS, CTAS) forward_kernel(ForwardArgs 
                 for (int k = 0; k < 32; k++) f[k] = 0.0f;
                 if (h == 0 && real) {
 #pragma unroll
-                    for (int k = 0; k < 5; k++) f[k] = (float)u[k];
+                    for (int k = 0; k < 8; k++)
+                        if ((uint32_t)k < nx) f[k] = (float)u[k];
                 }
 #pragma unroll
                 for (int k = 0; k < 32; k++)
-                    if (real && 32 * h + k == 5 + family) f[k] = 1.0f;
+                    if (real && 32 * h + k == nx + family) f[k] = 1.0f;
 #pragma unroll
                 for (int e = 0; e < 16; e++) p[e] = pack_bf16(f[2 * e], f[2 * e + 1]);
             }
@@ -1106,17 +1117,20 @@ extern "C" int pacuda_sg_error(const pacuda_sg_net *n) {
 namespace {
 
 using pacuda::phase::Cuts;
+using pacuda::phase::Map;
+using pacuda::phase::Space;
 
-// candidates first .. first + count - 1: the indices of those inside the cuts (unordered,
-// warp-aggregated appends; `count_out` counts all of them, also beyond `capacity`)
+// candidates first .. first + count - 1 of N final-state partons: the indices of those inside the
+// cuts (unordered, warp-aggregated appends; `count_out` counts all of them, also beyond `capacity`)
+template <int N>
 __global__ void candidates_kernel(uint64_t seed, uint64_t first, uint32_t count, double sqrt_s, Cuts cuts,
                                   uint64_t *index, uint32_t capacity, unsigned long long *count_out) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     bool pass = false;
     if (i < count) {
-        double u[pacuda::phase::UNIFORMS], p[5][4];
+        double u[Space<N>::UNIFORMS], p[Space<N>::LEGS][4];
         pacuda::phase::uniforms(seed, first + i, u);
-        pacuda::phase::map(u, sqrt_s, p);
+        Map<N>::momenta(u, sqrt_s, p);
         pass = pacuda::phase::passes(p, cuts);
     }
     const unsigned ballot = __ballot_sync(0xffffffffu, pass);
@@ -1138,6 +1152,7 @@ struct CandidateSegments {
     uint32_t segments;
 };
 
+template <int N>
 __global__ void candidate_segments_kernel(CandidateSegments c, double sqrt_s, Cuts cuts, uint32_t capacity) {
     uint32_t k = 0;
     while (k + 1 < c.segments && blockIdx.x >= c.block_first[k + 1]) k++;
@@ -1145,9 +1160,9 @@ __global__ void candidate_segments_kernel(CandidateSegments c, double sqrt_s, Cu
     const uint32_t i = (blockIdx.x - c.block_first[k]) * blockDim.x + threadIdx.x;
     bool pass = false;
     if (i < sg.count) {
-        double u[pacuda::phase::UNIFORMS], p[5][4];
+        double u[Space<N>::UNIFORMS], p[Space<N>::LEGS][4];
         pacuda::phase::uniforms(sg.seed, sg.first + i, u);
-        pacuda::phase::map(u, sqrt_s, p);
+        Map<N>::momenta(u, sqrt_s, p);
         pass = pacuda::phase::passes(p, cuts);
     }
     const unsigned ballot = __ballot_sync(0xffffffffu, pass);
@@ -1162,44 +1177,50 @@ __global__ void candidate_segments_kernel(CandidateSegments c, double sqrt_s, Cu
 }
 
 // the points of candidates index[0..n): source-major momenta [(leg * 4 + k) * n + i] for the
-// runner, the network's inputs [i][inputs] and the map's weight
+// runner, the network's inputs [i][inputs] (the phase-space numbers, then the family's one-hot)
+// and the map's weight
+template <int N>
 __global__ void points_kernel(uint64_t seed, const uint64_t *index, uint32_t n, double sqrt_s, double *momenta,
                               float *inputs_out, uint32_t inputs, uint32_t family, double *jac) {
+    constexpr int X = Space<N>::NUMBERS, L = Space<N>::LEGS;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    double u[pacuda::phase::UNIFORMS], p[5][4];
+    double u[Space<N>::UNIFORMS], p[L][4];
     pacuda::phase::uniforms(seed, index[i], u);
-    const double j = pacuda::phase::map(u, sqrt_s, p);
+    const double j = Map<N>::momenta(u, sqrt_s, p);
     if (momenta)
-        for (int leg = 0; leg < 5; leg++)
+        for (int leg = 0; leg < L; leg++)
             for (int k = 0; k < 4; k++) momenta[(size_t)(leg * 4 + k) * n + i] = p[leg][k];
     if (inputs_out)
         for (uint32_t f = 0; f < inputs; f++)
-            inputs_out[(size_t)i * inputs + f] = f < 5 ? (float)u[f] : (f == 5 + family ? 1.0f : 0.0f);
+            inputs_out[(size_t)i * inputs + f] = f < (uint32_t)X ? (float)u[f] : (f == X + family ? 1.0f : 0.0f);
     if (jac) jac[i] = j;
 }
 
-// |M|^2 = the sum of the runner's helicity outputs, w = |M|^2 J, and the accept/reject decision:
-// plain (s == null): kept when u5 w_max < w, weight max(1, w / w_max);
-// second stage: r = w / s, kept when u6 r_max < r, weight max(1, s / s_max) max(1, r / r_max)
+// |M|^2 = the sum of the runner's helicity outputs, w = |M|^2 J, and the accept/reject decision
+// (u_a, u_b: the candidate's two decision uniforms, after its phase-space numbers):
+// plain (s == null): kept when u_a w_max < w, weight max(1, w / w_max);
+// second stage: r = w / s, kept when u_b r_max < r, weight max(1, s / s_max) max(1, r / r_max)
+template <int N>
 __global__ void decide_kernel(uint64_t seed, const uint64_t *index, uint32_t n, const double *outputs, uint32_t helicities,
                               const double *jac, const double *s, double w_max, double s_max, double r_max, uint8_t *keep,
                               double *weight, double *me) {
+    constexpr int X = Space<N>::NUMBERS;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double m2 = 0.0;
     for (uint32_t h = 0; h < helicities; h++) m2 += outputs[(size_t)i * helicities + h];
     const double w = m2 * jac[i];
-    double u[pacuda::phase::UNIFORMS];
+    double u[Space<N>::UNIFORMS];
     pacuda::phase::uniforms(seed, index[i], u);
     bool k;
     double wt;
     if (!s) {
-        k = u[5] * w_max < w;
+        k = u[X] * w_max < w;
         wt = k ? fmax(1.0, w / w_max) : 0.0;
     } else {
         const double r = w / s[i];
-        k = u[6] * r_max < r;
+        k = u[X + 1] * r_max < r;
         wt = k ? fmax(1.0, s[i] / s_max) * fmax(1.0, r / r_max) : 0.0;
     }
     if (keep) keep[i] = k;
@@ -1207,24 +1228,32 @@ __global__ void decide_kernel(uint64_t seed, const uint64_t *index, uint32_t n, 
     if (me) me[i] = m2;
 }
 
+bool final_state_valid(uint32_t n) { return n == 3 || n == 4; }
+
 }  // namespace
 
-extern "C" int pacuda_uw_candidates(uint64_t seed, uint64_t first, uint32_t count, double sqrt_s,
+extern "C" int pacuda_uw_candidates(uint64_t seed, uint64_t first, uint32_t count, uint32_t final_state, double sqrt_s,
                                     const pacuda_uw_cuts *cuts, uint64_t *index, uint32_t capacity,
                                     unsigned long long *counter, void *stream) {
     g_last_launches = 0;
-    if (!cuts || !index || !counter || count == 0 || !(sqrt_s > 0)) return ST_INVALID;
+    if (!cuts || !index || !counter || count == 0 || !(sqrt_s > 0) || !final_state_valid(final_state)) return ST_INVALID;
     Cuts c{cuts->pt_min, cuts->eta_max, cuts->dr_min};
-    candidates_kernel<<<(count + 255) / 256, 256, 0, (cudaStream_t)stream>>>(seed, first, count, sqrt_s, c, index,
-                                                                              capacity, counter);
+    const dim3 grid((count + 255) / 256);
+    if (final_state == 4)
+        candidates_kernel<4><<<grid, 256, 0, (cudaStream_t)stream>>>(seed, first, count, sqrt_s, c, index, capacity, counter);
+    else
+        candidates_kernel<3><<<grid, 256, 0, (cudaStream_t)stream>>>(seed, first, count, sqrt_s, c, index, capacity, counter);
     g_last_launches++;
     return failed(cudaGetLastError(), "candidates") ? ST_DEVICE : ST_OK;
 }
 
-extern "C" int pacuda_uw_candidates_segments(const pacuda_uw_candidate_segment *segs, uint32_t segments, double sqrt_s,
-                                             const pacuda_uw_cuts *cuts, uint32_t capacity, void *stream) {
+extern "C" int pacuda_uw_candidates_segments(const pacuda_uw_candidate_segment *segs, uint32_t segments,
+                                             uint32_t final_state, double sqrt_s, const pacuda_uw_cuts *cuts,
+                                             uint32_t capacity, void *stream) {
     g_last_launches = 0;
-    if (!segs || !cuts || segments == 0 || segments > PACUDA_UW_MAX_SEGMENTS || !(sqrt_s > 0)) return ST_INVALID;
+    if (!segs || !cuts || segments == 0 || segments > PACUDA_UW_MAX_SEGMENTS || !(sqrt_s > 0) ||
+        !final_state_valid(final_state))
+        return ST_INVALID;
     CandidateSegments c;
     memset(&c, 0, sizeof c);
     uint32_t blocks = 0;
@@ -1237,48 +1266,67 @@ extern "C" int pacuda_uw_candidates_segments(const pacuda_uw_candidate_segment *
     c.block_first[segments] = blocks;
     c.segments = segments;
     if (blocks == 0) return ST_OK;
-    candidate_segments_kernel<<<blocks, 256, 0, (cudaStream_t)stream>>>(c, sqrt_s, Cuts{cuts->pt_min, cuts->eta_max,
-                                                                                       cuts->dr_min}, capacity);
+    const Cuts cc{cuts->pt_min, cuts->eta_max, cuts->dr_min};
+    if (final_state == 4)
+        candidate_segments_kernel<4><<<blocks, 256, 0, (cudaStream_t)stream>>>(c, sqrt_s, cc, capacity);
+    else
+        candidate_segments_kernel<3><<<blocks, 256, 0, (cudaStream_t)stream>>>(c, sqrt_s, cc, capacity);
     g_last_launches++;
     return failed(cudaGetLastError(), "candidates") ? ST_DEVICE : ST_OK;
 }
 
-extern "C" int pacuda_uw_points(uint64_t seed, const uint64_t *index, uint32_t n, double sqrt_s, double *momenta,
-                                float *inputs, uint32_t input_count, uint32_t family, double *jac, void *stream) {
+extern "C" int pacuda_uw_points(uint64_t seed, const uint64_t *index, uint32_t n, uint32_t final_state, double sqrt_s,
+                                double *momenta, float *inputs, uint32_t input_count, uint32_t family, double *jac,
+                                void *stream) {
     g_last_launches = 0;
-    if (!index || n == 0 || !(sqrt_s > 0) || (inputs && (input_count < 5 || input_count > IN || 5 + family >= input_count)))
+    const uint32_t x = 3 * final_state - 4;
+    if (!index || n == 0 || !(sqrt_s > 0) || !final_state_valid(final_state) ||
+        (inputs && (input_count < x || input_count > IN || x + family >= input_count)))
         return ST_INVALID;
-    points_kernel<<<(n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(seed, index, n, sqrt_s, momenta, inputs,
-                                                                       input_count, family, jac);
+    const dim3 grid((n + 127) / 128);
+    if (final_state == 4)
+        points_kernel<4><<<grid, 128, 0, (cudaStream_t)stream>>>(seed, index, n, sqrt_s, momenta, inputs, input_count,
+                                                                  family, jac);
+    else
+        points_kernel<3><<<grid, 128, 0, (cudaStream_t)stream>>>(seed, index, n, sqrt_s, momenta, inputs, input_count,
+                                                                  family, jac);
     g_last_launches++;
     return failed(cudaGetLastError(), "points") ? ST_DEVICE : ST_OK;
 }
 
-extern "C" int pacuda_uw_decide(uint64_t seed, const uint64_t *index, uint32_t n, const double *outputs,
-                                uint32_t helicities, const double *jac, const double *s, double w_max, double s_max,
-                                double r_max, uint8_t *keep, double *weight, double *me, void *stream) {
+extern "C" int pacuda_uw_decide(uint64_t seed, const uint64_t *index, uint32_t n, uint32_t final_state,
+                                const double *outputs, uint32_t helicities, const double *jac, const double *s,
+                                double w_max, double s_max, double r_max, uint8_t *keep, double *weight, double *me,
+                                void *stream) {
     g_last_launches = 0;
-    if (!index || !outputs || !jac || helicities == 0) return ST_INVALID;
+    if (!index || !outputs || !jac || helicities == 0 || !final_state_valid(final_state)) return ST_INVALID;
     if (n == 0) return ST_OK;
-    decide_kernel<<<(n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(seed, index, n, outputs, helicities, jac, s, w_max,
-                                                                       s_max, r_max, keep, weight, me);
+    const dim3 grid((n + 127) / 128);
+    if (final_state == 4)
+        decide_kernel<4><<<grid, 128, 0, (cudaStream_t)stream>>>(seed, index, n, outputs, helicities, jac, s, w_max,
+                                                                  s_max, r_max, keep, weight, me);
+    else
+        decide_kernel<3><<<grid, 128, 0, (cudaStream_t)stream>>>(seed, index, n, outputs, helicities, jac, s, w_max,
+                                                                  s_max, r_max, keep, weight, me);
     g_last_launches++;
     return failed(cudaGetLastError(), "decide") ? ST_DEVICE : ST_OK;
 }
 
 extern "C" int pacuda_uw_stage1_segments(const pacuda_sg_net *n, const pacuda_uw_segment *segs, uint32_t segments,
-                                         double mu, double sigma, uint32_t capacity, void *stream) {
+                                         uint32_t final_state, double mu, double sigma, uint32_t capacity,
+                                         void *stream) {
     g_last_launches = 0;
-    if (!n || !segs || segments == 0 || segments > PACUDA_UW_MAX_SEGMENTS) {
-        fprintf(stderr, "%s: stage 1: 1 to %d segments\n", kTag, PACUDA_UW_MAX_SEGMENTS);
+    if (!n || !segs || segments == 0 || segments > PACUDA_UW_MAX_SEGMENTS || !final_state_valid(final_state)) {
+        fprintf(stderr, "%s: stage 1: 1 to %d segments of 3 or 4 final-state partons\n", kTag, PACUDA_UW_MAX_SEGMENTS);
         return ST_INVALID;
     }
+    const uint32_t x = 3 * final_state - 4;
     ForwardArgs g;
     memset(&g, 0, sizeof g);
     uint32_t tiles = 0;
     for (uint32_t k = 0; k < segments; k++) {
         const pacuda_uw_segment &sg = segs[k];
-        if ((sg.count && !sg.index) || !sg.kept_index || !sg.kept_s || !sg.kept_count || 5 + sg.family >= n->inputs) {
+        if ((sg.count && !sg.index) || !sg.kept_index || !sg.kept_s || !sg.kept_count || x + sg.family >= n->inputs) {
             fprintf(stderr, "%s: stage 1: segment %u: a missing array or a family beyond the inputs\n", kTag, k);
             return ST_INVALID;
         }
@@ -1297,12 +1345,14 @@ extern "C" int pacuda_uw_stage1_segments(const pacuda_sg_net *n, const pacuda_uw
     g.mu = mu;
     g.sigma = sigma;
     g.capacity = capacity;
+    g.numbers = x;
     return launch_forward<FWD_CANDIDATES>(g, (cudaStream_t)stream) ? ST_OK : ST_DEVICE;
 }
 
 extern "C" int pacuda_uw_stage1(const pacuda_sg_net *n, uint64_t seed, const uint64_t *index, uint32_t count,
-                                uint32_t family, double mu, double sigma, double s_max, uint64_t *kept_index,
-                                double *kept_s, uint32_t capacity, unsigned long long *counter, void *stream) {
+                                uint32_t final_state, uint32_t family, double mu, double sigma, double s_max,
+                                uint64_t *kept_index, double *kept_s, uint32_t capacity, unsigned long long *counter,
+                                void *stream) {
     pacuda_uw_segment sg;
     sg.seed = seed;
     sg.index = index;
@@ -1313,5 +1363,5 @@ extern "C" int pacuda_uw_stage1(const pacuda_sg_net *n, uint64_t seed, const uin
     sg.kept_s = kept_s;
     sg.kept_count = counter;
     if (!index) return ST_INVALID;
-    return pacuda_uw_stage1_segments(n, &sg, 1, mu, sigma, capacity, stream);
+    return pacuda_uw_stage1_segments(n, &sg, 1, final_state, mu, sigma, capacity, stream);
 }

@@ -1,4 +1,4 @@
-"""Two-stage unweighting of massless 2 -> 3 subprocesses with the surrogate as its first stage
+"""Two-stage unweighting of massless 2 -> 3 and 2 -> 4 subprocesses with the surrogate as its first stage
 (include/pacuda_surrogate.h) and the f64 recurrence runner (include/pacuda_b200.h) as the exact
 second stage; plain unweighting with the runner alone beside it.
 
@@ -6,11 +6,12 @@ Per subprocess ("family"), candidates are seeded points of the unit cube mapped 
 (`oracle/unweight_oracle.py` restates the map, the cuts and the decisions):
 
 * plain: every candidate inside the cuts is evaluated exactly, w = |M|^2 J, and kept when
-  u5 w_max < w, with weight max(1, w / w_max);
+  u_a w_max < w, with weight max(1, w / w_max);
 * two-stage: the surrogate s = exp(mu + sigma net(x)), trained on the standardized log of the
   weight w = |M|^2 J, is evaluated on every candidate inside the cuts (one fused launch: inputs,
-  network, decision); the kept ones (u5 s_max < s) are evaluated exactly and kept when
-  u6 r_max < r, r = w / s, with weight max(1, s / s_max) max(1, r / r_max).
+  network, decision); the kept ones (u_a s_max < s) are evaluated exactly and kept when
+  u_b r_max < r, r = w / s, with weight max(1, s / s_max) max(1, r / r_max)
+(u_a, u_b: the candidate's two decision uniforms after its phase-space numbers).
 
 With those weights both samples are unbiased estimates of the distribution of w: a kept event's
 expected weight is w / (w_max) (plain) or w / (s_max r_max) (two-stage) for every candidate,
@@ -36,6 +37,11 @@ FAMILIES = list(processes.PP3J)
 ECM = 13000.0
 
 
+def final_state_of(name):
+    """The final-state partons of a subprocess (3 or 4)."""
+    return len(processes.PROCESSES[name]) - 2
+
+
 class Cuts(C.Structure):
     _fields_ = [("pt_min", C.c_double), ("eta_max", C.c_double), ("dr_min", C.c_double)]
 
@@ -53,20 +59,20 @@ class Segment(C.Structure):  # pacuda_uw_segment
 def _lib():
     L = S.lib()
     if not getattr(L, "_uw_bound", False):
-        L.pacuda_uw_candidates.argtypes = [C.c_uint64, C.c_uint64, C.c_uint32, C.c_double, C.c_void_p, C.c_void_p,
-                                           C.c_uint32, C.c_void_p, C.c_void_p]
-        L.pacuda_uw_points.argtypes = [C.c_uint64, C.c_void_p, C.c_uint32, C.c_double, C.c_void_p, C.c_void_p,
-                                       C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p]
-        L.pacuda_uw_decide.argtypes = [C.c_uint64, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p,
-                                       C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_void_p, C.c_void_p,
+        L.pacuda_uw_candidates.argtypes = [C.c_uint64, C.c_uint64, C.c_uint32, C.c_uint32, C.c_double, C.c_void_p,
+                                           C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]
+        L.pacuda_uw_points.argtypes = [C.c_uint64, C.c_void_p, C.c_uint32, C.c_uint32, C.c_double, C.c_void_p,
+                                       C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p]
+        L.pacuda_uw_decide.argtypes = [C.c_uint64, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32,
+                                       C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_void_p,
+                                       C.c_void_p, C.c_void_p, C.c_void_p]
+        L.pacuda_uw_stage1.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32,
+                                       C.c_double, C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_uint32,
                                        C.c_void_p, C.c_void_p]
-        L.pacuda_uw_stage1.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint32, C.c_uint32, C.c_double,
-                                       C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p,
-                                       C.c_void_p]
-        L.pacuda_uw_candidates_segments.argtypes = [C.c_void_p, C.c_uint32, C.c_double, C.c_void_p, C.c_uint32,
-                                                    C.c_void_p]
-        L.pacuda_uw_stage1_segments.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_double, C.c_double, C.c_uint32,
-                                                C.c_void_p]
+        L.pacuda_uw_candidates_segments.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_double, C.c_void_p,
+                                                    C.c_uint32, C.c_void_p]
+        L.pacuda_uw_stage1_segments.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_double,
+                                                C.c_double, C.c_uint32, C.c_void_p]
         L._uw_bound = True
     return L
 
@@ -87,16 +93,20 @@ def _stream():
 
 
 class Family:
-    """One subprocess: its plan for the runner (f64) and its buffers (candidates inside the cuts,
-    first-stage survivors, momenta and outputs of the exact evaluations, decisions)."""
+    """One subprocess: its plans for the runner (f64; a subprocess too large for one plan's words
+    has several, each over a part of its colour orderings, whose outputs add up) and its buffers
+    (candidates inside the cuts, first-stage survivors, momenta and outputs of the exact
+    evaluations, decisions)."""
 
     def __init__(self, name, index, capacity):
         import torch
 
         self.name, self.index = name, index
-        self.template = processes.template(name)
+        self.templates = processes.parts(name)
+        self.template = self.templates[0]
         self.helicities = self.template.outputs
-        self.plan = B.Plan(self.template, "f64")
+        self.legs = len(processes.PROCESSES[name])
+        self.plans = [B.Plan(t, "f64") for t in self.templates]
         self.capacity = capacity
         dev = "cuda"
         self.cand = torch.empty(capacity, dtype=torch.int64, device=dev)
@@ -105,8 +115,11 @@ class Family:
         self.jac = torch.empty(capacity, dtype=torch.float64, device=dev)
         self.keep = torch.empty(capacity, dtype=torch.uint8, device=dev)
         self.weight = torch.empty(capacity, dtype=torch.float64, device=dev)
-        self.momenta = torch.zeros(5 * 4 * capacity, dtype=torch.float64, device=dev)
+        self.momenta = torch.zeros(self.legs * 4 * capacity, dtype=torch.float64, device=dev)
         self.outputs = torch.empty(capacity * self.helicities, dtype=torch.float64, device=dev)
+        # the other parts' outputs, added to the first part's after each evaluation
+        self.part_outputs = [torch.empty(capacity * self.helicities, dtype=torch.float64, device=dev)
+                             for _ in self.templates[1:]]
 
 
 class Events:
@@ -135,16 +148,31 @@ class Pipeline:
         import torch
 
         self.names = list(families or FAMILIES)
+        states = {final_state_of(n) for n in self.names}
+        if len(states) != 1:
+            raise ValueError("the families of one pipeline have one final-state count")
+        self.final_state = states.pop()
+        self.numbers = 3 * self.final_state - 4
         self.sqrt_s = float(sqrt_s)
         self.cuts = Cuts(*cuts)
         self.seed = int(seed)
-        self.inputs = 5 + len(self.names)
+        self.inputs = self.numbers + len(self.names)
         self.capacity = capacity
         self.fams = [Family(n, k, capacity) for k, n in enumerate(self.names)]
         nf = len(self.fams)
         self.counters = torch.zeros(2 * nf, dtype=torch.int64, device="cuda")
-        self.batch = B.Batch([f.plan for f in self.fams], [f.momenta[: 20 * 1024] for f in self.fams],
-                             [f.outputs[: 1024 * f.helicities] for f in self.fams])
+        plans, moms, outs = self._parts([f.momenta[: 4 * f.legs * 1024] for f in self.fams], [1024] * nf)
+        self.batch = B.Batch(plans, moms, outs)
+
+    def _parts(self, moms, counts):
+        """Every family's plans with their momenta and output buffers (the batch's order)."""
+        plans, pm, po = [], [], []
+        for f, m, c in zip(self.fams, moms, counts):
+            for pl, o in zip(f.plans, [f.outputs] + f.part_outputs):
+                plans.append(pl)
+                pm.append(m)
+                po.append(o[: c * f.helicities])
+        return plans, pm, po
 
     def family_seed(self, k):
         return (self.seed * 1000003 + 7919 * (k + 1)) & ((1 << 64) - 1)
@@ -160,8 +188,8 @@ class Pipeline:
         for k, (fam, c) in enumerate(zip(self.fams, counts)):
             segs[k] = CandidateSegment(self.family_seed(k), first, int(c), fam.cand.data_ptr(),
                                        self.counters[k:k + 1].data_ptr())
-        _check(_lib().pacuda_uw_candidates_segments(segs, nf, self.sqrt_s, C.byref(self.cuts), self.capacity,
-                                                    _stream()), "candidates")
+        _check(_lib().pacuda_uw_candidates_segments(segs, nf, self.final_state, self.sqrt_s, C.byref(self.cuts),
+                                                    self.capacity, _stream()), "candidates")
         n = [int(v) for v in self.counters[:nf].tolist()]
         if max(n) > self.capacity:
             raise S.SurrogateError(f"{max(n)} passing candidates exceed the capacity {self.capacity}")
@@ -173,22 +201,29 @@ class Pipeline:
         the families' `jac` buffers and, optionally, the network's inputs into inputs[k]."""
         import torch
 
-        moms, outs, counts = [], [], []
+        moms, counts = [], []
         if not any(n):
             return [f.outputs.view(-1, f.helicities)[:0] for f in self.fams]
         for k, (fam, idx, m) in enumerate(zip(self.fams, index, n)):
             if m:
                 x = inputs[k] if inputs else None
-                _check(_lib().pacuda_uw_points(self.family_seed(k), _ptr(idx), m, self.sqrt_s, _ptr(fam.momenta),
-                                               _ptr(x) if x is not None else None, self.inputs if x is not None else 0,
-                                               k, _ptr(fam.jac) if jac else None, _stream()), "points")
+                _check(_lib().pacuda_uw_points(self.family_seed(k), _ptr(idx), m, self.final_state, self.sqrt_s,
+                                               _ptr(fam.momenta), _ptr(x) if x is not None else None,
+                                               self.inputs if x is not None else 0, k,
+                                               _ptr(fam.jac) if jac else None, _stream()), "points")
             mm = max(1, m)
-            moms.append(fam.momenta[: 20 * mm])
-            outs.append(fam.outputs[: mm * fam.helicities])
+            moms.append(fam.momenta[: 4 * fam.legs * mm])
             counts.append(mm)
-        self.batch.update(moms, counts, outs)
+        _, pm, po = self._parts(moms, counts)
+        self.batch.update(pm, [c for f, c in zip(self.fams, counts) for _ in f.plans], po)
         self.batch.run(torch.cuda.current_stream())
-        return [o.view(-1, f.helicities)[:m] for o, f, m in zip(outs, self.fams, n)]
+        out = []
+        for f, mm, m in zip(self.fams, counts, n):
+            o = f.outputs[: mm * f.helicities]
+            for extra in f.part_outputs:
+                o += extra[: mm * f.helicities]
+            out.append(o.view(-1, f.helicities)[:m])
+        return out
 
     def tune(self):
         """Times the runner's launch choices on the points of the last exact evaluation (batch_tune)."""
@@ -235,9 +270,9 @@ class Pipeline:
         events = []
         for k, (fam, m) in enumerate(zip(self.fams, n)):
             if m:
-                _check(_lib().pacuda_uw_decide(self.family_seed(k), _ptr(fam.cand), m, _ptr(out[k]), fam.helicities,
-                                               _ptr(fam.jac), None, w_max[k], 0.0, 0.0, _ptr(fam.keep),
-                                               _ptr(fam.weight), None, _stream()), "decide")
+                _check(_lib().pacuda_uw_decide(self.family_seed(k), _ptr(fam.cand), m, self.final_state, _ptr(out[k]),
+                                               fam.helicities, _ptr(fam.jac), None, w_max[k], 0.0, 0.0,
+                                               _ptr(fam.keep), _ptr(fam.weight), None, _stream()), "decide")
             events.append(Events(fam.cand[:m], fam.keep[:m], fam.weight[:m]))
         return events, sum(n)
 
@@ -251,7 +286,8 @@ class Pipeline:
         for k, (fam, m) in enumerate(zip(self.fams, n)):
             segs[k] = Segment(self.family_seed(k), fam.cand.data_ptr(), m, k, s_max[k], fam.kept.data_ptr(),
                               fam.kept_s.data_ptr(), self.counters[nf + k:nf + k + 1].data_ptr())
-        _check(_lib().pacuda_uw_stage1_segments(net.handle, segs, nf, mu, sigma, self.capacity, _stream()), "stage 1")
+        _check(_lib().pacuda_uw_stage1_segments(net.handle, segs, nf, self.final_state, mu, sigma, self.capacity,
+                                                _stream()), "stage 1")
         kept = [int(v) for v in self.counters[nf:].tolist()]
         if max(kept) > self.capacity:
             raise S.SurrogateError(f"{max(kept)} first-stage events exceed the capacity {self.capacity}")
@@ -259,9 +295,9 @@ class Pipeline:
         events = []
         for k, (fam, m) in enumerate(zip(self.fams, kept)):
             if m:
-                _check(_lib().pacuda_uw_decide(self.family_seed(k), _ptr(fam.kept), m, _ptr(out[k]), fam.helicities,
-                                               _ptr(fam.jac), _ptr(fam.kept_s), 0.0, s_max[k], r_max[k],
-                                               _ptr(fam.keep), _ptr(fam.weight), None, _stream()), "decide")
+                _check(_lib().pacuda_uw_decide(self.family_seed(k), _ptr(fam.kept), m, self.final_state, _ptr(out[k]),
+                                               fam.helicities, _ptr(fam.jac), _ptr(fam.kept_s), 0.0, s_max[k],
+                                               r_max[k], _ptr(fam.keep), _ptr(fam.weight), None, _stream()), "decide")
             events.append(Events(fam.kept[:m], fam.keep[:m], fam.weight[:m]))
         return events, sum(kept)
 

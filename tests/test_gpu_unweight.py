@@ -20,38 +20,64 @@ def _pipeline(families=("gg>ggg",), capacity=1 << 18):
     return unweight.Pipeline(families=list(families), capacity=capacity)
 
 
-def test_candidates_and_points_match_oracle():
+@pytest.mark.parametrize("family,final_state", [("gg>ggg", 3), ("gg>gggg", 4)])
+def test_candidates_and_points_match_oracle(family, final_state):
     import torch
 
-    pl = _pipeline()
+    from pacuda_b200 import unweight
+
+    pl = _pipeline((family,))
+    assert pl.final_state == final_state
     seed = pl.family_seed(0)
     n = 50000
     idx = pl.passing(0, 1000, n).cpu().numpy().astype(np.uint64)
-    u = U.uniforms(seed, np.arange(1000, 1000 + n, dtype=np.uint64))
-    p, jac = U.phase_space(u, SQRT_S)
+    u = U.uniforms(seed, np.arange(1000, 1000 + n, dtype=np.uint64), final_state)
+    p, jac = U.momenta(u, SQRT_S, final_state)
     want = np.arange(1000, 1000 + n, dtype=np.uint64)[U.passes(p)]
     assert np.array_equal(idx, want)
     # points of the passing candidates
-    from pacuda_b200 import unweight
-
-    m = len(idx)
+    m, legs, nx = len(idx), final_state + 2, 3 * final_state - 4
     ti = torch.tensor(idx.astype(np.int64), device="cuda")
-    mom = torch.empty(20 * m, dtype=torch.float64, device="cuda")
-    x = torch.empty(m, 6, dtype=torch.float32, device="cuda")
+    mom = torch.empty(4 * legs * m, dtype=torch.float64, device="cuda")
+    x = torch.empty(m, nx + 1, dtype=torch.float32, device="cuda")
     j = torch.empty(m, dtype=torch.float64, device="cuda")
     L = unweight._lib()
-    assert L.pacuda_uw_points(seed, C.c_void_p(ti.data_ptr()), m, SQRT_S, C.c_void_p(mom.data_ptr()),
-                              C.c_void_p(x.data_ptr()), 6, 0, C.c_void_p(j.data_ptr()), None) == 0
+    assert L.pacuda_uw_points(seed, C.c_void_p(ti.data_ptr()), m, final_state, SQRT_S, C.c_void_p(mom.data_ptr()),
+                              C.c_void_p(x.data_ptr()), nx + 1, 0, C.c_void_p(j.data_ptr()), None) == 0
     torch.cuda.synchronize()
     keep = U.passes(p)
-    got = mom.cpu().numpy().reshape(5, 4, m).transpose(2, 0, 1)
-    # exp, tanh and the boost's cancellations round differently on the device: 1e-9 relative
+    got = mom.cpu().numpy().reshape(legs, 4, m).transpose(2, 0, 1)
+    # exp, tanh and the boosts' cancellations round differently on the device: 1e-9 relative
     assert np.allclose(got, p[keep], rtol=1e-9, atol=1e-7)
     assert np.allclose(j.cpu().numpy(), jac[keep], rtol=1e-10, atol=0)
-    assert np.array_equal(x.cpu().numpy(), U.features(u[keep], 0, 1))
+    assert np.array_equal(x.cpu().numpy(), U.features(u[keep], 0, 1, final_state))
 
 
-def test_decisions_match_oracle():
+def test_parts_of_a_family_add_up_to_the_oracle():
+    """A subprocess of several plans (g g -> 4 g: three parts of its colour orderings): the
+    pipeline's exact evaluation is the parts' outputs added in part order, bit for bit the
+    oracle's parts added the same way."""
+    import torch
+
+    from oracle import oracle as O
+    from pacuda_b200 import phase_space, processes
+
+    pl = _pipeline(("gg>gggg",), capacity=1 << 12)
+    fam = pl.fams[0]
+    assert len(fam.plans) > 1
+    idx = pl.passing(0, 0, 4000)[:300]
+    m = idx.numel()
+    out = pl.exact([idx], [m])[0].cpu().numpy()
+    p = fam.momenta[: 24 * m].cpu().numpy().reshape(6, 4, m).transpose(2, 0, 1).copy()
+    want = None
+    for t in processes.parts("gg>gggg"):
+        _, w = O.evaluate(t, p, kernel=1)
+        want = w if want is None else want + w
+    assert np.array_equal(out.view(np.uint64), want.view(np.uint64))
+
+
+@pytest.mark.parametrize("final_state", [3, 4])
+def test_decisions_match_oracle(final_state):
     import torch
 
     from pacuda_b200 import unweight
@@ -74,24 +100,27 @@ def test_decisions_match_oracle():
     for h in range(hel):
         m2 = m2 + out[:, h]
     w = m2 * jac
-    u = U.uniforms(seed, idx)
+    u = U.uniforms(seed, idx, final_state)
+    nx = U.numbers(final_state)
     # plain
     w_max = float(np.quantile(w, 0.9))
-    assert L.pacuda_uw_decide(seed, P(ti), n, P(to), hel, P(tj), None, w_max, 0.0, 0.0, P(keep), P(wt), P(me), None) == 0
-    k, weights = U.plain_decide(w, u[:, 5], w_max)
+    assert L.pacuda_uw_decide(seed, P(ti), n, final_state, P(to), hel, P(tj), None, w_max, 0.0, 0.0, P(keep), P(wt),
+                              P(me), None) == 0
+    k, weights = U.plain_decide(w, u[:, nx], w_max)
     assert np.array_equal(keep.cpu().numpy().astype(bool), k)
     assert np.array_equal(wt.cpu().numpy(), weights)
     assert np.array_equal(me.cpu().numpy(), m2)
     # second stage
     s_max, r_max = float(np.quantile(s, 0.95)), 1.2
-    assert L.pacuda_uw_decide(seed, P(ti), n, P(to), hel, P(tj), P(ts), 0.0, s_max, r_max, P(keep), P(wt), None,
-                              None) == 0
-    k2, w2, _ = U.stage2_decide(w, s, np.maximum(1.0, s / s_max), u[:, 6], r_max)
+    assert L.pacuda_uw_decide(seed, P(ti), n, final_state, P(to), hel, P(tj), P(ts), 0.0, s_max, r_max, P(keep),
+                              P(wt), None, None) == 0
+    k2, w2, _ = U.stage2_decide(w, s, np.maximum(1.0, s / s_max), u[:, nx + 1], r_max)
     assert np.array_equal(keep.cpu().numpy().astype(bool), k2)
     assert np.allclose(wt.cpu().numpy(), w2, rtol=1e-15, atol=0)
 
 
-def test_stage1_matches_oracle():
+@pytest.mark.parametrize("family,final_state", [("gg>ggg", 3), ("gg>gggg", 4)])
+def test_stage1_matches_oracle(family, final_state):
     """The fused first stage (inputs, network, decision in one launch) over a list of
     candidates keeps those the restatement keeps with the CPU network's values, except where
     u s_max lies within 2 % of s (the device network rounds differently)."""
@@ -101,31 +130,32 @@ def test_stage1_matches_oracle():
     from pacuda_b200 import surrogate as S
     from pacuda_b200 import unweight
 
-    pl = _pipeline()
-    net = S.Network(6, max_batch=1024, seed=5)
+    pl = _pipeline((family,))
+    nx = U.numbers(final_state)
+    net = S.Network(nx + 1, max_batch=1024, seed=5)
     p = net.params()
     mu, sigma = -2.0, 1.5
     n, first = 40000, 123
     seed = pl.family_seed(0)
     cand = pl.passing(0, first, n)  # sorted indices inside the cuts
     idx = cand.cpu().numpy().astype(np.uint64)
-    u = U.uniforms(seed, idx)
-    out = SO.forward(p, U.features(u, 0, 1)).astype(np.float64)
+    u = U.uniforms(seed, idx, final_state)
+    out = SO.forward(p, U.features(u, 0, 1, final_state)).astype(np.float64)
     sv = np.exp(mu + sigma * out)
     s_max = float(np.quantile(sv, 0.99))
     pl.counters.zero_()
     L = unweight._lib()
     f0 = pl.fams[0]
-    assert L.pacuda_uw_stage1(net.handle, seed, C.c_void_p(cand.data_ptr()), cand.numel(), 0, mu, sigma, s_max,
-                              C.c_void_p(f0.kept.data_ptr()), C.c_void_p(f0.kept_s.data_ptr()), pl.capacity,
+    assert L.pacuda_uw_stage1(net.handle, seed, C.c_void_p(cand.data_ptr()), cand.numel(), final_state, 0, mu, sigma,
+                              s_max, C.c_void_p(f0.kept.data_ptr()), C.c_void_p(f0.kept_s.data_ptr()), pl.capacity,
                               C.c_void_p(pl.counters.data_ptr()), None) == 0
     torch.cuda.synchronize()
     assert net.error() == 0
     kept = int(pl.counters[0])
     got = f0.kept[:kept].cpu().numpy().astype(np.uint64)
     pos = {int(c): i for i, c in enumerate(idx)}
-    want_keep = u[:, 5] * s_max < sv
-    borderline = np.abs(u[:, 5] * s_max - sv) <= 0.02 * np.maximum(sv, 1e-300)
+    want_keep = u[:, nx] * s_max < sv
+    borderline = np.abs(u[:, nx] * s_max - sv) <= 0.02 * np.maximum(sv, 1e-300)
     got_mask = np.zeros(len(idx), dtype=bool)
     got_mask[[pos[int(c)] for c in got]] = True
     assert np.array_equal(got_mask[~borderline], want_keep[~borderline])

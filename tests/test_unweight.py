@@ -52,6 +52,81 @@ def test_map_volume_and_distributions_match_rambo():
         assert chi2 / 20 < 3.0, chi2
 
 
+def test_four_parton_map_is_massless_and_conserves_momentum():
+    u = U.uniforms(5, np.arange(4096, dtype=np.uint64), final_state=4)
+    assert u.shape == (4096, 10)
+    p, jac = U.momenta(u, 13000.0, final_state=4)
+    assert p.shape == (4096, 6, 4)
+    assert np.allclose(p[:, :, 0] ** 2 - (p[:, :, 1:] ** 2).sum(axis=2), 0.0, atol=1e-6 * 13000.0 ** 2 * 1e-6)
+    assert np.allclose(p[:, :2].sum(axis=1), p[:, 2:].sum(axis=1), atol=1e-8 * 13000.0)
+    assert np.all(p[:, 2:, 0] >= 0) and np.all(jac >= 0)
+
+
+def test_four_parton_map_volume_and_distributions_match_rambo():
+    """The 2 -> 4 map's weight, taken at flat invariants and angles (s_Q / s, s_R / s_Q,
+    (1 + cos theta) / 2 uniform: the uniforms that give them, times the inverse transforms'
+    derivatives), is the flat sequential-decay density s s_Q (1 - s_Q / s)(1 - s_R / s_Q) / (2048 pi^5)
+    at every point, which integrates to the massless four-body volume s^2 / (24576 pi^5); and the
+    map's momenta weighted by it follow RAMBO's flat distributions (every parton's energy, every
+    pair's invariant mass)."""
+    sqrt_s, n = 1000.0, 1 << 18
+    s = sqrt_s * sqrt_s
+    vol = s * s / (24576.0 * math.pi ** 5)
+    v = np.random.default_rng(13).uniform(size=(n, 8))
+    u = np.zeros((n, 10))
+    dxdv = np.ones(n)
+    for k in (0, 3):  # logistic invariants
+        u[:, k] = (np.log(v[:, k] / (1.0 - v[:, k])) / U.MAP_L + 1.0) / 2.0
+        dxdv /= 2.0 * U.MAP_L * v[:, k] * (1.0 - v[:, k])
+    for k, e in ((1, U.MAP_E1), (4, U.MAP_E2), (6, U.MAP_E2)):  # tanh angles
+        c = 2.0 * v[:, k] - 1.0
+        u[:, k] = (np.arctanh(c) / e + 1.0) / 2.0
+        dxdv /= e * (1.0 - c * c)
+    for k in (2, 5, 7):
+        u[:, k] = v[:, k]
+    inside = ((u[:, :8] > 0) & (u[:, :8] < 1)).all(axis=1)  # all but the map's uncovered edges
+    assert inside.mean() > 0.9999
+    u, v, dxdv = u[inside], v[inside], dxdv[inside]
+    p, jac = U.momenta(u, sqrt_s, final_state=4)
+    flat = jac * dxdv
+    sq = s * v[:, 0]
+    want = s * sq * (1.0 - v[:, 0]) * (1.0 - v[:, 3]) / (2048.0 * math.pi ** 5)
+    assert np.allclose(flat, want, rtol=1e-9, atol=0)
+    assert abs(flat.mean() - vol) < 4 * flat.std() / math.sqrt(flat.size)
+    r = phase_space.rambo(6, n, 14, ecm=sqrt_s)
+    pairs = [(i, j) for i in range(2, 6) for j in range(i + 1, 6)]
+
+    def obs(q):
+        e = q[:, 2:, 0].reshape(-1)
+        m = []
+        for i, j in pairs:
+            k = q[:, i] + q[:, j]
+            m.append(np.sqrt(np.maximum(0.0, k[:, 0] ** 2 - (k[:, 1:] ** 2).sum(axis=1))))
+        return (e, 4), (np.stack(m, axis=1).reshape(-1), len(pairs))
+
+    for (a, na), (b, _) in zip(obs(p), obs(r)):
+        edges = np.linspace(0, max(a.max(), b.max()), 21)
+        wa = np.repeat(flat, na) * n / flat.size
+        ha, _ = np.histogram(a, edges, weights=wa)
+        va, _ = np.histogram(a, edges, weights=wa ** 2)
+        hb, _ = np.histogram(b, edges)
+        hb = hb * vol
+        vb = hb * vol
+        chi2 = ((ha - hb) ** 2 / (va + vb + 1e-300))[hb > 0].sum()
+        assert chi2 / 20 < 3.0, chi2
+
+
+def test_four_parton_features_and_cuts():
+    u = U.uniforms(21, np.arange(5000, dtype=np.uint64), final_state=4)
+    f = U.features(u, 2, 4, final_state=4)
+    assert f.shape == (5000, 12) and np.array_equal(f[:, :8], u[:, :8].astype(np.float32))
+    assert np.all(f[:, 8 + 2] == 1.0) and np.all(f[:, [8, 9, 11]] == 0.0)
+    p, _ = U.momenta(u, 13000.0, final_state=4)
+    ok = U.passes(p, 20.0, 5.0, 0.4)
+    assert 0.05 < ok.mean() < 1.0
+    assert np.array_equal(ok, phase_space.passes_cuts(p))
+
+
 def test_cuts_agree_with_the_benchmark_cuts():
     u = U.uniforms(3, np.arange(20000, dtype=np.uint64))
     p, _ = U.phase_space(u, 13000.0)
