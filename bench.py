@@ -638,10 +638,12 @@ def dram_bytes_per_point():
 
 
 def hbm_peak():
+    """(HBM GB/s of this pool's B200s, its source): MEASURED_PEAKS.json's copy bandwidth, else the
+    earlier measurement on this pool (6650)."""
     try:
-        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]
+        return float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs"
     except (OSError, ValueError, KeyError):
-        return 6650.0
+        return 6650.0, "fallback (no MEASURED_PEAKS.json)"
 
 
 def bf16_peak():
@@ -1035,7 +1037,7 @@ def main():
                                 "algorithmic_gbs": alg_bytes / (ms * 1e-3) / 1e9,
                                 "algorithmic_bytes_note": "momenta in (legs x 4 x 8 B) and every helicity output out "
                                                           "(8 B each) per point",
-                                "peak_gbs": hbm_peak(), "peak_source": "MEASURED_PEAKS.json hbm_gbs"},
+                                "peak_gbs": hbm_peak()[0], "peak_source": hbm_peak()[1]},
                         "flops_per_point": {n: pl.flops for (n, _, _), pl in zip(fams, plans)}},
            "points_per_family": {n: p.shape[0] for n, _, p in fams},
            "lanes_per_point": {n: batch.lanes_per_point(k) for k, (n, _, _) in enumerate(fams)},
@@ -1097,8 +1099,10 @@ def main():
 
             res["surrogate"] = surrogate_line(torch)
             if not args.no_precision:
-                # p p -> 4 jets: the combined configuration's learned part
-                res["surrogate_pp4j"] = surrogate_line(torch, families=processes.PP4J)
+                # p p -> 4 jets: the combined configuration's learned part (2^25 candidates: 5.6 % pass
+                # the cuts and plain unweighting keeps 7e-4 of those, so 2^22 would give ~160 events)
+                res["surrogate_pp4j"] = surrogate_line(torch, families=processes.PP4J, candidates=1 << 25,
+                                                       epochs=600)
     if world > 1:
         import torch.distributed as dist
 
