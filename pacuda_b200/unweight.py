@@ -323,11 +323,18 @@ def train(net, x, y, epochs, batch=16384, lr=2e-3, lr_end=2e-5, seed=0, importan
     loss = torch.zeros(1, dtype=torch.float32, device="cuda")
     history = []
     step = 0
+    if importance is not None:
+        # draws by inverse CDF (the cumulative sum once, in f64 on the host; uniforms from the
+        # seeded generator; a sorted search): the same draws on every run, which torch's
+        # multinomial sampling on the device does not give
+        cdf = torch.cumsum(importance.detach().double().cpu(), 0)
+        cdf = (cdf / cdf[-1]).to(x.device)
     for _ in range(epochs):
         if importance is None:
             perm = torch.randperm(x.shape[0], device="cuda", generator=gen)[:n]
         else:
-            perm = torch.multinomial(importance, n, replacement=True, generator=gen)
+            u = torch.rand(n, dtype=torch.float64, device="cuda", generator=gen)
+            perm = torch.searchsorted(cdf, u).clamp_(max=x.shape[0] - 1)
         xs, ys = x[perm].contiguous(), y[perm].contiguous()
         loss.zero_()
         for b in range(n // batch):

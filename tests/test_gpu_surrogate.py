@@ -135,3 +135,27 @@ def test_training_fits_a_smooth_function():
     assert losses[-1] < losses[0] / 20, losses
     pred = net.forward(xt).cpu().numpy()
     assert np.mean((pred - ys) ** 2) < losses[0] / 20
+
+
+def test_kernels_are_deterministic():
+    """The same inputs give the same bits: the inference kernel's outputs, the gradient and loss
+    of one batch computed twice, and two networks of one seed after the same 40 Adam steps (the
+    kernels' sums run in fixed orders; no atomics in any value)."""
+    import torch
+
+    from pacuda_b200 import surrogate as S
+
+    net, _ = _net(3, batch=4096)
+    x = torch.tensor(_inputs(4096, 4), device="cuda")
+    y = torch.tensor(np.random.default_rng(5).normal(size=4096).astype(np.float32), device="cuda")
+    g1, l1 = net.gradients(x, y)
+    g2, l2 = net.gradients(x, y)
+    assert torch.equal(g1, g2) and torch.equal(l1, l2)
+    xs = torch.tensor(_inputs(40000, 9), device="cuda")
+    assert torch.equal(net.forward(xs), net.forward(xs))
+    a, b = S.Network(INPUTS, max_batch=4096, seed=21), S.Network(INPUTS, max_batch=4096, seed=21)
+    for step in range(40):
+        for n in (a, b):
+            n.train_step(x, y, 1e-3 * (1 + step % 3))
+    assert a.error() == 0 and b.error() == 0
+    assert np.array_equal(a.params().view(np.uint32), b.params().view(np.uint32))
