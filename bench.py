@@ -11,7 +11,8 @@ colour orderings summed, in f64 (bit for bit the reference runner's f64 arithmet
   L2, so no flush is needed); clocks: nvidia-smi samples taken inside the timed region;
 * e2e: the call a generator makes, umami_matrix_element of the p p -> 3 jets UMAMI library
   (pacuda_b200/umami), one call per step over all events from pinned host momenta to |M|^2 in
-  host memory, the copies in the timed region; e2e_abi: the runner's own C ABI
+  host memory, the copies in the timed region (under torchrun every rank's call on its shard,
+  started together, the slowest rank's time); e2e_abi: the runner's own C ABI
   (pacman_recurrence_v1_run + _reduce_resolved per tile of 2^16 points) the same way;
 * reference_gpu: the reference's own runner (recurrence_runner.cu built from its sources for
   sm_100a, unmodified) through its C ABI on the same points, per kernel kind (f64, df64, mixed),
@@ -800,10 +801,12 @@ def reference_gpu(kinds=("f64", "df64", "mixed"), steps=2, warmup=1, keep_path=N
     return res
 
 
-def e2e_umami(fams, steps, warmup, outs=None):
+def e2e_umami(fams, steps, warmup, outs=None, sync=None):
     """points/s through the UMAMI call a generator makes (umami_matrix_element, the reference's
     production entry point): every step one call over all events, from pinned host momenta (copied
-    to the device inside the call) to |M|^2 in host memory (copied back inside the call)."""
+    to the device inside the call) to |M|^2 in host memory (copied back inside the call). `sync`,
+    when given, is called right before the timed calls (the ranks' barrier); the line's `seconds`
+    is this process's time per step."""
     import ctypes as C
     import tempfile
 
@@ -854,6 +857,8 @@ def e2e_umami(fams, steps, warmup, outs=None):
 
     for _ in range(warmup):
         step()
+    if sync:
+        sync()
     t0 = time.perf_counter()
     for _ in range(steps):
         step()
@@ -873,7 +878,7 @@ def e2e_umami(fams, steps, warmup, outs=None):
         r.lib.pacman_recurrence_v1_host_free(ptr)
     return {"value": n / dt, "unit": "points/s", "h2d_bytes_per_step": n * legs * 4 * 8 + n * 24,
             "d2h_bytes_per_step": n * 8, "api": "umami_matrix_element (helicity sum, one call per step)",
-            "calls_per_step": 1}
+            "calls_per_step": 1, "seconds": dt}
 
 
 def main():
@@ -1047,6 +1052,23 @@ def main():
            "max_m2_per_family": [float(x) for x in peak_m2.cpu()]}
     if clk:
         res["clocks"] = clk
+    if world > 1 and not args.no_e2e and not args.family:
+        # end to end at N GPUs: every rank's UMAMI call on its own shard from its pinned host
+        # momenta, the ranks started together; the job's time per step is the slowest rank's
+        from pacuda_b200.umami import build as ub
+
+        if rank == 0:
+            ub.pp3j_library()  # built once, before the other ranks look for it
+        dist.barrier()
+        line = e2e_umami(fams, max(3, args.steps // 2), 2, [o.cpu().numpy() for o in out], sync=dist.barrier)
+        slowest = torch.tensor([line["seconds"]], dtype=torch.float64, device="cuda")
+        dist.all_reduce(slowest, op=dist.ReduceOp.MAX)
+        line["value"] = points / float(slowest)
+        line["seconds"] = float(slowest)
+        line["h2d_bytes_per_step"] *= world  # the whole job's copies
+        line["d2h_bytes_per_step"] *= world
+        line["api"] += f", one call per rank on its shard, {world} ranks, the slowest rank's time"
+        res["e2e"] = line
     if rank == 0 and world == 1:
         if not args.no_e2e:
             outs = [o.cpu().numpy() for o in out]
