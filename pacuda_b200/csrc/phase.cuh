@@ -216,5 +216,150 @@ template <int L> __device__ __forceinline__ bool passes(const double (&p)[L][4],
     return true;
 }
 
+// ---- a first look in f32: candidates that certainly fail the cuts ----------------------------
+// The f64 map above defines every candidate's point, and the cuts on it decide the list. Most
+// candidates fail by a wide margin (a soft or collinear parton), so the listing first maps each
+// one in f32, written to stay accurate where the f64 form cancels: 1 - sigma, cos(theta) and
+// sin(theta) from one exponential each, and a boost by velocity |q| / E_q of a frame of mass m
+// with gamma - 1 = |q|^2 / (m (E_q + m)) and gamma beta = |q| / m instead of 1 / sqrt(1 - beta^2).
+// Its uniforms are the same stream's states read to 24 bits, its exponentials and angles the
+// hardware approximations (relative errors near 2^-21). Every final-state component it gives then
+// differs from the f64 map's by about 5e-7 sqrt(s) at most (the 24-bit uniforms dominate; a float32
+// restatement of these formulas on 4e5 candidates of each map stays below that against the f64
+// map), 40 times less than the margin: a candidate is dropped here only when it fails a cut by more
+// than PHASE32_DELTA = 2e-5 sqrt(s) per component allows (pT by 2 delta, |pz| - pT sinh(eta_max)
+// by (1 + 1.5 sinh(eta_max)) delta, Delta R by the propagated bounds on eta and phi). Every other
+// candidate goes through the f64 map and cuts, so the list is the f64 decision's.
+constexpr float PHASE32_DELTA = 2e-5f;
+
+// the first k uniforms of candidate `index` to 24 bits (the states of uniforms() above)
+template <int K> __device__ __forceinline__ void uniforms32(uint64_t seed, uint64_t index, float (&u)[K]) {
+    uint64_t state = splitmix64(seed ^ (index * 0xD1B54A32D192ED03ull)) | 1ull;
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+        state ^= state << 13;
+        state ^= state >> 7;
+        state ^= state << 17;
+        u[k] = ((float)(uint32_t)(state >> 40) + 0.5f) * 5.9604644775390625e-8f;
+    }
+}
+
+// cos(theta) = tanh(x), sin(theta) = 1 / cosh(x) from t = e^-|x|, and (cos, sin)(2 pi v): a unit
+// direction
+__device__ __forceinline__ void direction32(float x, float v, float (&n)[3]) {
+    const float t = __expf(-fabsf(x)), t2 = t * t, r = 1.0f / (1.0f + t2);
+    const float c = copysignf((1.0f - t2) * r, x), st = 2.0f * t * r;
+    float sp, cp;
+    __sincosf(3.14159265358979f * (2.0f * v - 1.0f), &sp, &cp);  // the angle 2 pi v - pi
+    n[0] = -st * cp;
+    n[1] = -st * sp;
+    n[2] = c;
+}
+
+// the decay of a frame of mass m moving along the unit vector w with momentum q and energy e
+// into two massless partons back to back along +-n in its rest frame: their momenta in the
+// frame where it moves (its rest-frame momentum k = m / 2)
+__device__ __forceinline__ void decay32(float m, float e, float q, const float (&w)[3], const float (&n)[3],
+                                        float (&a)[3], float (&b)[3]) {
+    const float k = 0.5f * m, cw = n[0] * w[0] + n[1] * w[1] + n[2] * w[2];
+    const float along = q * q * cw / (2.0f * (e + m)), mid = 0.5f * q;
+    for (int i = 0; i < 3; i++) {
+        a[i] = k * n[i] + (along + mid) * w[i];
+        b[i] = -k * n[i] + (mid - along) * w[i];
+    }
+}
+
+// a momentum (energy en, vector v) in the frame of mass m moving along w with momentum q and
+// energy e, seen where it moves: the vector part
+__device__ __forceinline__ void boost32(float m, float e, float q, const float (&w)[3], float en, const float (&v)[3],
+                                        float (&out)[3]) {
+    const float par = v[0] * w[0] + v[1] * w[1] + v[2] * w[2];
+    const float f = (q * q * par / (e + m) + q * en) / m;
+    for (int i = 0; i < 3; i++) out[i] = v[i] + f * w[i];
+}
+
+// sigma(L (2 u - 1)) and 1 - sigma from one exponential
+__device__ __forceinline__ void logistic32(float u, float &sg, float &omsg) {
+    const float ey = __expf(-(float)MAP_L * (2.0f * u - 1.0f)), r = 1.0f / (1.0f + ey);
+    sg = r;
+    omsg = ey * r;
+}
+
+// the final-state partons' (px, py, pz) of the 2 -> 3 and 2 -> 4 maps in f32
+__device__ __forceinline__ void final32(const float (&u)[Space<3>::NUMBERS], double sqrt_s, float (&p)[3][3]) {
+    const float rs = (float)sqrt_s;
+    float sg, omsg;
+    logistic32(u[0], sg, omsg);
+    const float e1 = 0.5f * rs * omsg, eq = 0.5f * rs * (1.0f + sg), mq = rs * sqrtf(sg);
+    float n1[3], n2[3], w[3];
+    direction32((float)MAP_E1 * (2.0f * u[1] - 1.0f), u[2], n1);
+    for (int i = 0; i < 3; i++) {
+        p[0][i] = e1 * n1[i];
+        w[i] = -n1[i];
+    }
+    direction32((float)MAP_E2 * (2.0f * u[3] - 1.0f), u[4], n2);
+    decay32(mq, eq, e1, w, n2, p[1], p[2]);
+}
+
+__device__ __forceinline__ void final32(const float (&u)[Space<4>::NUMBERS], double sqrt_s, float (&p)[4][3]) {
+    const float rs = (float)sqrt_s;
+    float sg1, omsg1, sg2, omsg2;
+    logistic32(u[0], sg1, omsg1);
+    logistic32(u[3], sg2, omsg2);
+    const float e1 = 0.5f * rs * omsg1, eq = 0.5f * rs * (1.0f + sg1), mq = rs * sqrtf(sg1);
+    const float k2 = 0.5f * mq * omsg2, er = 0.5f * mq * (1.0f + sg2), mr = mq * sqrtf(sg2);
+    float n1[3], n2[3], n3[3], w[3], v[3];
+    direction32((float)MAP_E1 * (2.0f * u[1] - 1.0f), u[2], n1);
+    for (int i = 0; i < 3; i++) {
+        p[0][i] = e1 * n1[i];
+        w[i] = -n1[i];
+    }
+    direction32((float)MAP_E2 * (2.0f * u[4] - 1.0f), u[5], n2);
+    direction32((float)MAP_E2 * (2.0f * u[6] - 1.0f), u[7], n3);
+    // in Q's rest frame: p2 = k2 n2, R moving along -n2; p3, p4 from R's decay
+    float q2[3], q3[3], q4[3];
+    for (int i = 0; i < 3; i++) {
+        q2[i] = k2 * n2[i];
+        v[i] = -n2[i];
+    }
+    decay32(mr, er, k2, v, n3, q3, q4);
+    const float c3 = n3[0] * v[0] + n3[1] * v[1] + n3[2] * v[2];
+    const float en3 = 0.5f * (er + k2 * c3), en4 = 0.5f * (er - k2 * c3);
+    // to the lab along Q
+    boost32(mq, eq, e1, w, k2, q2, p[1]);
+    boost32(mq, eq, e1, w, en3, q3, p[2]);
+    boost32(mq, eq, e1, w, en4, q4, p[3]);
+}
+
+// whether the candidate whose f32 partons are p certainly fails the cuts (see above)
+template <int F>
+__device__ __forceinline__ bool surely_fails32(const float (&p)[F][3], double sqrt_s, const Cuts &c) {
+    const float d = PHASE32_DELTA * (float)sqrt_s, sh = sinhf((float)c.eta_max);
+    float pt[F];
+    for (int i = 0; i < F; i++) {
+        pt[i] = sqrtf(p[i][0] * p[i][0] + p[i][1] * p[i][1]);
+        if (pt[i] < (float)c.pt_min - 2.0f * d) return true;
+        if (fabsf(p[i][2]) - pt[i] * sh > d * (1.0f + 1.5f * sh)) return true;
+    }
+    float eta[F], phi[F], err[F];
+    for (int i = 0; i < F; i++) {
+        const float low = pt[i] - 2.0f * d;
+        if (!(low > 0.0f)) return false;
+        const float z = p[i][2] / pt[i];
+        eta[i] = copysignf(__logf(fabsf(z) + sqrtf(z * z + 1.0f)), z);
+        phi[i] = atan2f(p[i][1], p[i][0]);
+        err[i] = 4.0f * d / low + 1e-5f;  // eta's bound 2.5 d / low, phi's 1.5 d / low, the functions' rounding
+    }
+    const float pi = 3.14159265f;
+    for (int i = 0; i < F; i++)
+        for (int j = i + 1; j < F; j++) {
+            float dp = fabsf(phi[i] - phi[j]);
+            if (dp > pi) dp = 2.0f * pi - dp;
+            const float de = eta[i] - eta[j];
+            if (sqrtf(de * de + dp * dp) + err[i] + err[j] + 1e-5f < (float)c.dr_min) return true;
+        }
+    return false;
+}
+
 }  // namespace phase
 }  // namespace pacuda

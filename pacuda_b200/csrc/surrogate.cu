@@ -1120,28 +1120,63 @@ using pacuda::phase::Cuts;
 using pacuda::phase::Map;
 using pacuda::phase::Space;
 
-// candidates first .. first + count - 1 of N final-state partons: the indices of those inside the
-// cuts (unordered, warp-aggregated appends; `count_out` counts all of them, also beyond `capacity`)
+// The candidates first .. first + count - 1 of one stream: the indices of those inside the cuts,
+// appended (unordered, warp-aggregated) to index[] while below `capacity`; *count_out counts all
+// of them. A block takes 256 consecutive candidates: each thread gives its candidate the f32 first
+// look (phase.cuh surely_fails32), the ones it cannot drop are gathered in shared memory, and the
+// block's first threads take those through the f64 map and cuts, which decide. (Blocks of 256
+// threads: the kernels below are launched so.)
 template <int N>
-__global__ void candidates_kernel(uint64_t seed, uint64_t first, uint32_t count, double sqrt_s, Cuts cuts,
-                                  uint64_t *index, uint32_t capacity, unsigned long long *count_out) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    bool pass = false;
+__device__ __forceinline__ void list_block(uint64_t seed, uint64_t first, uint32_t count, double sqrt_s,
+                                           const Cuts &cuts, uint64_t *index, uint32_t capacity,
+                                           unsigned long long *count_out, uint32_t i) {
+    constexpr int F = N, L = Space<N>::LEGS;
+    __shared__ uint64_t maybe[256];
+    __shared__ uint32_t n_maybe;
+    if (threadIdx.x == 0) n_maybe = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    bool check = false;
     if (i < count) {
-        double u[Space<N>::UNIFORMS], p[Space<N>::LEGS][4];
-        pacuda::phase::uniforms(seed, first + i, u);
+        float u[Space<N>::NUMBERS], q[F][3];
+        pacuda::phase::uniforms32(seed, first + i, u);
+        pacuda::phase::final32(u, sqrt_s, q);
+        check = !pacuda::phase::surely_fails32(q, sqrt_s, cuts);
+    }
+    {
+        const unsigned ballot = __ballot_sync(0xffffffffu, check);
+        uint32_t base = 0;
+        if (lane == 0 && ballot) base = atomicAdd(&n_maybe, (uint32_t)__popc(ballot));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (check) maybe[base + __popc(ballot & ((1u << lane) - 1u))] = first + i;
+    }
+    __syncthreads();
+    const uint32_t m = n_maybe;
+    if (threadIdx.x >= ((m + 31u) & ~31u)) return;  // whole warps without a listed candidate
+    bool pass = false;
+    uint64_t cand = 0;
+    if (threadIdx.x < m) {
+        cand = maybe[threadIdx.x];
+        double u[Space<N>::UNIFORMS], p[L][4];
+        pacuda::phase::uniforms(seed, cand, u);
         Map<N>::momenta(u, sqrt_s, p);
         pass = pacuda::phase::passes(p, cuts);
     }
     const unsigned ballot = __ballot_sync(0xffffffffu, pass);
-    const int lane = threadIdx.x & 31;
     unsigned long long base = 0;
     if (lane == 0 && ballot) base = atomicAdd(count_out, (unsigned long long)__popc(ballot));
     base = __shfl_sync(0xffffffffu, base, 0);
     if (pass) {
         const unsigned long long slot = base + __popc(ballot & ((1u << lane) - 1u));
-        if (slot < capacity) index[slot] = first + i;
+        if (slot < capacity) index[slot] = cand;
     }
+}
+
+template <int N>
+__global__ void __launch_bounds__(256) candidates_kernel(uint64_t seed, uint64_t first, uint32_t count, double sqrt_s,
+                                                         Cuts cuts, uint64_t *index, uint32_t capacity,
+                                                         unsigned long long *count_out) {
+    list_block<N>(seed, first, count, sqrt_s, cuts, index, capacity, count_out, blockIdx.x * 256 + threadIdx.x);
 }
 
 // several subprocesses' candidates in one launch: block b lists segment k's candidates when
@@ -1153,27 +1188,13 @@ struct CandidateSegments {
 };
 
 template <int N>
-__global__ void candidate_segments_kernel(CandidateSegments c, double sqrt_s, Cuts cuts, uint32_t capacity) {
+__global__ void __launch_bounds__(256) candidate_segments_kernel(CandidateSegments c, double sqrt_s, Cuts cuts,
+                                                                 uint32_t capacity) {
     uint32_t k = 0;
     while (k + 1 < c.segments && blockIdx.x >= c.block_first[k + 1]) k++;
     const pacuda_uw_candidate_segment &sg = c.seg[k];
-    const uint32_t i = (blockIdx.x - c.block_first[k]) * blockDim.x + threadIdx.x;
-    bool pass = false;
-    if (i < sg.count) {
-        double u[Space<N>::UNIFORMS], p[Space<N>::LEGS][4];
-        pacuda::phase::uniforms(sg.seed, sg.first + i, u);
-        Map<N>::momenta(u, sqrt_s, p);
-        pass = pacuda::phase::passes(p, cuts);
-    }
-    const unsigned ballot = __ballot_sync(0xffffffffu, pass);
-    const int lane = threadIdx.x & 31;
-    unsigned long long base = 0;
-    if (lane == 0 && ballot) base = atomicAdd(sg.counter, (unsigned long long)__popc(ballot));
-    base = __shfl_sync(0xffffffffu, base, 0);
-    if (pass) {
-        const unsigned long long slot = base + __popc(ballot & ((1u << lane) - 1u));
-        if (slot < capacity) sg.index[slot] = sg.first + i;
-    }
+    list_block<N>(sg.seed, sg.first, sg.count, sqrt_s, cuts, sg.index, capacity, sg.counter,
+                  (blockIdx.x - c.block_first[k]) * 256 + threadIdx.x);
 }
 
 // the points of candidates index[0..n): source-major momenta [(leg * 4 + k) * n + i] for the

@@ -53,6 +53,25 @@ def test_candidates_and_points_match_oracle(family, final_state):
     assert np.array_equal(x.cpu().numpy(), U.features(u[keep], 0, 1, final_state))
 
 
+@pytest.mark.parametrize("family,final_state", [("qg>qgg", 3), ("qg>qggg", 4)])
+def test_listing_of_many_candidates_matches_oracle(family, final_state):
+    """2^22 candidates: the device's list (an f32 first look that drops only certain failures,
+    then the f64 map and cuts for the rest) holds exactly the candidates the f64 restatement
+    passes."""
+    pl = _pipeline((family,), capacity=1 << 21)
+    seed = pl.family_seed(0)
+    n, first = 1 << 22, 12345
+    got = pl.passing(0, first, n).cpu().numpy().astype(np.uint64)
+    want = []
+    for a in range(first, first + n, 1 << 20):
+        idx = np.arange(a, min(first + n, a + (1 << 20)), dtype=np.uint64)
+        p, _ = U.momenta(U.uniforms(seed, idx, final_state), SQRT_S, final_state)
+        want.append(idx[U.passes(p)])
+    want = np.concatenate(want)
+    assert 0.01 < len(want) / n < 0.5
+    assert np.array_equal(got, want), (len(got), len(want), np.setdiff1d(want, got)[:5], np.setdiff1d(got, want)[:5])
+
+
 def test_parts_of_a_family_add_up_to_the_oracle():
     """A subprocess of several plans (g g -> 4 g: three parts of its colour orderings): the
     pipeline's exact evaluation is the parts' outputs added in part order, bit for bit the
