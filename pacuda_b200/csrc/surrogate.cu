@@ -1122,28 +1122,32 @@ using pacuda::phase::Space;
 
 // The candidates first .. first + count - 1 of one stream: the indices of those inside the cuts,
 // appended (unordered, warp-aggregated) to index[] while below `capacity`; *count_out counts all
-// of them. A block takes 256 consecutive candidates: each thread gives its candidate the f32 first
-// look (phase.cuh surely_fails32), the ones it cannot drop are gathered in shared memory, and the
-// block's first threads take those through the f64 map and cuts, which decide. (Blocks of 256
-// threads: the kernels below are launched so.)
+// of them. A block takes LIST_ROUNDS x 256 consecutive candidates (candidate k of the block in
+// round k / 256 on thread k % 256): each thread gives its candidates the f32 first look
+// (phase.cuh surely_fails32), the ones it cannot drop are gathered in shared memory, and then the
+// block's threads take those through the f64 map and cuts, which decide; gathering several rounds
+// keeps the f64 pass's warps full. (Blocks of 256 threads: the kernels below are launched so.)
+constexpr uint32_t LIST_ROUNDS = 16, LIST_BLOCK = 256 * LIST_ROUNDS;
+
 template <int N>
 __device__ __forceinline__ void list_block(uint64_t seed, uint64_t first, uint32_t count, double sqrt_s,
                                            const Cuts &cuts, uint64_t *index, uint32_t capacity,
-                                           unsigned long long *count_out, uint32_t i) {
+                                           unsigned long long *count_out, uint32_t block_first) {
     constexpr int F = N, L = Space<N>::LEGS;
-    __shared__ uint64_t maybe[256];
+    __shared__ uint64_t maybe[LIST_BLOCK];
     __shared__ uint32_t n_maybe;
     if (threadIdx.x == 0) n_maybe = 0;
     __syncthreads();
     const int lane = threadIdx.x & 31;
-    bool check = false;
-    if (i < count) {
-        float u[Space<N>::NUMBERS], q[F][3];
-        pacuda::phase::uniforms32(seed, first + i, u);
-        pacuda::phase::final32(u, sqrt_s, q);
-        check = !pacuda::phase::surely_fails32(q, sqrt_s, cuts);
-    }
-    {
+    for (uint32_t r = 0; r < LIST_ROUNDS; r++) {
+        const uint64_t i = (uint64_t)block_first + r * 256 + threadIdx.x;
+        bool check = false;
+        if (i < count) {
+            float u[Space<N>::NUMBERS], q[F][3];
+            pacuda::phase::uniforms32(seed, first + i, u);
+            pacuda::phase::final32(u, sqrt_s, q);
+            check = !pacuda::phase::surely_fails32(q, sqrt_s, cuts);
+        }
         const unsigned ballot = __ballot_sync(0xffffffffu, check);
         uint32_t base = 0;
         if (lane == 0 && ballot) base = atomicAdd(&n_maybe, (uint32_t)__popc(ballot));
@@ -1152,23 +1156,25 @@ __device__ __forceinline__ void list_block(uint64_t seed, uint64_t first, uint32
     }
     __syncthreads();
     const uint32_t m = n_maybe;
-    if (threadIdx.x >= ((m + 31u) & ~31u)) return;  // whole warps without a listed candidate
-    bool pass = false;
-    uint64_t cand = 0;
-    if (threadIdx.x < m) {
-        cand = maybe[threadIdx.x];
-        double u[Space<N>::UNIFORMS], p[L][4];
-        pacuda::phase::uniforms(seed, cand, u);
-        Map<N>::momenta(u, sqrt_s, p);
-        pass = pacuda::phase::passes(p, cuts);
-    }
-    const unsigned ballot = __ballot_sync(0xffffffffu, pass);
-    unsigned long long base = 0;
-    if (lane == 0 && ballot) base = atomicAdd(count_out, (unsigned long long)__popc(ballot));
-    base = __shfl_sync(0xffffffffu, base, 0);
-    if (pass) {
-        const unsigned long long slot = base + __popc(ballot & ((1u << lane) - 1u));
-        if (slot < capacity) index[slot] = cand;
+    for (uint32_t at = 0; at < m; at += 256) {
+        if (at + threadIdx.x >= ((m + 31u) & ~31u)) break;  // whole warps past the last gathered candidate
+        bool pass = false;
+        uint64_t cand = 0;
+        if (at + threadIdx.x < m) {
+            cand = maybe[at + threadIdx.x];
+            double u[Space<N>::UNIFORMS], p[L][4];
+            pacuda::phase::uniforms(seed, cand, u);
+            Map<N>::momenta(u, sqrt_s, p);
+            pass = pacuda::phase::passes(p, cuts);
+        }
+        const unsigned ballot = __ballot_sync(0xffffffffu, pass);
+        unsigned long long base = 0;
+        if (lane == 0 && ballot) base = atomicAdd(count_out, (unsigned long long)__popc(ballot));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (pass) {
+            const unsigned long long slot = base + __popc(ballot & ((1u << lane) - 1u));
+            if (slot < capacity) index[slot] = cand;
+        }
     }
 }
 
@@ -1176,7 +1182,7 @@ template <int N>
 __global__ void __launch_bounds__(256) candidates_kernel(uint64_t seed, uint64_t first, uint32_t count, double sqrt_s,
                                                          Cuts cuts, uint64_t *index, uint32_t capacity,
                                                          unsigned long long *count_out) {
-    list_block<N>(seed, first, count, sqrt_s, cuts, index, capacity, count_out, blockIdx.x * 256 + threadIdx.x);
+    list_block<N>(seed, first, count, sqrt_s, cuts, index, capacity, count_out, blockIdx.x * LIST_BLOCK);
 }
 
 // several subprocesses' candidates in one launch: block b lists segment k's candidates when
@@ -1194,7 +1200,7 @@ __global__ void __launch_bounds__(256) candidate_segments_kernel(CandidateSegmen
     while (k + 1 < c.segments && blockIdx.x >= c.block_first[k + 1]) k++;
     const pacuda_uw_candidate_segment &sg = c.seg[k];
     list_block<N>(sg.seed, sg.first, sg.count, sqrt_s, cuts, sg.index, capacity, sg.counter,
-                  (blockIdx.x - c.block_first[k]) * 256 + threadIdx.x);
+                  (blockIdx.x - c.block_first[k]) * LIST_BLOCK);
 }
 
 // the points of candidates index[0..n): source-major momenta [(leg * 4 + k) * n + i] for the
@@ -1259,7 +1265,7 @@ extern "C" int pacuda_uw_candidates(uint64_t seed, uint64_t first, uint32_t coun
     g_last_launches = 0;
     if (!cuts || !index || !counter || count == 0 || !(sqrt_s > 0) || !final_state_valid(final_state)) return ST_INVALID;
     Cuts c{cuts->pt_min, cuts->eta_max, cuts->dr_min};
-    const dim3 grid((count + 255) / 256);
+    const dim3 grid((count + LIST_BLOCK - 1) / LIST_BLOCK);
     if (final_state == 4)
         candidates_kernel<4><<<grid, 256, 0, (cudaStream_t)stream>>>(seed, first, count, sqrt_s, c, index, capacity, counter);
     else
@@ -1282,7 +1288,7 @@ extern "C" int pacuda_uw_candidates_segments(const pacuda_uw_candidate_segment *
         if ((segs[k].count && !segs[k].index) || !segs[k].counter) return ST_INVALID;
         c.seg[k] = segs[k];
         c.block_first[k] = blocks;
-        blocks += (segs[k].count + 255) / 256;
+        blocks += (segs[k].count + LIST_BLOCK - 1) / LIST_BLOCK;
     }
     c.block_first[segments] = blocks;
     c.segments = segments;
