@@ -72,6 +72,21 @@ def test_listing_of_many_candidates_matches_oracle(family, final_state):
     assert np.array_equal(got, want), (len(got), len(want), np.setdiff1d(want, got)[:5], np.setdiff1d(got, want)[:5])
 
 
+@pytest.mark.parametrize("count", [1, 255, 4095, 4097, 12289])
+def test_listing_of_ragged_counts_matches_oracle(count):
+    """Counts that leave a listing block partly filled (a block takes 16 rounds of 256 candidates),
+    two families of different counts in one launch: each family's list is the f64 restatement's."""
+    pl = _pipeline(("gg>ggg", "qg>qgg"))
+    firsts = 777
+    counts = [count, count + 3]
+    n = pl.candidates(firsts, counts)
+    for k in range(2):
+        got = np.sort(pl.fams[k].cand[:n[k]].cpu().numpy().astype(np.uint64))
+        idx = np.arange(firsts, firsts + counts[k], dtype=np.uint64)
+        p, _ = U.momenta(U.uniforms(pl.family_seed(k), idx, 3), SQRT_S, 3)
+        assert np.array_equal(got, idx[U.passes(p)])
+
+
 def test_parts_of_a_family_add_up_to_the_oracle():
     """A subprocess of several plans (g g -> 4 g: three parts of its colour orderings): the
     pipeline's exact evaluation is the parts' outputs added in part order, bit for bit the
