@@ -459,6 +459,30 @@ def surrogate_kernels(torch, count=1 << 21, steps=5):
     return res
 
 
+def listing_case(torch, steps=5):
+    """The candidate listing alone (a small, self-contained case for profiling): every family's
+    candidates of one step listed inside the cuts, the p p -> 3 jets step's 2^22 candidates
+    (1 + steps launches) and then the p p -> 4 jets step's 2^25 (1 + steps); time per call with
+    its count read."""
+    from pacuda_b200 import processes
+    from pacuda_b200 import unweight as UW
+
+    res = {}
+    for name, fams, cand in (("pp3j", processes.PP3J, 1 << 22), ("pp4j", processes.PP4J, 1 << 25)):
+        counts = split_points(cand, SEED)
+        pl = UW.Pipeline(families=list(fams), capacity=int(0.4 * max(counts)) + 4096)
+        n = pl.candidates(0, counts)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            pl.candidates(0, counts)
+        e1.record()
+        e1.synchronize()
+        res[name] = {"candidates": cand, "ms": e0.elapsed_time(e1) / steps, "listed": n}
+        del pl
+    return res
+
+
 def oracle_parity(cases):
     """Bitwise parity of device outputs with the oracle: cases (label, template, point-major
     momenta, device outputs [point][helicity])."""
@@ -904,6 +928,8 @@ def main():
     ap.add_argument("--surrogate-args", default="", help="key=value,... for the surrogate line (development runs)")
     ap.add_argument("--surrogate-kernels", action="store_true", help="only the surrogate kernels on a random network "
                                                                       "(the profiling case)")
+    ap.add_argument("--listing", action="store_true", help="only the candidate listing of the two learned-part "
+                                                            "workloads (the profiling case)")
     ap.add_argument("--reference-gpu-kind", default=None, help=argparse.SUPPRESS)  # the worker of reference_gpu()
     ap.add_argument("--keep", default=None, help=argparse.SUPPRESS)
     args = ap.parse_args()
@@ -950,6 +976,9 @@ def main():
     build.build()
     if args.surrogate_kernels:
         print(json.dumps({"surrogate_kernels": surrogate_kernels(torch)}))
+        return
+    if args.listing:
+        print(json.dumps({"listing": listing_case(torch)}))
         return
     if args.surrogate_only:
         kw = {}
